@@ -1,0 +1,132 @@
+/*
+ * pscbfm_b200.h -- C ABI of the B200-native colored bond-fluctuation-model
+ * (BFM) sweep.
+ *
+ * One handle is one simulated system, with the life cycle of the reference's
+ * UpdaterGPUScBFM_AB_Type<T> (src/pscbfm/UpdaterGPUScBFM_AB_Type.h:177-518):
+ * setters -> bfm_initialize -> bfm_run (any number of times) -> read back ->
+ * bfm_cleanup / bfm_destroy.  Each entry point below names the reference
+ * method it replaces.  All functions return a status code (BFM_OK on
+ * success); bfm_last_error() gives the message of the last failure on that
+ * handle.  Plain pointers and sizes only: the library owns every device
+ * buffer, the caller owns the host buffers it passes in.
+ *
+ * Threading: one host thread per handle; handles are independent (each has
+ * its own stream and keeps its box constants in kernel arguments, unlike the
+ * reference's global __constant__ tables, .cu:84-133).
+ */
+#ifndef PSCBFM_B200_H
+#define PSCBFM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+enum {
+    BFM_OK = 0,
+    BFM_EINVAL = 1,      /* invalid argument: the reference throws std::invalid_argument */
+    BFM_ERUNTIME = 2,    /* invalid state / bond set / box: the reference throws std::runtime_error */
+    BFM_ECUDA = 3,       /* a CUDA call failed (the reference exit()s, cudacommon.hpp:36-51) */
+    BFM_ETIMEOUT = 4,    /* a bounded device-side wait gave up */
+    BFM_ENOTINIT = 5,    /* call needs bfm_initialize first */
+    BFM_EUNSUPPORTED = 6 /* feature not provided by this build */
+};
+
+/* random number generators, numbering of the reference's enum class Rng
+ * (UpdaterGPUScBFM_AB_Type.h:413-420) */
+enum { BFM_RNG_INTHASH = 1, BFM_RNG_SARU = 2, BFM_RNG_PHILOX = 3, BFM_RNG_PCG = 4, BFM_RNG_XORWOW = 5 };
+
+typedef struct bfm_handle bfm_handle;
+
+/* constructor / destructor: UpdaterGPUScBFM_AB_Type() / ~UpdaterGPUScBFM_AB_Type()
+ * (UpdaterGPUScBFM_AB_Type.h:453-454) */
+int bfm_create(bfm_handle **out);
+int bfm_destroy(bfm_handle *h);
+const char *bfm_last_error(const bfm_handle *h);
+
+/* setGpu (UpdaterGPUScBFM_AB_Type.h:490) */
+int bfm_set_gpu(bfm_handle *h, int gpu);
+/* copyBondSet (.h:491), dx, dy, dz in [-4, 3]; forbidden != 0 marks a forbidden bond */
+int bfm_copy_bond_set(bfm_handle *h, int dx, int dy, int dz, int forbidden);
+/* setNrOfAllMonomers (.h:492); may be called once per set-up */
+int bfm_set_nr_of_all_monomers(bfm_handle *h, uint32_t n);
+/* setAttribute (.h:493); stored, not used for the colouring */
+int bfm_set_attribute(bfm_handle *h, uint32_t i, int32_t attribute);
+/* setMonomerCoordinates (.h:494) */
+int bfm_set_monomer_coordinates(bfm_handle *h, uint32_t i, int32_t x, int32_t y, int32_t z);
+/* setConnectivity (.h:495): directed, the caller adds both directions; at most 8 per monomer */
+int bfm_set_connectivity(bfm_handle *h, uint32_t i, uint32_t j);
+/* setLatticeSize (.h:496): powers of two, 8 <= L <= 1024 per axis */
+int bfm_set_lattice_size(bfm_handle *h, uint64_t bx, uint64_t by, uint64_t bz);
+/* setPeriodicity (.h:505); only fully periodic boxes are simulated */
+int bfm_set_periodicity(bfm_handle *h, int px, int py, int pz);
+/* setAge / getAge (.h:506-507) */
+int bfm_set_age(bfm_handle *h, int64_t age);
+int bfm_get_age(const bfm_handle *h, int64_t *age);
+/* setRng / getRng (.h:508-509); IntHash (default, as .cu:1407) and Saru */
+int bfm_set_rng(bfm_handle *h, int rng);
+int bfm_get_rng(const bfm_handle *h, int *rng);
+/* setStepsBetweenSortings (.h:513), default 5000 (.cu:1379) */
+int bfm_set_steps_between_sortings(bfm_handle *h, int64_t steps);
+
+/* bulk variants of setMonomerCoordinates / setConnectivity for large systems:
+ * xyz holds 3*n int32; deg holds n counts, nbr8 holds 8 ids per monomer */
+int bfm_set_all_coordinates(bfm_handle *h, const int32_t *xyz, size_t n);
+int bfm_set_all_connectivity(bfm_handle *h, const uint8_t *deg, const uint32_t *nbr8, size_t n);
+
+/* initialize (.h:485, .cu:2393-2537): colouring, species slabs, lattices, first spatial sort */
+int bfm_initialize(bfm_handle *h);
+/* runSimulationOnGPU (.h:498, .cu:2902-3400): nmcs Monte-Carlo steps;
+ * synchronous, positions can be read back on return */
+int bfm_run(bfm_handle *h, uint32_t nmcs);
+/* getMonomerPositionInX/Y/Z (.h:501-503) */
+int bfm_get_monomer_position(bfm_handle *h, uint32_t i, int32_t *x, int32_t *y, int32_t *z);
+/* all positions (unfolded, as doCopyBack .cu:3402-3484 returns them), 3*n int32 */
+int bfm_get_positions(bfm_handle *h, int32_t *xyz, size_t n);
+/* cleanup (.h:487, .cu:3486-3502): frees the set-up; setters may be used again */
+int bfm_cleanup(bfm_handle *h);
+
+/* diagnostics used by the parity tests */
+/* the occupation bit lattice, Z-order, 32-bit words (bit i of word w = site 32*w+i) */
+int bfm_get_lattice(bfm_handle *h, uint32_t *words, size_t nwords);
+int bfm_get_lattice_words(const bfm_handle *h, size_t *nwords);
+int bfm_get_nspecies(const bfm_handle *h, uint32_t *nspecies);
+/* colour of every monomer (after initialize) */
+int bfm_get_colors(const bfm_handle *h, uint32_t *colors, size_t n);
+/* original ids of species sp in slot order (the RNG subsequence order); *count receives the size */
+int bfm_get_species_order(bfm_handle *h, uint32_t sp, uint32_t *ids, size_t cap, size_t *count);
+/* [attempted moves, candidates after the check kernel, accepted moves] since initialize */
+int bfm_get_counters(bfm_handle *h, uint64_t out3[3]);
+/* device time of the kernels of the last bfm_run, milliseconds (CUDA events on the handle's stream) */
+int bfm_get_last_run_ms(const bfm_handle *h, double *ms);
+/* kernel launches issued by the last bfm_run */
+int bfm_get_last_run_launches(const bfm_handle *h, uint64_t *launches);
+/* launch path: 0 = one check + one perform kernel per colour substep, captured
+ * in CUDA graphs; 1 = same kernels launched one by one */
+int bfm_set_launch_mode(bfm_handle *h, int mode);
+
+/* The species colouring initialize() uses (the reference's graphColoring,
+ * graphColoring.tpp:103-439, with uniform rebalancing as called at
+ * UpdaterGPUScBFM_AB_Type.cu:1566-1570); host only.  deg[n], nbr8[8n];
+ * colors[n] receives the colours, *ncolors their number. */
+int bfm_color_graph(uint32_t n, const uint8_t *deg, const uint32_t *nbr8, int uniform, uint32_t *colors,
+                    uint32_t *ncolors);
+
+/* Process-global R250 colour/seed generator, the counterpart of LeMonADE's
+ * RandomNumberGenerators whose r250_rand32() the reference calls
+ * (UpdaterGPUScBFM_AB_Type.cu:3065-3066).  State = 250 words + index. */
+int bfm_r250_seed(uint64_t seed);
+int bfm_r250_seed_words(const uint32_t *words, size_t n); /* n >= 250 */
+int bfm_r250_get_state(uint32_t state251[251]);
+int bfm_r250_set_state(const uint32_t state251[251]);
+uint32_t bfm_r250_rand32(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PSCBFM_B200_H */

@@ -1,0 +1,533 @@
+/*
+ * oracle/bfm_oracle.cpp -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A CPU restatement of the reference's colored bond-fluctuation-model sweep
+ * (lgh0504/pscbfm, src/pscbfm/UpdaterGPUScBFM_AB_Type.cu).  It is the checker
+ * for the product's CUDA path: only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline leg / reference arm of bench.py load it.  The product never
+ * links it and never falls back to it.
+ *
+ * Parity pins:
+ *   - RNG kernels (Saru, Hash) and the graph colouring are compared in CPU
+ *     tests against the reference's own headers (rngs/Saru.h, rngs/Hash.h,
+ *     graphColoring.tpp) compiled from its sources into oracle/_ref/.
+ *   - The whole sweep is compared on the GPU against the reference's own
+ *     updater (UpdaterGPUScBFM_AB_Type.cu built for sm_100a, oracle/_ref/).
+ *   - The host R250 generator of LeMonADE is absent from the reference tree;
+ *     oracle/r250.h restates the published R250 and that one part is unpinned.
+ *
+ * Every function below cites the reference lines it restates.
+ */
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <stack>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+#include <atomic>
+#include <omp.h>
+
+#include "r250.h"
+
+namespace orc {
+
+/* ------------------------------------------------------------------ RNGs */
+
+/* Saru (S. Worley, HOOMD-blue): seed premix + one LCG/Weyl step.
+ * Restates rngs/Saru.h:153-170 (init), :240-247 (u32<1>), :257-261 (Weyl<1>).
+ * The caller passes (seed, iteration, subsequence) already truncated to
+ * 32 bits, as Saru::rng32 does (Saru.h:35-40). */
+static inline uint32_t saru_u32(uint32_t s1, uint32_t s2, uint32_t s3)
+{
+    s3 ^= (s1 << 7) ^ (s2 >> 6);
+    s2 += (s1 >> 4) ^ (s3 >> 15);
+    s1 ^= (s2 << 9) + (s3 << 8);
+    s3 ^= 0xA5366B4Du * ((s2 >> 11) ^ (s1 << 1));
+    s2 += 0x72BE1579u * ((s1 << 4) ^ (s3 >> 16));
+    s1 ^= 0x3F38A6EDu * ((s3 >> 5) ^ (uint32_t)((int32_t)s2 >> 22));
+    s2 += s1 * s3;
+    s1 += s3 ^ (s2 >> 2);
+    s2 ^= (uint32_t)((int32_t)s2 >> 17);
+    uint32_t lcg = 0x79DEDEA3u * (s1 ^ (uint32_t)((int32_t)s1 >> 14));
+    uint32_t weyl = (lcg + s2) ^ (uint32_t)((int32_t)lcg >> 8);
+    lcg = lcg + weyl * (weyl ^ 0xDDDF97F5u);
+    weyl = 0xABCB96F7u + (weyl >> 1);
+    lcg = 0x4BEB5D59u * lcg + 0x2600E1F7u;
+    weyl = weyl + 0x8009D14Bu + ((uint32_t)((int32_t)weyl >> 31) & 0xDA879ADDu);
+    const uint32_t v = (lcg ^ (lcg >> 26)) + weyl;
+    return (v ^ (v >> 20)) * 0x6957F5A7u;
+}
+
+/* Robert Jenkins' 32-bit integer hash, as used by rngs/Hash.h:24-46 */
+static inline uint32_t jenkins_hash(uint32_t a)
+{
+    a = (a + 0x7ED55D16u) + (a << 12);
+    a = (a ^ 0xC761C23Cu) ^ (a >> 19);
+    a = (a + 0x165667B1u) + (a << 5);
+    a = (a + 0xD3A2646Cu) ^ (a << 9);
+    a = (a + 0xFD7046C5u) + (a << 3);
+    a = (a ^ 0xB55A4F09u) ^ (a >> 16);
+    return a;
+}
+
+/* Hash::rng32 (Hash.h:65-69): state = subsequence, hash(hash(state) ^ seed) */
+static inline uint32_t hash_rng(uint32_t seed, uint32_t subseq)
+{
+    return jenkins_hash(jenkins_hash(subseq) ^ seed);
+}
+
+enum { RNG_INTHASH = 1, RNG_SARU = 2, RNG_PHILOX = 3 };
+
+/* ---------------------------------------------------------- Z-order index */
+
+/* 10-bit -> 30-bit dilation with two zero bits between payload bits.  Equal to
+ * diluteBits<uint32_t,2> (UpdaterGPUScBFM_AB_Type.cu:204-230) for inputs
+ * below 1024. */
+static inline uint32_t dilate3(uint32_t x)
+{
+    x &= 0x3FFu;
+    x = (x | (x << 16)) & 0x030000FFu;
+    x = (x | (x << 8)) & 0x0300F00Fu;
+    x = (x | (x << 4)) & 0x030C30C3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+
+/* linearizeBoxVectorIndex with USE_ZCURVE_FOR_LATTICE (.cu:289-316) */
+static inline uint32_t zindex(int64_t x, int64_t y, int64_t z, uint32_t mx, uint32_t my, uint32_t mz)
+{
+    return dilate3((uint32_t)x & mx) | (dilate3((uint32_t)y & my) << 1) | (dilate3((uint32_t)z & mz) << 2);
+}
+
+/* linearizeBondVectorIndex (.cu:871-889) */
+static inline uint32_t bond_index(int64_t dx, int64_t dy, int64_t dz)
+{
+    return (uint32_t)(dx & 7) | ((uint32_t)(dy & 7) << 3) | ((uint32_t)(dz & 7) << 6);
+}
+
+/* ------------------------------------------------------- graph colouring */
+
+/* Restates graphColoring() (graphColoring.tpp:103-439): a depth-first greedy
+ * colouring (smallest colour not used by an already coloured neighbour, walk
+ * to the first uncoloured neighbour, stack the node when it has more than one
+ * uncoloured neighbour), optionally followed by the uniform rebalancing pass
+ * (:323-418) which moves nodes of over-full colours to the rarest colour that
+ * none of their neighbours has.  The rarest-first list is ordered with the
+ * same std::sort call as the reference (:335-338) and re-ordered after each
+ * change by a stable sort on the frequency (:390-394 use a stable bubble sort). */
+static std::vector<uint32_t> graph_coloring(uint32_t n, const uint32_t *nnbr, const uint32_t *nbr, bool uniform)
+{
+    const uint32_t NONE = 0xFFFFFFFFu;
+    const long long cNoNode = -1;
+    const uint32_t nMaxColors = 255;
+    std::vector<uint32_t> color(n, NONE);
+    std::vector<size_t> freq;
+    std::vector<uint8_t> used;
+    for (uint32_t start = 0; start < n; ++start) {
+        if (color[start] != NONE) continue;
+        std::stack<uint32_t> todo;
+        long long node = start;
+        while (true) {
+            used.assign(257, 0);
+            size_t nUncolored = 0;
+            long long firstUncolored = cNoNode;
+            for (uint32_t j = 0; j < nnbr[node]; ++j) {
+                const uint32_t nb = nbr[(size_t)node * 8 + j];
+                const uint32_t c = color[nb];
+                if (c != NONE) used[c] = 1;
+                else {
+                    ++nUncolored;
+                    if (firstUncolored == cNoNode) firstUncolored = nb;
+                }
+            }
+            uint32_t c = 0;
+            while (c < nMaxColors && used[c]) ++c;
+            if (c == nMaxColors)
+                throw std::runtime_error("Already used up the maximum amount of colors. Can't color the given polymer system automatically!");
+            color[node] = c;
+            if (c >= freq.size()) freq.resize(c + 1, 0);
+            ++freq[c];
+            if (nUncolored == 0 && todo.empty()) break;
+            if (nUncolored > 1) todo.push((uint32_t)node);
+            node = firstUncolored;
+            if (nUncolored == 0) {
+                while (!todo.empty()) {
+                    node = todo.top();
+                    size_t n2 = 0;
+                    long long first2 = cNoNode;
+                    for (uint32_t j = 0; j < nnbr[node]; ++j) {
+                        const uint32_t nb = nbr[(size_t)node * 8 + j];
+                        if (color[nb] == NONE) {
+                            ++n2;
+                            if (first2 == cNoNode) first2 = nb;
+                        }
+                    }
+                    if (n2 < 2) todo.pop();
+                    if (first2 != cNoNode) { node = first2; break; }
+                    node = cNoNode;
+                }
+                if (todo.empty() && node == cNoNode) break;
+            }
+        }
+    }
+    if (uniform && !freq.empty()) {
+        const size_t k = freq.size();
+        std::vector<std::pair<uint32_t, size_t>> rare(k);
+        for (size_t i = 0; i < k; ++i) rare[i] = {(uint32_t)i, freq[i]};
+        std::sort(rare.begin(), rare.end(),
+                  [](const std::pair<uint32_t, size_t> &a, const std::pair<uint32_t, size_t> &b) { return a.second < b.second; });
+        const size_t target = ((size_t)n + k - 1) / k;
+        for (uint32_t node = 0; node < n; ++node) {
+            if (freq[color[node]] <= target) continue;
+            for (size_t i = 0; i < k && rare[i].second < target; ++i) {
+                const uint32_t nc = rare[i].first;
+                bool ok = true;
+                for (uint32_t j = 0; j < nnbr[node]; ++j)
+                    if (color[nbr[(size_t)node * 8 + j]] == nc) ok = false;
+                if (!ok) continue;
+                const uint32_t oc = color[node];
+                --freq[oc];
+                ++freq[nc];
+                size_t iNew = 0, iOld = 0;
+                for (size_t q = 0; q < k; ++q) {
+                    if (rare[q].first == oc) iOld = q;
+                    if (rare[q].first == nc) iNew = q;
+                }
+                --rare[iOld].second;
+                ++rare[iNew].second;
+                std::stable_sort(rare.begin(), rare.end(),
+                                 [](const std::pair<uint32_t, size_t> &a, const std::pair<uint32_t, size_t> &b) { return a.second < b.second; });
+                color[node] = nc;
+            }
+        }
+    }
+    return color;
+}
+
+/* ------------------------------------------------- colored sweep emulator */
+
+static const int DX[6] = {-1, 1, 0, 0, 0, 0};
+static const int DY[6] = {0, 0, -1, 1, 0, 0};
+static const int DZ[6] = {0, 0, 0, 0, -1, 1};
+
+struct Sweep {
+    uint32_t Lx = 0, Ly = 0, Lz = 0, mx = 0, my = 0, mz = 0;
+    uint32_t n = 0;
+    std::vector<uint32_t> nnbr, nbr;          /* nbr: n x 8, original ids */
+    uint8_t forbidden[512];
+    int rng = RNG_SARU;
+    int64_t age = 0;
+    int64_t sortEvery = 5000;
+    std::vector<int64_t> px, py, pz;          /* absolute positions */
+    std::vector<uint32_t> color;
+    uint32_t nSpecies = 0;
+    std::vector<std::vector<uint32_t>> slab;  /* slab[s][i] = original id */
+    std::vector<uint8_t> lattice, tmp;
+    std::vector<uint8_t> flags;
+    std::vector<uint32_t> target;
+    uint64_t nAttempt = 0, nCandidate = 0, nAccept = 0;
+    int nThreads = 1;
+
+    uint32_t z(int64_t x, int64_t y, int64_t zz) const { return zindex(x, y, zz, mx, my, mz); }
+
+    /* doSpatialSorting (.cu:1835-1943): per species, order by the Z-curve
+     * index of the wrapped position.  The keys are unique (excluded volume),
+     * so any correct sort gives the reference's order. */
+    void spatialSort()
+    {
+        for (auto &s : slab) {
+            std::vector<std::pair<uint32_t, uint32_t>> kv(s.size());
+            for (size_t i = 0; i < s.size(); ++i) kv[i] = {z(px[s[i]], py[s[i]], pz[s[i]]), s[i]};
+            std::sort(kv.begin(), kv.end());
+            for (size_t i = 0; i < s.size(); ++i) s[i] = kv[i].second;
+        }
+    }
+
+    /* checkFront (.cu:420-869, version 6): OR over the 3x3 face one cell in
+     * front of the moved monomer, i.e. at r0 + 2*D along the move axis and
+     * -1..+1 along the two other axes. */
+    bool front(const std::vector<uint8_t> &lat, int64_t x0, int64_t y0, int64_t z0, int dir) const
+    {
+        const int axis = dir >> 1;
+        const int s2 = (dir & 1) ? 2 : -2;
+        for (int a = -1; a <= 1; ++a)
+            for (int b = -1; b <= 1; ++b) {
+                int64_t x = x0, y = y0, zz = z0;
+                if (axis == 0) { x += s2; y += a; zz += b; }
+                else if (axis == 1) { y += s2; x += a; zz += b; }
+                else { zz += s2; x += a; y += b; }
+                if (lat[z(x, y, zz)]) return true;
+            }
+        return false;
+    }
+
+    uint32_t draw(uint32_t seed, uint64_t iteration, uint32_t local) const
+    {
+        if (rng == RNG_INTHASH) return hash_rng(seed, local);
+        return saru_u32(seed, (uint32_t)iteration, local);
+    }
+
+    /* one colour substep: kernelSimulationScBFMCheckSpecies (.cu:930-1028)
+     * followed by kernelSimulationScBFMPerformSpeciesAndApply (.cu:1148-1190)
+     * with a clean temporary lattice (.cu:3050-3062, :3199-3209). */
+    void substep(uint32_t sp, uint32_t seed, uint64_t iteration)
+    {
+        const std::vector<uint32_t> &ids = slab[sp];
+        const long long m = (long long)ids.size();
+        flags.assign(m, 0);
+        target.assign(m, 0);
+        uint64_t nc = 0, na = 0;
+#pragma omp parallel for num_threads(nThreads) reduction(+ : nc) schedule(static)
+        for (long long i = 0; i < m; ++i) {
+            const uint32_t id = ids[i];
+            const uint32_t rn = draw(seed, iteration, (uint32_t)i);
+            const int dir = (int)(rn % 6u);
+            const int64_t x1 = px[id] + DX[dir], y1 = py[id] + DY[dir], z1 = pz[id] + DZ[dir];
+            bool bad = false;
+            for (uint32_t j = 0; j < nnbr[id] && !bad; ++j) {
+                const uint32_t nb = nbr[(size_t)id * 8 + j];
+                if (forbidden[bond_index(px[nb] - x1, py[nb] - y1, pz[nb] - z1)]) bad = true;
+            }
+            if (bad) continue;
+            if (front(lattice, px[id], py[id], pz[id], dir)) continue;
+            flags[i] = (uint8_t)(dir | 8);
+            target[i] = z(x1, y1, z1);
+            __atomic_store_n(&tmp[target[i]], (uint8_t)1, __ATOMIC_RELAXED);
+            ++nc;
+        }
+#pragma omp parallel for num_threads(nThreads) reduction(+ : na) schedule(static)
+        for (long long i = 0; i < m; ++i) {
+            if (!(flags[i] & 8)) continue;
+            const uint32_t id = ids[i];
+            const int dir = flags[i] & 7;
+            if (front(tmp, px[id], py[id], pz[id], dir)) continue;
+            lattice[z(px[id], py[id], pz[id])] = 0;
+            px[id] += DX[dir];
+            py[id] += DY[dir];
+            pz[id] += DZ[dir];
+            lattice[z(px[id], py[id], pz[id])] = 1;
+            ++na;
+        }
+        /* clear the temporary lattice: only candidate targets were set */
+#pragma omp parallel for num_threads(nThreads) schedule(static)
+        for (long long i = 0; i < m; ++i)
+            if (flags[i] & 8) __atomic_store_n(&tmp[target[i]], (uint8_t)0, __ATOMIC_RELAXED);
+        nAttempt += (uint64_t)m;
+        nCandidate += nc;
+        nAccept += na;
+    }
+
+    /* runSimulationOnGPU (.cu:2902-3400), periodic boxes */
+    void run(uint32_t nMCS, R250State &r250)
+    {
+        for (uint32_t iStep = 0; iStep < nMCS; ++iStep, ++age) {
+            if (age % sortEvery == 0) spatialSort();
+            for (uint32_t iSub = 0; iSub < nSpecies; ++iSub) {
+                /* .cu:3049: mAge has already been advanced by iStep */
+                const uint64_t currentAge = (uint64_t)age + (uint64_t)iStep * nSpecies + iSub;
+                const uint32_t sp = (uint32_t)((uint64_t)r250_next(r250) % nSpecies);
+                const uint32_t seed = r250_next(r250);
+                substep(sp, seed, currentAge);
+            }
+        }
+    }
+};
+
+} // namespace orc
+
+using namespace orc;
+
+/* ================================================================ C ABI === */
+extern "C" {
+
+uint32_t orc_saru(uint32_t seed, uint32_t iteration, uint32_t subseq) { return saru_u32(seed, iteration, subseq); }
+uint32_t orc_hash_rng(uint32_t seed, uint32_t subseq) { return hash_rng(seed, subseq); }
+uint32_t orc_zindex(int64_t x, int64_t y, int64_t z, uint32_t mx, uint32_t my, uint32_t mz) { return zindex(x, y, z, mx, my, mz); }
+
+void orc_r250_seed_u64(uint32_t *state251, uint64_t seed)
+{
+    R250State s;
+    r250_seed_u64(s, seed);
+    std::memcpy(state251, s.buf, sizeof(s.buf));
+    state251[250] = s.idx;
+}
+void orc_r250_seed_words(uint32_t *state251, const uint32_t *words250)
+{
+    R250State s;
+    r250_seed_words(s, words250);
+    std::memcpy(state251, s.buf, sizeof(s.buf));
+    state251[250] = s.idx;
+}
+void orc_r250_draw(uint32_t *state251, uint32_t *out, size_t n)
+{
+    R250State s;
+    std::memcpy(s.buf, state251, sizeof(s.buf));
+    s.idx = state251[250];
+    for (size_t i = 0; i < n; ++i) out[i] = r250_next(s);
+    std::memcpy(state251, s.buf, sizeof(s.buf));
+    state251[250] = s.idx;
+}
+
+/* colors_out[n]; returns number of colours or -1 on error */
+int orc_graph_coloring(uint32_t n, const uint32_t *nnbr, const uint32_t *nbr8, int uniform, uint32_t *colors_out)
+{
+    try {
+        auto c = graph_coloring(n, nnbr, nbr8, uniform != 0);
+        uint32_t k = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            colors_out[i] = c[i];
+            k = std::max(k, c[i] + 1);
+        }
+        return (int)k;
+    } catch (...) {
+        return -1;
+    }
+}
+
+/* Stateful emulator mirroring the updater life cycle: create = setters +
+ * initialize (.cu:2393-2537), run = runSimulationOnGPU, get = copy-back. */
+void *orc_sweep_create(uint32_t Lx, uint32_t Ly, uint32_t Lz, uint32_t n, const int32_t *pos3, const uint32_t *nnbr,
+                       const uint32_t *nbr8, const uint8_t *forbidden512, int rng, int64_t age, int64_t sortEvery,
+                       int nThreads)
+{
+    try {
+        auto *s = new Sweep();
+        s->Lx = Lx; s->Ly = Ly; s->Lz = Lz;
+        s->mx = Lx - 1; s->my = Ly - 1; s->mz = Lz - 1;
+        s->n = n;
+        s->nnbr.assign(nnbr, nnbr + n);
+        s->nbr.assign(nbr8, nbr8 + (size_t)n * 8);
+        std::memcpy(s->forbidden, forbidden512, 512);
+        s->rng = rng;
+        s->age = age;
+        s->sortEvery = sortEvery;
+        s->nThreads = nThreads > 0 ? nThreads : 1;
+        s->px.resize(n); s->py.resize(n); s->pz.resize(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            s->px[i] = pos3[3 * i];
+            s->py[i] = pos3[3 * i + 1];
+            s->pz[i] = pos3[3 * i + 2];
+        }
+        s->color = graph_coloring(n, nnbr, nbr8, true);
+        uint32_t k = 0;
+        for (uint32_t i = 0; i < n; ++i) k = std::max(k, s->color[i] + 1);
+        s->nSpecies = k;
+        s->slab.assign(k, {});
+        for (uint32_t i = 0; i < n; ++i) s->slab[s->color[i]].push_back(i); /* .cu:1648-1650 */
+        const uint32_t Lm = std::max(Lx, std::max(Ly, Lz));
+        const size_t sites = (size_t)Lm * Lm * Lm;
+        s->lattice.assign(sites, 0);
+        s->tmp.assign(sites, 0);
+        for (uint32_t i = 0; i < n; ++i) s->lattice[s->z(s->px[i], s->py[i], s->pz[i])] = 1; /* .cu:2164-2171 */
+        if (s->age != 0) s->spatialSort(); /* .cu:2511-2512 */
+        return s;
+    } catch (...) {
+        return nullptr;
+    }
+}
+
+void orc_sweep_destroy(void *h) { delete (Sweep *)h; }
+
+void orc_sweep_run(void *h, uint32_t nMCS, uint32_t *state251)
+{
+    auto *s = (Sweep *)h;
+    R250State r;
+    std::memcpy(r.buf, state251, sizeof(r.buf));
+    r.idx = state251[250];
+    s->run(nMCS, r);
+    std::memcpy(state251, r.buf, sizeof(r.buf));
+    state251[250] = r.idx;
+}
+
+void orc_sweep_get(void *h, int32_t *pos3)
+{
+    auto *s = (Sweep *)h;
+    for (uint32_t i = 0; i < s->n; ++i) {
+        pos3[3 * i] = (int32_t)s->px[i];
+        pos3[3 * i + 1] = (int32_t)s->py[i];
+        pos3[3 * i + 2] = (int32_t)s->pz[i];
+    }
+}
+
+int64_t orc_sweep_age(void *h) { return ((Sweep *)h)->age; }
+uint32_t orc_sweep_nspecies(void *h) { return ((Sweep *)h)->nSpecies; }
+void orc_sweep_colors(void *h, uint32_t *out)
+{
+    auto *s = (Sweep *)h;
+    std::memcpy(out, s->color.data(), sizeof(uint32_t) * s->n);
+}
+/* slot order of species sp (original ids), after the latest spatial sort */
+uint32_t orc_sweep_slab(void *h, uint32_t sp, uint32_t *out)
+{
+    auto *s = (Sweep *)h;
+    if (out) std::memcpy(out, s->slab[sp].data(), sizeof(uint32_t) * s->slab[sp].size());
+    return (uint32_t)s->slab[sp].size();
+}
+void orc_sweep_stats(void *h, uint64_t *out3)
+{
+    auto *s = (Sweep *)h;
+    out3[0] = s->nAttempt;
+    out3[1] = s->nCandidate;
+    out3[2] = s->nAccept;
+}
+
+/* -------------------------------------------- serial (random-sequential) BFM
+ * The statistical reference: LeMonADE's serial updater (UpdaterSimpleSimulator
+ * with MoveLocalSc) is not in the reference tree, so this is a plain
+ * Metropolis BFM written from the model definition: pick a random monomer and
+ * one of the 6 unit moves, accept if all bonds stay in the bond set and the
+ * 2x2x2 cube does not overlap another one.  One MCS = n attempts. */
+static inline uint64_t xs_next(uint64_t &s)
+{
+    s ^= s << 13;
+    s ^= s >> 7;
+    s ^= s << 17;
+    return s;
+}
+
+uint64_t orc_serial_run(uint32_t Lx, uint32_t Ly, uint32_t Lz, uint32_t n, int32_t *pos3, const uint32_t *nnbr,
+                        const uint32_t *nbr8, const uint8_t *forbidden512, uint64_t nMCS, uint64_t seed)
+{
+    const uint32_t mx = Lx - 1, my = Ly - 1, mz = Lz - 1;
+    const uint32_t Lm = std::max(Lx, std::max(Ly, Lz));
+    std::vector<uint8_t> lat((size_t)Lm * Lm * Lm, 0);
+    for (uint32_t i = 0; i < n; ++i) lat[zindex(pos3[3 * i], pos3[3 * i + 1], pos3[3 * i + 2], mx, my, mz)] = 1;
+    uint64_t st = seed ? seed : 0x9E3779B97F4A7C15ull;
+    uint64_t accepted = 0;
+    const uint64_t total = nMCS * (uint64_t)n;
+    for (uint64_t t = 0; t < total; ++t) {
+        const uint64_t r = xs_next(st);
+        const uint32_t id = (uint32_t)(((r >> 32) * (uint64_t)n) >> 32);
+        const int dir = (int)((r & 0xFFFFFFFFull) % 6ull);
+        int32_t *p = pos3 + 3 * (size_t)id;
+        const int64_t x1 = p[0] + DX[dir], y1 = p[1] + DY[dir], z1 = p[2] + DZ[dir];
+        bool bad = false;
+        for (uint32_t j = 0; j < nnbr[id] && !bad; ++j) {
+            const int32_t *q = pos3 + 3 * (size_t)nbr8[(size_t)id * 8 + j];
+            if (forbidden512[bond_index(q[0] - x1, q[1] - y1, q[2] - z1)]) bad = true;
+        }
+        if (bad) continue;
+        const int axis = dir >> 1;
+        const int s2 = (dir & 1) ? 2 : -2;
+        for (int a = -1; a <= 1 && !bad; ++a)
+            for (int b = -1; b <= 1 && !bad; ++b) {
+                int64_t x = p[0], y = p[1], zz = p[2];
+                if (axis == 0) { x += s2; y += a; zz += b; }
+                else if (axis == 1) { y += s2; x += a; zz += b; }
+                else { zz += s2; x += a; y += b; }
+                if (lat[zindex(x, y, zz, mx, my, mz)]) bad = true;
+            }
+        if (bad) continue;
+        lat[zindex(p[0], p[1], p[2], mx, my, mz)] = 0;
+        p[0] = (int32_t)x1; p[1] = (int32_t)y1; p[2] = (int32_t)z1;
+        lat[zindex(x1, y1, z1, mx, my, mz)] = 1;
+        ++accepted;
+    }
+    return accepted;
+}
+
+} /* extern "C" */

@@ -1,0 +1,125 @@
+"""Build and load the native library ``libpscbfm_b200.so`` (CUDA, sm_100a).
+
+The library is built in-tree next to this file so that it travels with the
+repository.  There is no fallback: if the shared object is missing or cannot
+be loaded, :func:`lib` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIBNAME = "libpscbfm_b200.so"
+LIBPATH = os.path.join(HERE, LIBNAME)
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+SOURCES = ["bfm_engine.cu"]
+HEADERS = ["bfm_device.cuh", "bfm_host.hpp", "../../include/pscbfm_b200.h"]
+
+NVCC_FLAGS = [
+    "-std=c++17",
+    "-O3",
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-lineinfo",
+    "-Xcompiler", "-fPIC",
+    "-shared",
+]
+
+
+def _stale() -> bool:
+    if not os.path.exists(LIBPATH):
+        return True
+    t = os.path.getmtime(LIBPATH)
+    for f in SOURCES + HEADERS:
+        if os.path.getmtime(os.path.join(CSRC, f)) > t:
+            return True
+    return False
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile the CUDA sources into the in-tree shared library."""
+    if not force and not _stale():
+        return LIBPATH
+    cmd = [NVCC, *NVCC_FLAGS, "-o", LIBPATH] + [os.path.join(CSRC, s) for s in SOURCES]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True, cwd=CSRC)
+    return LIBPATH
+
+
+_lock = threading.Lock()
+_lib = None
+
+# status codes of include/pscbfm_b200.h
+BFM_OK, BFM_EINVAL, BFM_ERUNTIME, BFM_ECUDA, BFM_ETIMEOUT, BFM_ENOTINIT, BFM_EUNSUPPORTED = range(7)
+
+_c = ctypes
+_P = _c.c_void_p
+_SIGS = {
+    "bfm_create": (_c.c_int, [_c.POINTER(_P)]),
+    "bfm_destroy": (_c.c_int, [_P]),
+    "bfm_last_error": (_c.c_char_p, [_P]),
+    "bfm_set_gpu": (_c.c_int, [_P, _c.c_int]),
+    "bfm_copy_bond_set": (_c.c_int, [_P, _c.c_int, _c.c_int, _c.c_int, _c.c_int]),
+    "bfm_set_nr_of_all_monomers": (_c.c_int, [_P, _c.c_uint32]),
+    "bfm_set_attribute": (_c.c_int, [_P, _c.c_uint32, _c.c_int32]),
+    "bfm_set_monomer_coordinates": (_c.c_int, [_P, _c.c_uint32, _c.c_int32, _c.c_int32, _c.c_int32]),
+    "bfm_set_connectivity": (_c.c_int, [_P, _c.c_uint32, _c.c_uint32]),
+    "bfm_set_lattice_size": (_c.c_int, [_P, _c.c_uint64, _c.c_uint64, _c.c_uint64]),
+    "bfm_set_periodicity": (_c.c_int, [_P, _c.c_int, _c.c_int, _c.c_int]),
+    "bfm_set_age": (_c.c_int, [_P, _c.c_int64]),
+    "bfm_get_age": (_c.c_int, [_P, _c.POINTER(_c.c_int64)]),
+    "bfm_set_rng": (_c.c_int, [_P, _c.c_int]),
+    "bfm_get_rng": (_c.c_int, [_P, _c.POINTER(_c.c_int)]),
+    "bfm_set_steps_between_sortings": (_c.c_int, [_P, _c.c_int64]),
+    "bfm_set_all_coordinates": (_c.c_int, [_P, _P, _c.c_size_t]),
+    "bfm_set_all_connectivity": (_c.c_int, [_P, _P, _P, _c.c_size_t]),
+    "bfm_initialize": (_c.c_int, [_P]),
+    "bfm_run": (_c.c_int, [_P, _c.c_uint32]),
+    "bfm_get_monomer_position": (_c.c_int, [_P, _c.c_uint32, _c.POINTER(_c.c_int32), _c.POINTER(_c.c_int32), _c.POINTER(_c.c_int32)]),
+    "bfm_get_positions": (_c.c_int, [_P, _P, _c.c_size_t]),
+    "bfm_cleanup": (_c.c_int, [_P]),
+    "bfm_get_lattice": (_c.c_int, [_P, _P, _c.c_size_t]),
+    "bfm_get_lattice_words": (_c.c_int, [_P, _c.POINTER(_c.c_size_t)]),
+    "bfm_get_nspecies": (_c.c_int, [_P, _c.POINTER(_c.c_uint32)]),
+    "bfm_get_colors": (_c.c_int, [_P, _P, _c.c_size_t]),
+    "bfm_get_species_order": (_c.c_int, [_P, _c.c_uint32, _P, _c.c_size_t, _c.POINTER(_c.c_size_t)]),
+    "bfm_get_counters": (_c.c_int, [_P, _P]),
+    "bfm_get_last_run_ms": (_c.c_int, [_P, _c.POINTER(_c.c_double)]),
+    "bfm_get_last_run_launches": (_c.c_int, [_P, _c.POINTER(_c.c_uint64)]),
+    "bfm_set_launch_mode": (_c.c_int, [_P, _c.c_int]),
+    "bfm_color_graph": (_c.c_int, [_c.c_uint32, _P, _P, _c.c_int, _P, _P]),
+    "bfm_r250_seed": (_c.c_int, [_c.c_uint64]),
+    "bfm_r250_seed_words": (_c.c_int, [_P, _c.c_size_t]),
+    "bfm_r250_get_state": (_c.c_int, [_P]),
+    "bfm_r250_set_state": (_c.c_int, [_P]),
+    "bfm_r250_rand32": (_c.c_uint32, []),
+}
+
+
+def exported_symbols() -> list[str]:
+    """Names of every entry point declared in include/pscbfm_b200.h."""
+    return list(_SIGS)
+
+
+def lib() -> ctypes.CDLL:
+    """Load the native library (building it first if the sources are newer)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if _stale():
+                build()
+            if not os.path.exists(LIBPATH):
+                raise RuntimeError(f"{LIBPATH} is missing: build the CUDA extension first")
+            L = ctypes.CDLL(LIBPATH)
+            for name, (res, args) in _SIGS.items():
+                fn = getattr(L, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = L
+        return _lib

@@ -1,0 +1,164 @@
+/*
+ * bfm_device.cuh -- device arithmetic of the colored BFM sweep.
+ *
+ * Positions are stored as Z-order (Morton) codes of the wrapped lattice
+ * coordinates: bit 3k holds bit k of x, bit 3k+1 bit k of y, bit 3k+2 bit k
+ * of z.  This is exactly the lattice index of the reference
+ * (linearizeBoxVectorIndex with USE_ZCURVE_FOR_LATTICE,
+ * UpdaterGPUScBFM_AB_Type.cu:289-316), so a position is also its own lattice
+ * address and its own spatial sort key (.cu:1809-1817).  Unit moves,
+ * periodic wrap, the 3x3 leading face and the bond vector are computed
+ * directly on the codes with dilated-integer arithmetic:
+ *     a (+) unit_k = ((a | ~M_k) + unit_k) & M_k
+ *     a (-) b      = (a - b) & M_k
+ * where M_k masks the payload bits of axis k inside the box.
+ */
+#pragma once
+#include <cstdint>
+
+namespace bfm {
+
+/* Per-system geometry: payload masks of the three axes, limited to the box
+ * (power-of-two edge lengths, so masking is the periodic wrap). */
+struct Geometry {
+    uint32_t m[3];      /* m[0] = dilated(Lx-1), m[1] = dilated(Ly-1) << 1, m[2] = dilated(Lz-1) << 2 */
+};
+
+__host__ __device__ inline uint32_t dilate3(uint32_t x)
+{
+    x &= 0x3FFu;
+    x = (x | (x << 16)) & 0x030000FFu;
+    x = (x | (x << 8)) & 0x0300F00Fu;
+    x = (x | (x << 4)) & 0x030C30C3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+
+__host__ __device__ inline uint32_t undilate3(uint32_t x)
+{
+    x &= 0x09249249u;
+    x = (x | (x >> 2)) & 0x030C30C3u;
+    x = (x | (x >> 4)) & 0x0300F00Fu;
+    x = (x | (x >> 8)) & 0x030000FFu;
+    x = (x | (x >> 16)) & 0x000003FFu;
+    return x;
+}
+
+__host__ __device__ inline uint32_t zcode(uint32_t x, uint32_t y, uint32_t z)
+{
+    return dilate3(x) | (dilate3(y) << 1) | (dilate3(z) << 2);
+}
+
+/* +1 / -1 along one axis with periodic wrap (mask = that axis' payload) */
+__host__ __device__ inline uint32_t zinc(uint32_t a, uint32_t mask, uint32_t unit)
+{
+    return (a & ~mask) | (((a | ~mask) + unit) & mask);
+}
+__host__ __device__ inline uint32_t zdec(uint32_t a, uint32_t mask, uint32_t unit)
+{
+    return (a & ~mask) | (((a & mask) - unit) & mask);
+}
+
+/* Move direction table of the reference (.cu:1539-1541): 0:-x 1:+x 2:-y 3:+y 4:-z 5:+z */
+__host__ __device__ inline uint32_t zstep(uint32_t a, int dir, const Geometry &g)
+{
+    const int ax = dir >> 1;
+    const uint32_t unit = 1u << ax;
+    return (dir & 1) ? zinc(a, g.m[ax], unit) : zdec(a, g.m[ax], unit);
+}
+
+/* Interleaved 9-bit code of the bond vector (b - a) mod 8 per axis.  The
+ * bond table is stored in this order (see host table builder). */
+__host__ __device__ inline uint32_t zbond(uint32_t b, uint32_t a)
+{
+    const uint32_t dx = ((b & 0x049u) - (a & 0x049u)) & 0x049u;
+    const uint32_t dy = ((b & 0x092u) - (a & 0x092u)) & 0x092u;
+    const uint32_t dz = ((b & 0x124u) - (a & 0x124u)) & 0x124u;
+    return dx | dy | dz;
+}
+
+/* The nine lattice sites of the leading face of a monomer at r0 moving in
+ * dir: along the move axis at r0 + 2*D, along the two other axes -1, 0, +1
+ * (checkFront, .cu:420-869).  Written out as the 3 values of each transverse
+ * axis plus the common part. */
+struct Face {
+    uint32_t base;      /* all bits except the two transverse axes */
+    uint32_t b[3];      /* transverse axis B: coordinate -1, 0, +1 */
+    uint32_t c[3];      /* transverse axis C: coordinate -1, 0, +1 */
+};
+
+__host__ __device__ inline Face zface(uint32_t r0, int dir, const Geometry &g)
+{
+    const int ax = dir >> 1;
+    const int bx = (ax == 0) ? 1 : 0;
+    const int cx = (ax == 2) ? 1 : 2;
+    const uint32_t unit = 1u << ax;
+    uint32_t p = (dir & 1) ? zinc(zinc(r0, g.m[ax], unit), g.m[ax], unit)
+                           : zdec(zdec(r0, g.m[ax], unit), g.m[ax], unit);
+    const uint32_t mb = g.m[bx], mc = g.m[cx];
+    const uint32_t ub = 1u << bx, uc = 1u << cx;
+    Face f;
+    f.base = p & ~(mb | mc);
+    const uint32_t vb = p & mb, vc = p & mc;
+    f.b[0] = (vb - ub) & mb;
+    f.b[1] = vb;
+    f.b[2] = ((vb | ~mb) + ub) & mb;
+    f.c[0] = (vc - uc) & mc;
+    f.c[1] = vc;
+    f.c[2] = ((vc | ~mc) + uc) & mc;
+    return f;
+}
+
+/* ------------------------------------------------------------------ RNGs */
+
+enum RngKind { RNG_INTHASH = 1, RNG_SARU = 2, RNG_PHILOX = 3 };
+
+/* Saru generator (S. Worley, HOOMD-blue; rngs/Saru.h:153-170 and
+ * :240-261 of the reference): churn (seed, iteration, subsequence) into an
+ * LCG + Weyl state and take one output.  The three keys are 32-bit, as in
+ * the reference where they are truncated at Saru::init. */
+__host__ __device__ inline uint32_t saru(uint32_t k1, uint32_t k2, uint32_t k3)
+{
+    k3 ^= (k1 << 7) ^ (k2 >> 6);
+    k2 += (k1 >> 4) ^ (k3 >> 15);
+    k1 ^= (k2 << 9) + (k3 << 8);
+    k3 ^= 0xA5366B4Du * ((k2 >> 11) ^ (k1 << 1));
+    k2 += 0x72BE1579u * ((k1 << 4) ^ (k3 >> 16));
+    k1 ^= 0x3F38A6EDu * ((k3 >> 5) ^ (uint32_t)((int32_t)k2 >> 22));
+    k2 += k1 * k3;
+    k1 += k3 ^ (k2 >> 2);
+    k2 ^= (uint32_t)((int32_t)k2 >> 17);
+    uint32_t x = 0x79DEDEA3u * (k1 ^ (uint32_t)((int32_t)k1 >> 14));
+    uint32_t y = (x + k2) ^ (uint32_t)((int32_t)x >> 8);
+    x = x + y * (y ^ 0xDDDF97F5u);
+    y = 0xABCB96F7u + (y >> 1);
+    x = 0x4BEB5D59u * x + 0x2600E1F7u;
+    y = y + 0x8009D14Bu + ((uint32_t)((int32_t)y >> 31) & 0xDA879ADDu);
+    const uint32_t v = (x ^ (x >> 26)) + y;
+    return (v ^ (v >> 20)) * 0x6957F5A7u;
+}
+
+/* Robert Jenkins' 32-bit integer mix, the reference's IntHash generator
+ * (rngs/Hash.h:24-46, :65-69): hash(hash(subsequence) ^ seed). */
+__host__ __device__ inline uint32_t jhash(uint32_t a)
+{
+    a = (a + 0x7ED55D16u) + (a << 12);
+    a = (a ^ 0xC761C23Cu) ^ (a >> 19);
+    a = (a + 0x165667B1u) + (a << 5);
+    a = (a + 0xD3A2646Cu) ^ (a << 9);
+    a = (a + 0xFD7046C5u) + (a << 3);
+    a = (a ^ 0xB55A4F09u) ^ (a >> 16);
+    return a;
+}
+
+template <int RNG>
+__host__ __device__ inline uint32_t draw(uint32_t seed, uint32_t iteration, uint32_t local)
+{
+    if (RNG == RNG_INTHASH) return jhash(jhash(local) ^ seed);
+    return saru(seed, iteration, local);
+}
+
+/* Direction from the random number: rn % 6 (.cu:967) */
+__host__ __device__ inline int direction(uint32_t rn) { return (int)(rn % 6u); }
+
+} // namespace bfm

@@ -1,0 +1,1108 @@
+/*
+ * bfm_engine.cu -- the colored BFM sweep on one B200 (sm_100a), behind the C
+ * ABI declared in include/pscbfm_b200.h.
+ *
+ * Data layout in HBM (one handle):
+ *   pos   uint32[npad]          Z-order code of the wrapped position, one slot
+ *                               per monomer; slots grouped by colour (species)
+ *                               in slabs padded to 128 slots (512 B)
+ *   img   int32[3][npad]        periodic image counters (unfolded position =
+ *                               wrapped + img * L), touched only on wrap moves
+ *   nbr   uint32[maxdeg][npad]  neighbour slot ids, row j = j-th bond
+ *   deg   uint8[npad]           bonds per monomer
+ *   flags uint8[npad]           check -> perform hand-over (dir | 8)
+ *   lat   uint32[L^3/32]        occupation, 1 bit per site, Z-order
+ *   tmp   uint32[2][L^3/32]     bit lattice of move targets, double buffered
+ *
+ * One colour substep = k_check (RNG, bond test, leading-face test on lat,
+ * mark target in tmp) + k_perform (leading-face test on tmp, apply), the
+ * two-phase scheme of the reference's kernelSimulationScBFMCheckSpecies
+ * (.cu:930-1028) and kernelSimulationScBFMPerformSpeciesAndApply
+ * (.cu:1148-1190).  The colour, seed and RNG iteration of every substep are
+ * drawn on the host exactly as runSimulationOnGPU does (.cu:3047-3066) and
+ * uploaded as a schedule, so a whole chunk of substeps runs without the host.
+ */
+#include <cuda_runtime.h>
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "bfm_device.cuh"
+#include "bfm_host.hpp"
+#include "../../include/pscbfm_b200.h"
+
+using namespace bfm;
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr uint32_t kSlabAlign = 128;
+constexpr uint32_t kNoId = 0xFFFFFFFFu;
+constexpr uint32_t kChunk = 4096;       /* substeps per uploaded schedule chunk */
+constexpr uint32_t kGraphSubsteps = 64; /* substeps per captured CUDA graph */
+
+struct Species {
+    uint32_t off, n;
+};
+
+/* one colour substep, as drawn by the host */
+struct Substep {
+    uint32_t species;
+    uint32_t seed;
+    uint32_t iter;   /* RNG iteration = currentAge truncated to 32 bit (.cu:3049) */
+    uint32_t buf;    /* temporary lattice buffer used by this substep */
+};
+
+struct Bondset {
+    uint32_t forbidden[16]; /* 512 bits indexed by the interleaved bond code (zbond) */
+};
+
+struct Sys {
+    uint32_t *pos;
+    int32_t *img;
+    const uint32_t *nbr;
+    const uint8_t *deg;
+    uint8_t *flags;
+    uint32_t *lat;
+    uint32_t *tmp;
+    const Species *spec;
+    unsigned long long *counters;
+    uint32_t npad;
+    uint32_t latWords;
+    Geometry g;
+    Bondset bonds;
+};
+
+/* ------------------------------------------------------------- kernels */
+
+__device__ __forceinline__ bool face_occupied(const uint32_t *__restrict__ lat, uint32_t r0, int dir, const Geometry &g)
+{
+    const Face f = zface(r0, dir, g);
+    uint32_t any = 0;
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const uint32_t s = f.base | f.b[b] | f.c[c];
+            any |= __ldg(lat + (s >> 5)) >> (s & 31u);
+        }
+    return any & 1u;
+}
+
+/* Check phase of one colour substep, plus zeroing of the other temporary
+ * buffer (used by the previous substep, needed clean by the next one). */
+template <int RNG>
+__global__ void __launch_bounds__(kThreads) k_check(Sys s, const Substep *__restrict__ sched, uint32_t k)
+{
+    const Substep d = sched[k];
+    const Species sp = s.spec[d.species];
+    __shared__ uint32_t forbid[16];
+    if (threadIdx.x < 16) forbid[threadIdx.x] = s.bonds.forbidden[threadIdx.x];
+
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    {
+        uint4 *clr = reinterpret_cast<uint4 *>(s.tmp + (size_t)(d.buf ^ 1u) * s.latWords);
+        const uint32_t n4 = s.latWords >> 2;
+        for (uint32_t w = tid; w < n4; w += stride) clr[w] = make_uint4(0, 0, 0, 0);
+    }
+    __syncthreads();
+
+    uint32_t *tmp = s.tmp + (size_t)d.buf * s.latWords;
+    unsigned int nCand = 0;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < sp.n; base += stride) {
+        const uint32_t i = base + threadIdx.x;
+        int cand = 0;
+        if (i < sp.n) {
+            const uint32_t slot = sp.off + i;
+            const uint32_t r0 = s.pos[slot];
+            const int dir = direction(draw<RNG>(d.seed, d.iter, i));
+            const uint32_t r1 = zstep(r0, dir, s.g);
+            const uint32_t nb = s.deg[slot];
+            bool ok = true;
+            for (uint32_t j = 0; j < nb; ++j) {
+                const uint32_t q = s.pos[s.nbr[(size_t)j * s.npad + slot]];
+                const uint32_t code = zbond(q, r1);
+                if ((forbid[code >> 5] >> (code & 31u)) & 1u) {
+                    ok = false;
+                    break;
+                }
+            }
+            if (ok) ok = !face_occupied(s.lat, r0, dir, s.g);
+            uint8_t f = 0;
+            if (ok) {
+                f = (uint8_t)(dir | 8);
+                atomicOr(tmp + (r1 >> 5), 1u << (r1 & 31u));
+                cand = 1;
+            }
+            s.flags[slot] = f;
+        }
+        nCand += __syncthreads_count(cand);
+    }
+    if (threadIdx.x == 0 && nCand && s.counters) atomicAdd(s.counters + 0, (unsigned long long)nCand);
+}
+
+/* Perform phase: a candidate moves unless another candidate's target lies
+ * in its leading face (the deterministic two-phase rule of the reference). */
+__global__ void __launch_bounds__(kThreads) k_perform(Sys s, const Substep *__restrict__ sched, uint32_t k)
+{
+    const Substep d = sched[k];
+    const Species sp = s.spec[d.species];
+    const uint32_t *tmp = s.tmp + (size_t)d.buf * s.latWords;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    unsigned int nAcc = 0;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < sp.n; base += stride) {
+        const uint32_t i = base + threadIdx.x;
+        int acc = 0;
+        if (i < sp.n) {
+            const uint32_t slot = sp.off + i;
+            const uint8_t f = s.flags[slot];
+            if (f & 8) {
+                const uint32_t r0 = s.pos[slot];
+                const int dir = f & 7;
+                if (!face_occupied(tmp, r0, dir, s.g)) {
+                    const uint32_t r1 = zstep(r0, dir, s.g);
+                    const uint32_t w0 = r0 >> 5, w1 = r1 >> 5;
+                    const uint32_t b0 = 1u << (r0 & 31u), b1 = 1u << (r1 & 31u);
+                    if (w0 == w1) {
+                        atomicXor(s.lat + w0, b0 | b1);
+                    } else {
+                        atomicXor(s.lat + w0, b0);
+                        atomicXor(s.lat + w1, b1);
+                    }
+                    s.pos[slot] = r1;
+                    const int ax = dir >> 1;
+                    const bool wrapped = (dir & 1) ? ((r1 & s.g.m[ax]) == 0) : ((r0 & s.g.m[ax]) == 0);
+                    if (wrapped) s.img[(size_t)ax * s.npad + slot] += (dir & 1) ? 1 : -1;
+                    acc = 1;
+                }
+            }
+        }
+        nAcc += __syncthreads_count(acc);
+    }
+    if (threadIdx.x == 0 && nAcc && s.counters) atomicAdd(s.counters + 1, (unsigned long long)nAcc);
+}
+
+/* spatial re-sort support: inv[perm[i]] = i */
+__global__ void k_invert(const uint32_t *__restrict__ perm, uint32_t *__restrict__ inv, uint32_t npad)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npad; i += gridDim.x * blockDim.x) inv[perm[i]] = i;
+}
+
+/* gather every per-slot array into the new slot order and remap neighbour ids */
+__global__ void k_permute(const uint32_t *__restrict__ perm, const uint32_t *__restrict__ inv, uint32_t npad,
+                          uint32_t maxdeg, const uint32_t *__restrict__ pos, const int32_t *__restrict__ img,
+                          const uint32_t *__restrict__ nbr, const uint8_t *__restrict__ deg,
+                          const uint32_t *__restrict__ s2o, uint32_t *__restrict__ pos2, int32_t *__restrict__ img2,
+                          uint32_t *__restrict__ nbr2, uint8_t *__restrict__ deg2, uint32_t *__restrict__ s2o2,
+                          uint32_t *__restrict__ o2s)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npad; i += gridDim.x * blockDim.x) {
+        const uint32_t p = perm[i];
+        pos2[i] = pos[p];
+        img2[i] = img[p];
+        img2[npad + i] = img[npad + p];
+        img2[2 * (size_t)npad + i] = img[2 * (size_t)npad + p];
+        const uint8_t dg = deg[p];
+        deg2[i] = dg;
+        for (uint32_t j = 0; j < maxdeg; ++j)
+            nbr2[(size_t)j * npad + i] = j < dg ? inv[nbr[(size_t)j * npad + p]] : 0u;
+        const uint32_t o = s2o[p];
+        s2o2[i] = o;
+        if (o != kNoId) o2s[o] = i;
+    }
+}
+
+/* unfolded positions in original monomer order (doCopyBack, .cu:3402-3484) */
+__global__ void k_unpack(const uint32_t *__restrict__ pos, const int32_t *__restrict__ img,
+                         const uint32_t *__restrict__ s2o, uint32_t npad, int32_t Lx, int32_t Ly, int32_t Lz,
+                         int32_t *__restrict__ out)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npad; i += gridDim.x * blockDim.x) {
+        const uint32_t o = s2o[i];
+        if (o == kNoId) continue;
+        const uint32_t c = pos[i];
+        out[3 * (size_t)o + 0] = (int32_t)undilate3(c) + img[i] * Lx;
+        out[3 * (size_t)o + 1] = (int32_t)undilate3(c >> 1) + img[npad + i] * Ly;
+        out[3 * (size_t)o + 2] = (int32_t)undilate3(c >> 2) + img[2 * (size_t)npad + i] * Lz;
+    }
+}
+
+/* ------------------------------------------------------------- host side */
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct InvalidArgument : std::invalid_argument {
+    using std::invalid_argument::invalid_argument;
+};
+
+#define CK(call)                                                                                          \
+    do {                                                                                                  \
+        cudaError_t e_ = (call);                                                                          \
+        if (e_ != cudaSuccess)                                                                            \
+            throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_));                          \
+    } while (0)
+
+template <typename T>
+void dalloc(T *&p, size_t n)
+{
+    p = nullptr;
+    if (n) CK(cudaMalloc((void **)&p, n * sizeof(T)));
+}
+template <typename T>
+void dfree(T *&p)
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+std::mutex g_r250_mutex;
+R250 &global_r250()
+{
+    static R250 r = [] {
+        R250 t;
+        t.seed_u64(0);
+        return t;
+    }();
+    return r;
+}
+
+uint32_t ilog2(uint64_t v)
+{
+    uint32_t l = 0;
+    while (v >>= 1) ++l;
+    return l;
+}
+
+struct Engine {
+    /* ---- configuration (setters) */
+    int gpu = 0;
+    uint8_t forbidden[512]; /* linear index (dx&7)|(dy&7)<<3|(dz&7)<<6, as copyBondSet (.cu:2540-2545) */
+    bool nSet = false;
+    uint32_t n = 0;
+    std::vector<int32_t> xyz;
+    std::vector<int32_t> attr;
+    std::vector<uint8_t> deg;
+    std::vector<uint32_t> nbr; /* n x 8 original ids */
+    uint64_t L[3] = {0, 0, 0};
+    bool periodic[3] = {true, true, true};
+    int64_t age = 0;
+    int rng = BFM_RNG_INTHASH; /* the reference's default (.cu:1407) */
+    int64_t sortEvery = 5000;
+    int launchMode = 0;
+
+    /* ---- derived at initialize */
+    bool initialized = false;
+    Geometry g{};
+    Bondset bonds{};
+    uint32_t Lm = 0, keyBits = 0;
+    size_t latWords = 0;
+    std::vector<uint32_t> color;
+    std::vector<Species> spec;
+    uint32_t nSpecies = 0, npad = 0, maxdeg = 0, nmax = 0;
+
+    /* ---- device state */
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    uint32_t *d_pos = nullptr, *d_pos2 = nullptr;
+    int32_t *d_img = nullptr, *d_img2 = nullptr;
+    uint32_t *d_nbr = nullptr, *d_nbr2 = nullptr;
+    uint8_t *d_deg = nullptr, *d_deg2 = nullptr;
+    uint32_t *d_s2o = nullptr, *d_s2o2 = nullptr, *d_o2s = nullptr;
+    uint8_t *d_flags = nullptr;
+    uint32_t *d_lat = nullptr, *d_tmp = nullptr;
+    Species *d_spec = nullptr;
+    Substep *d_sched[2] = {nullptr, nullptr};
+    Substep *h_sched[2] = {nullptr, nullptr};
+    cudaEvent_t schedFree[2] = {nullptr, nullptr};
+    unsigned long long *d_counters = nullptr;
+    uint32_t *d_perm = nullptr, *d_inv = nullptr, *d_iota = nullptr, *d_keys = nullptr;
+    void *d_cub = nullptr;
+    size_t cubBytes = 0;
+    int32_t *d_out = nullptr;
+    int32_t *h_out = nullptr;
+    bool hostPosValid = false;
+
+    /* graphs: [schedule buffer][rng kind index] */
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int graphRng = -1;
+
+    uint64_t substepCounter = 0;
+    uint64_t nAttempts = 0;
+    bool sortedFresh = false;
+    double lastRunMs = 0;
+    uint64_t lastLaunches = 0;
+
+    std::string err;
+
+    ~Engine() { release(); }
+
+    void requireN(uint32_t i) const
+    {
+        if (!nSet) throw std::runtime_error("setNrOfAllMonomers has not been called");
+        if (i >= n) throw InvalidArgument("monomer index " + std::to_string(i) + " out of range (n = " + std::to_string(n) + ")");
+    }
+
+    void release()
+    {
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto &ge : graph)
+            if (ge) {
+                cudaGraphExecDestroy(ge);
+                ge = nullptr;
+            }
+        graphRng = -1;
+        dfree(d_pos); dfree(d_pos2); dfree(d_img); dfree(d_img2); dfree(d_nbr); dfree(d_nbr2);
+        dfree(d_deg); dfree(d_deg2); dfree(d_s2o); dfree(d_s2o2); dfree(d_o2s); dfree(d_flags);
+        dfree(d_lat); dfree(d_tmp); dfree(d_spec); dfree(d_counters); dfree(d_perm); dfree(d_inv);
+        dfree(d_iota); dfree(d_keys); dfree(d_out);
+        if (d_cub) cudaFree(d_cub);
+        d_cub = nullptr;
+        for (int b = 0; b < 2; ++b) {
+            dfree(d_sched[b]);
+            if (h_sched[b]) cudaFreeHost(h_sched[b]);
+            h_sched[b] = nullptr;
+            if (schedFree[b]) cudaEventDestroy(schedFree[b]);
+            schedFree[b] = nullptr;
+        }
+        if (h_out) cudaFreeHost(h_out);
+        h_out = nullptr;
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        ev0 = ev1 = nullptr;
+        if (stream) cudaStreamDestroy(stream);
+        stream = nullptr;
+        initialized = false;
+        hostPosValid = false;
+    }
+
+    Sys sys() const
+    {
+        Sys s;
+        s.pos = d_pos;
+        s.img = d_img;
+        s.nbr = d_nbr;
+        s.deg = d_deg;
+        s.flags = d_flags;
+        s.lat = d_lat;
+        s.tmp = d_tmp;
+        s.spec = d_spec;
+        s.counters = d_counters;
+        s.npad = npad;
+        s.latWords = (uint32_t)latWords;
+        s.g = g;
+        s.bonds = bonds;
+        return s;
+    }
+
+    /* ------------------------------------------------------ initialize */
+    void initialize()
+    {
+        if (initialized)
+            throw std::runtime_error("Initialize was already called and may not be called again until cleanup was called!");
+        if (!nSet || n == 0) throw std::runtime_error("setNrOfAllMonomers must be called with n > 0 before initialize");
+        for (int a = 0; a < 3; ++a) {
+            if (L[a] == 0) throw std::runtime_error("setLatticeSize must be called before initialize");
+            if (!periodic[a]) throw std::runtime_error("only fully periodic boxes are supported by this build");
+        }
+        if (rng != BFM_RNG_INTHASH && rng != BFM_RNG_SARU)
+            throw std::runtime_error("random number generator " + std::to_string(rng) + " is not provided by this build (IntHash = 1, Saru = 2)");
+        /* initializeBondTable (.cu:1516-1559): exactly 108 allowed bonds */
+        unsigned nAllowed = 0;
+        for (int i = 0; i < 512; ++i) nAllowed += forbidden[i] ? 0 : 1;
+        if (nAllowed != 108)
+            throw std::runtime_error("Wrong bond-set! Expected 108 allowed bonds, but got " + std::to_string(nAllowed));
+        std::memset(&bonds, 0, sizeof(bonds));
+        for (uint32_t dz = 0; dz < 8; ++dz)
+            for (uint32_t dy = 0; dy < 8; ++dy)
+                for (uint32_t dx = 0; dx < 8; ++dx)
+                    if (forbidden[dx | (dy << 3) | (dz << 6)]) {
+                        const uint32_t code = zcode(dx, dy, dz);
+                        bonds.forbidden[code >> 5] |= 1u << (code & 31);
+                    }
+
+        Lm = (uint32_t)std::max(L[0], std::max(L[1], L[2]));
+        keyBits = 3 * ilog2(Lm);
+        latWords = ((size_t)Lm * Lm * Lm) / 32;
+        for (int a = 0; a < 3; ++a) g.m[a] = dilate3((uint32_t)L[a] - 1) << a;
+
+        /* graph colouring (initializeSpeciesSorting, .cu:1561-1686) */
+        for (uint32_t i = 0; i < n; ++i)
+            for (uint32_t j = 0; j < deg[i]; ++j)
+                if (nbr[(size_t)i * 8 + j] >= n)
+                    throw InvalidArgument("bond partner id out of range for monomer " + std::to_string(i));
+        color = color_graph(n, deg.data(), nbr.data(), true);
+        nSpecies = 0;
+        for (uint32_t i = 0; i < n; ++i) nSpecies = std::max(nSpecies, color[i] + 1);
+        std::vector<uint32_t> count(nSpecies, 0);
+        for (uint32_t i = 0; i < n; ++i) ++count[color[i]];
+        spec.assign(nSpecies, Species{0, 0});
+        uint32_t off = 0;
+        nmax = 0;
+        for (uint32_t c = 0; c < nSpecies; ++c) {
+            spec[c].off = off;
+            spec[c].n = count[c];
+            nmax = std::max(nmax, count[c]);
+            off += (count[c] + kSlabAlign - 1) / kSlabAlign * kSlabAlign;
+        }
+        npad = std::max(off, kSlabAlign);
+        maxdeg = 0;
+        for (uint32_t i = 0; i < n; ++i) maxdeg = std::max<uint32_t>(maxdeg, deg[i]);
+
+        /* slot order inside a species: ascending original id (.cu:1648-1650) */
+        std::vector<uint32_t> o2s(n), s2o(npad, kNoId);
+        {
+            std::vector<uint32_t> next(nSpecies);
+            for (uint32_t c = 0; c < nSpecies; ++c) next[c] = spec[c].off;
+            for (uint32_t i = 0; i < n; ++i) {
+                o2s[i] = next[color[i]]++;
+                s2o[o2s[i]] = i;
+            }
+        }
+
+        /* wrapped codes + image counters (initializeSortedMonomerPositions, .cu:2066-2139),
+         * occupation lattice (initializeLattices, .cu:2141-2236) and the
+         * excluded-volume / bond checks of checkSystem (.cu:2789-2900) */
+        std::vector<uint32_t> hpos(npad, 0);
+        std::vector<int32_t> himg(3 * (size_t)npad, 0);
+        std::vector<uint32_t> hlat(latWords, 0);
+        std::vector<uint64_t> cells(((size_t)Lm * Lm * Lm + 63) / 64, 0);
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint32_t slot = o2s[i];
+            uint32_t w[3];
+            for (int a = 0; a < 3; ++a) {
+                const int64_t v = xyz[3 * (size_t)i + a];
+                const int64_t La = (int64_t)L[a];
+                int64_t q = v / La;
+                int64_t r = v - q * La;
+                if (r < 0) { r += La; --q; }
+                w[a] = (uint32_t)r;
+                himg[(size_t)a * npad + slot] = (int32_t)q;
+            }
+            const uint32_t code = zcode(w[0], w[1], w[2]);
+            hpos[slot] = code;
+            if ((hlat[code >> 5] >> (code & 31)) & 1u)
+                throw InvalidArgument("two monomers share the lattice position of monomer " + std::to_string(i));
+            hlat[code >> 5] |= 1u << (code & 31);
+            for (int c = 0; c < 8; ++c) {
+                const uint32_t cc = zcode((w[0] + (c & 1)) & (uint32_t)(L[0] - 1), (w[1] + ((c >> 1) & 1)) & (uint32_t)(L[1] - 1),
+                                          (w[2] + ((c >> 2) & 1)) & (uint32_t)(L[2] - 1));
+                if ((cells[cc >> 6] >> (cc & 63)) & 1u)
+                    throw InvalidArgument("excluded volume violated: the 2x2x2 cube of monomer " + std::to_string(i) + " overlaps another one");
+                cells[cc >> 6] |= 1ull << (cc & 63);
+            }
+        }
+        for (uint32_t i = 0; i < n; ++i)
+            for (uint32_t j = 0; j < deg[i]; ++j) {
+                const uint32_t k = nbr[(size_t)i * 8 + j];
+                const int64_t dx = (int64_t)xyz[3 * (size_t)k] - xyz[3 * (size_t)i];
+                const int64_t dy = (int64_t)xyz[3 * (size_t)k + 1] - xyz[3 * (size_t)i + 1];
+                const int64_t dz = (int64_t)xyz[3 * (size_t)k + 2] - xyz[3 * (size_t)i + 2];
+                if (dx < -3 || dx > 3 || dy < -3 || dy > 3 || dz < -3 || dz > 3 ||
+                    forbidden[(dx & 7) | ((dy & 7) << 3) | ((dz & 7) << 6)])
+                    throw InvalidArgument("bond " + std::to_string(i) + "-" + std::to_string(k) + " (" + std::to_string(dx) + "," +
+                                          std::to_string(dy) + "," + std::to_string(dz) + ") is not in the bond set");
+            }
+        std::vector<uint32_t> hnbr((size_t)std::max(maxdeg, 1u) * npad, 0);
+        std::vector<uint8_t> hdeg(npad, 0);
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint32_t slot = o2s[i];
+            hdeg[slot] = deg[i];
+            for (uint32_t j = 0; j < deg[i]; ++j) hnbr[(size_t)j * npad + slot] = o2s[nbr[(size_t)i * 8 + j]];
+        }
+
+        CK(cudaSetDevice(gpu));
+        CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        CK(cudaEventCreate(&ev0));
+        CK(cudaEventCreate(&ev1));
+        const size_t nbrRows = std::max(maxdeg, 1u);
+        dalloc(d_pos, npad); dalloc(d_pos2, npad);
+        dalloc(d_img, 3 * (size_t)npad); dalloc(d_img2, 3 * (size_t)npad);
+        dalloc(d_nbr, nbrRows * npad); dalloc(d_nbr2, nbrRows * npad);
+        dalloc(d_deg, npad); dalloc(d_deg2, npad);
+        dalloc(d_s2o, npad); dalloc(d_s2o2, npad); dalloc(d_o2s, n);
+        dalloc(d_flags, npad);
+        dalloc(d_lat, latWords);
+        dalloc(d_tmp, 2 * latWords);
+        dalloc(d_spec, nSpecies);
+        dalloc(d_counters, 4);
+        dalloc(d_perm, npad); dalloc(d_inv, npad); dalloc(d_iota, npad); dalloc(d_keys, npad);
+        dalloc(d_out, 3 * (size_t)n);
+        for (int b = 0; b < 2; ++b) {
+            dalloc(d_sched[b], std::max(kChunk, 256u * 2u));
+            CK(cudaMallocHost((void **)&h_sched[b], std::max(kChunk, 256u * 2u) * sizeof(Substep)));
+            CK(cudaEventCreateWithFlags(&schedFree[b], cudaEventDisableTiming));
+        }
+        CK(cudaMallocHost((void **)&h_out, 3 * (size_t)n * sizeof(int32_t)));
+        {
+            cub::DeviceRadixSort::SortPairs(nullptr, cubBytes, d_pos, d_keys, d_iota, d_perm, (int)nmax, 0, (int)keyBits, stream);
+            CK(cudaMalloc(&d_cub, std::max<size_t>(cubBytes, 16)));
+        }
+        std::vector<uint32_t> iota(npad);
+        for (uint32_t i = 0; i < npad; ++i) iota[i] = i;
+        CK(cudaMemcpyAsync(d_pos, hpos.data(), npad * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_img, himg.data(), himg.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_nbr, hnbr.data(), hnbr.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_deg, hdeg.data(), npad, cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_s2o, s2o.data(), npad * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_o2s, o2s.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_lat, hlat.data(), latWords * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_spec, spec.data(), nSpecies * sizeof(Species), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_iota, iota.data(), npad * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_perm, iota.data(), npad * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemsetAsync(d_tmp, 0, 2 * latWords * sizeof(uint32_t), stream));
+        CK(cudaMemsetAsync(d_flags, 0, npad, stream));
+        CK(cudaMemsetAsync(d_counters, 0, 4 * sizeof(unsigned long long), stream));
+        CK(cudaStreamSynchronize(stream));
+        substepCounter = 0;
+        nAttempts = 0;
+        initialized = true;
+        sortedFresh = false;
+        /* the reference sorts at initialize when age != 0 (.cu:2511-2512) and
+         * at the first step when age % stepsBetweenSortings == 0 (.cu:3005);
+         * the Z-order sort is idempotent, so sorting here always gives the
+         * same slot order before the first substep. */
+        spatialSort();
+        hostPosValid = false;
+    }
+
+    /* doSpatialSorting (.cu:1835-1943): per species, order slots by the
+     * Z-order code of the wrapped position (the position code itself). */
+    void spatialSort()
+    {
+        for (uint32_t c = 0; c < nSpecies; ++c) {
+            if (spec[c].n == 0) continue;
+            size_t bytes = cubBytes;
+            CK(cub::DeviceRadixSort::SortPairs(d_cub, bytes, d_pos + spec[c].off, d_keys, d_iota + spec[c].off,
+                                               d_perm + spec[c].off, (int)spec[c].n, 0, (int)keyBits, stream));
+        }
+        const int blocks = (int)std::min<uint32_t>((npad + kThreads - 1) / kThreads, 148 * 16);
+        k_invert<<<blocks, kThreads, 0, stream>>>(d_perm, d_inv, npad);
+        k_permute<<<blocks, kThreads, 0, stream>>>(d_perm, d_inv, npad, maxdeg, d_pos, d_img, d_nbr, d_deg, d_s2o, d_pos2,
+                                                   d_img2, d_nbr2, d_deg2, d_s2o2, d_o2s);
+        CK(cudaGetLastError());
+        std::swap(d_pos, d_pos2);
+        std::swap(d_img, d_img2);
+        std::swap(d_nbr, d_nbr2);
+        std::swap(d_deg, d_deg2);
+        std::swap(d_s2o, d_s2o2);
+        /* the captured graphs hold the old pointers */
+        for (auto &ge : graph)
+            if (ge) {
+                cudaGraphExecDestroy(ge);
+                ge = nullptr;
+            }
+        graphRng = -1;
+        sortedFresh = true;
+    }
+
+    int checkBlocks() const
+    {
+        const uint32_t want = std::max<uint32_t>((nmax + kThreads - 1) / kThreads, (uint32_t)((latWords / 4 + kThreads - 1) / kThreads));
+        return (int)std::max<uint32_t>(1, std::min<uint32_t>(want, 148u * 64u));
+    }
+    int performBlocks() const { return (int)std::max<uint32_t>(1, std::min<uint32_t>((nmax + kThreads - 1) / kThreads, 148u * 64u)); }
+
+    void launchSubstep(const Substep *sched, uint32_t k)
+    {
+        const Sys s = sys();
+        if (rng == BFM_RNG_SARU)
+            k_check<RNG_SARU><<<checkBlocks(), kThreads, 0, stream>>>(s, sched, k);
+        else
+            k_check<RNG_INTHASH><<<checkBlocks(), kThreads, 0, stream>>>(s, sched, k);
+        k_perform<<<performBlocks(), kThreads, 0, stream>>>(s, sched, k);
+    }
+
+    /* substeps per captured graph: a whole number of MCS */
+    uint32_t graphSubsteps() const { return std::max(1u, kGraphSubsteps / nSpecies) * nSpecies; }
+
+    void buildGraph(int b)
+    {
+        cudaGraph_t gr;
+        CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        for (uint32_t k = 0; k < graphSubsteps(); ++k) launchSubstep(d_sched[b], k);
+        CK(cudaStreamEndCapture(stream, &gr));
+        CK(cudaGraphInstantiate(&graph[b], gr, 0));
+        CK(cudaGraphDestroy(gr));
+    }
+
+    /* runSimulationOnGPU (.cu:2902-3400) */
+    void run(uint32_t nMCS)
+    {
+        if (!initialized) throw std::runtime_error("initialize must be called before runSimulationOnGPU");
+        hostPosValid = false;
+        if (graphRng != rng) {
+            for (auto &ge : graph)
+                if (ge) {
+                    cudaGraphExecDestroy(ge);
+                    ge = nullptr;
+                }
+            graphRng = rng;
+        }
+        R250 &r250 = global_r250();
+        std::lock_guard<std::mutex> lock(g_r250_mutex);
+        CK(cudaEventRecord(ev0, stream));
+        uint64_t launches = 0;
+        uint32_t iStep = 0;
+        int b = 0;
+        const uint32_t cap = launchMode == 0 ? graphSubsteps() : (kChunk / nSpecies) * nSpecies;
+        while (iStep < nMCS) {
+            /* one schedule chunk: whole MCS only, ending before a re-sort */
+            CK(cudaEventSynchronize(schedFree[b]));
+            Substep *hs = h_sched[b];
+            uint32_t m = 0;
+            bool sortFirst = false;
+            const uint32_t step0 = iStep;
+            while (iStep < nMCS && m + nSpecies <= cap) {
+                const int64_t a = age + iStep; /* mAge, advanced once per MCS (.cu:3002) */
+                if (a % sortEvery == 0) {      /* .cu:3005 */
+                    if (iStep != step0) break;
+                    sortFirst = true;
+                }
+                for (uint32_t sub = 0; sub < nSpecies; ++sub) {
+                    Substep &d = hs[m++];
+                    const uint64_t currentAge = (uint64_t)a + (uint64_t)iStep * nSpecies + sub; /* .cu:3049 */
+                    d.species = (uint32_t)((uint64_t)r250.next() % nSpecies);                /* .cu:3065 */
+                    d.seed = r250.next();                                                    /* .cu:3066 */
+                    d.iter = (uint32_t)currentAge;
+                    d.buf = (uint32_t)(substepCounter++ & 1u);
+                    nAttempts += spec[d.species].n;
+                }
+                ++iStep;
+            }
+            if (sortFirst && !sortedFresh) spatialSort();
+            CK(cudaMemcpyAsync(d_sched[b], hs, m * sizeof(Substep), cudaMemcpyHostToDevice, stream));
+            CK(cudaEventRecord(schedFree[b], stream));
+            if (launchMode == 0 && m == cap) {
+                if (!graph[b]) buildGraph(b);
+                CK(cudaGraphLaunch(graph[b], stream));
+                launches += 2 * (uint64_t)m;
+            } else {
+                for (uint32_t k = 0; k < m; ++k) launchSubstep(d_sched[b], k);
+                launches += 2 * (uint64_t)m;
+            }
+            CK(cudaGetLastError());
+            sortedFresh = false;
+            b ^= 1;
+        }
+        age += nMCS;
+        CK(cudaEventRecord(ev1, stream));
+        CK(cudaEventSynchronize(ev1));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ev0, ev1));
+        lastRunMs = ms;
+        lastLaunches = launches;
+        CK(cudaGetLastError());
+    }
+
+    void readback()
+    {
+        if (!initialized) throw std::runtime_error("initialize must be called first");
+        if (hostPosValid) return;
+        const int blocks = (int)std::min<uint32_t>((npad + kThreads - 1) / kThreads, 148 * 16);
+        k_unpack<<<blocks, kThreads, 0, stream>>>(d_pos, d_img, d_s2o, npad, (int32_t)L[0], (int32_t)L[1], (int32_t)L[2], d_out);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(h_out, d_out, 3 * (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        hostPosValid = true;
+    }
+};
+
+} // namespace
+
+struct bfm_handle {
+    Engine e;
+};
+
+/* ================================================================ C ABI */
+
+#define GUARD(h, ...)                                                 \
+    do {                                                               \
+        if (!(h)) return BFM_EINVAL;                                   \
+        try {                                                          \
+            __VA_ARGS__;                                               \
+            return BFM_OK;                                             \
+        } catch (CudaError const &ex) {                                \
+            (h)->e.err = ex.what();                                    \
+            return BFM_ECUDA;                                          \
+        } catch (std::invalid_argument const &ex) {                    \
+            (h)->e.err = ex.what();                                    \
+            return BFM_EINVAL;                                         \
+        } catch (std::exception const &ex) {                           \
+            (h)->e.err = ex.what();                                    \
+            return BFM_ERUNTIME;                                       \
+        }                                                              \
+    } while (0)
+
+extern "C" {
+
+int bfm_create(bfm_handle **out)
+{
+    if (!out) return BFM_EINVAL;
+    try {
+        auto *h = new bfm_handle();
+        std::memset(h->e.forbidden, 1, sizeof(h->e.forbidden));
+        *out = h;
+        return BFM_OK;
+    } catch (...) {
+        return BFM_ERUNTIME;
+    }
+}
+
+int bfm_destroy(bfm_handle *h)
+{
+    delete h;
+    return BFM_OK;
+}
+
+const char *bfm_last_error(const bfm_handle *h) { return h ? h->e.err.c_str() : "null handle"; }
+
+int bfm_set_gpu(bfm_handle *h, int gpu)
+{
+    GUARD(h, {
+        int count = 0;
+        CK(cudaGetDeviceCount(&count));
+        if (gpu < 0 || gpu >= count)
+            throw InvalidArgument("GPU with ID " + std::to_string(gpu) + " not present. Only " + std::to_string(count) + " GPUs are available.");
+        CK(cudaSetDevice(gpu));
+        h->e.gpu = gpu;
+    });
+}
+
+int bfm_copy_bond_set(bfm_handle *h, int dx, int dy, int dz, int forbidden)
+{
+    GUARD(h, {
+        if (dx < -4 || dx > 4 || dy < -4 || dy > 4 || dz < -4 || dz > 4) throw InvalidArgument("bond vector component outside [-4,4]");
+        h->e.forbidden[(dx & 7) | ((dy & 7) << 3) | ((dz & 7) << 6)] = forbidden ? 1 : 0;
+    });
+}
+
+int bfm_set_nr_of_all_monomers(bfm_handle *h, uint32_t n)
+{
+    GUARD(h, {
+        if (h->e.nSet) throw std::runtime_error("Number of Monomers already set to " + std::to_string(h->e.n) + "!");
+        h->e.n = n;
+        h->e.nSet = true;
+        h->e.xyz.assign(3 * (size_t)n, 0);
+        h->e.attr.assign(n, 0);
+        h->e.deg.assign(n, 0);
+        h->e.nbr.assign((size_t)n * 8, 0);
+    });
+}
+
+int bfm_set_attribute(bfm_handle *h, uint32_t i, int32_t a)
+{
+    GUARD(h, {
+        h->e.requireN(i);
+        h->e.attr[i] = a;
+    });
+}
+
+int bfm_set_monomer_coordinates(bfm_handle *h, uint32_t i, int32_t x, int32_t y, int32_t z)
+{
+    GUARD(h, {
+        h->e.requireN(i);
+        h->e.xyz[3 * (size_t)i] = x;
+        h->e.xyz[3 * (size_t)i + 1] = y;
+        h->e.xyz[3 * (size_t)i + 2] = z;
+    });
+}
+
+int bfm_set_connectivity(bfm_handle *h, uint32_t i, uint32_t j)
+{
+    GUARD(h, {
+        h->e.requireN(i);
+        if (h->e.deg[i] >= 8) throw InvalidArgument("The maximum amount of bonds per monomer (8) has been exceeded!");
+        h->e.nbr[(size_t)i * 8 + h->e.deg[i]++] = j;
+    });
+}
+
+int bfm_set_lattice_size(bfm_handle *h, uint64_t bx, uint64_t by, uint64_t bz)
+{
+    GUARD(h, {
+        const uint64_t b[3] = {bx, by, bz};
+        for (int a = 0; a < 3; ++a)
+            if (b[a] < 8 || b[a] > 1024 || (b[a] & (b[a] - 1)))
+                throw std::runtime_error("box size must be a power of two between 8 and 1024 in each direction, got " + std::to_string(b[a]));
+        for (int a = 0; a < 3; ++a) h->e.L[a] = b[a];
+    });
+}
+
+int bfm_set_periodicity(bfm_handle *h, int px, int py, int pz)
+{
+    GUARD(h, {
+        h->e.periodic[0] = px != 0;
+        h->e.periodic[1] = py != 0;
+        h->e.periodic[2] = pz != 0;
+    });
+}
+
+int bfm_set_age(bfm_handle *h, int64_t age) { GUARD(h, { h->e.age = age; }); }
+int bfm_get_age(const bfm_handle *h, int64_t *age)
+{
+    if (!h || !age) return BFM_EINVAL;
+    *age = h->e.age;
+    return BFM_OK;
+}
+int bfm_set_rng(bfm_handle *h, int rng)
+{
+    GUARD(h, {
+        if (rng < 1 || rng > 5) throw InvalidArgument("unknown random number generator " + std::to_string(rng));
+        h->e.rng = rng;
+    });
+}
+int bfm_get_rng(const bfm_handle *h, int *rng)
+{
+    if (!h || !rng) return BFM_EINVAL;
+    *rng = h->e.rng;
+    return BFM_OK;
+}
+int bfm_set_steps_between_sortings(bfm_handle *h, int64_t steps)
+{
+    GUARD(h, {
+        if (steps <= 0) throw InvalidArgument("steps between sortings must be positive");
+        h->e.sortEvery = steps;
+    });
+}
+
+int bfm_set_all_coordinates(bfm_handle *h, const int32_t *xyz, size_t n)
+{
+    GUARD(h, {
+        if (!h->e.nSet || n != h->e.n || !xyz) throw InvalidArgument("coordinate array does not match setNrOfAllMonomers");
+        std::memcpy(h->e.xyz.data(), xyz, 3 * n * sizeof(int32_t));
+    });
+}
+
+int bfm_set_all_connectivity(bfm_handle *h, const uint8_t *deg, const uint32_t *nbr8, size_t n)
+{
+    GUARD(h, {
+        if (!h->e.nSet || n != h->e.n || !deg || !nbr8) throw InvalidArgument("connectivity arrays do not match setNrOfAllMonomers");
+        for (size_t i = 0; i < n; ++i)
+            if (deg[i] > 8) throw InvalidArgument("The maximum amount of bonds per monomer (8) has been exceeded!");
+        std::memcpy(h->e.deg.data(), deg, n);
+        std::memcpy(h->e.nbr.data(), nbr8, n * 8 * sizeof(uint32_t));
+    });
+}
+
+int bfm_initialize(bfm_handle *h)
+{
+    if (!h) return BFM_EINVAL;
+    try {
+        h->e.initialize();
+        return BFM_OK;
+    } catch (CudaError const &ex) {
+        h->e.err = ex.what();
+        h->e.release();
+        return BFM_ECUDA;
+    } catch (std::invalid_argument const &ex) {
+        h->e.err = ex.what();
+        h->e.release();
+        return BFM_EINVAL;
+    } catch (std::exception const &ex) {
+        h->e.err = ex.what();
+        h->e.release();
+        return BFM_ERUNTIME;
+    }
+}
+
+int bfm_run(bfm_handle *h, uint32_t nmcs)
+{
+    if (h && !h->e.initialized) {
+        h->e.err = "initialize must be called before runSimulationOnGPU";
+        return BFM_ENOTINIT;
+    }
+    GUARD(h, { h->e.run(nmcs); });
+}
+
+int bfm_get_monomer_position(bfm_handle *h, uint32_t i, int32_t *x, int32_t *y, int32_t *z)
+{
+    if (h && !h->e.initialized) {
+        h->e.err = "initialize must be called first";
+        return BFM_ENOTINIT;
+    }
+    GUARD(h, {
+        h->e.requireN(i);
+        h->e.readback();
+        if (x) *x = h->e.h_out[3 * (size_t)i];
+        if (y) *y = h->e.h_out[3 * (size_t)i + 1];
+        if (z) *z = h->e.h_out[3 * (size_t)i + 2];
+    });
+}
+
+int bfm_get_positions(bfm_handle *h, int32_t *xyz, size_t n)
+{
+    if (h && !h->e.initialized) {
+        h->e.err = "initialize must be called first";
+        return BFM_ENOTINIT;
+    }
+    GUARD(h, {
+        if (!xyz || n != h->e.n) throw InvalidArgument("position buffer does not match the number of monomers");
+        h->e.readback();
+        std::memcpy(xyz, h->e.h_out, 3 * n * sizeof(int32_t));
+    });
+}
+
+int bfm_cleanup(bfm_handle *h)
+{
+    GUARD(h, {
+        h->e.release();
+        h->e.nSet = false;
+        h->e.n = 0;
+    });
+}
+
+int bfm_get_lattice_words(const bfm_handle *h, size_t *nwords)
+{
+    if (!h || !nwords) return BFM_EINVAL;
+    if (!h->e.initialized) return BFM_ENOTINIT;
+    *nwords = h->e.latWords;
+    return BFM_OK;
+}
+
+int bfm_get_lattice(bfm_handle *h, uint32_t *words, size_t nwords)
+{
+    if (h && !h->e.initialized) return BFM_ENOTINIT;
+    GUARD(h, {
+        if (!words || nwords != h->e.latWords) throw InvalidArgument("lattice buffer size mismatch");
+        CK(cudaMemcpyAsync(words, h->e.d_lat, nwords * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->e.stream));
+        CK(cudaStreamSynchronize(h->e.stream));
+    });
+}
+
+int bfm_get_nspecies(const bfm_handle *h, uint32_t *ns)
+{
+    if (!h || !ns) return BFM_EINVAL;
+    if (!h->e.initialized) return BFM_ENOTINIT;
+    *ns = h->e.nSpecies;
+    return BFM_OK;
+}
+
+int bfm_get_colors(const bfm_handle *h, uint32_t *colors, size_t n)
+{
+    if (!h || !colors) return BFM_EINVAL;
+    if (!h->e.initialized) return BFM_ENOTINIT;
+    if (n != h->e.n) return BFM_EINVAL;
+    std::memcpy(colors, h->e.color.data(), n * sizeof(uint32_t));
+    return BFM_OK;
+}
+
+int bfm_get_species_order(bfm_handle *h, uint32_t sp, uint32_t *ids, size_t cap, size_t *count)
+{
+    if (h && !h->e.initialized) return BFM_ENOTINIT;
+    GUARD(h, {
+        if (sp >= h->e.nSpecies) throw InvalidArgument("species index out of range");
+        const Species s = h->e.spec[sp];
+        if (count) *count = s.n;
+        if (ids) {
+            if (cap < s.n) throw InvalidArgument("buffer too small");
+            CK(cudaMemcpyAsync(ids, h->e.d_s2o + s.off, s.n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->e.stream));
+            CK(cudaStreamSynchronize(h->e.stream));
+        }
+    });
+}
+
+int bfm_get_counters(bfm_handle *h, uint64_t out3[3])
+{
+    if (h && !h->e.initialized) return BFM_ENOTINIT;
+    GUARD(h, {
+        unsigned long long c[4];
+        CK(cudaMemcpyAsync(c, h->e.d_counters, sizeof(c), cudaMemcpyDeviceToHost, h->e.stream));
+        CK(cudaStreamSynchronize(h->e.stream));
+        out3[0] = h->e.nAttempts;
+        out3[1] = c[0];
+        out3[2] = c[1];
+    });
+}
+
+int bfm_get_last_run_ms(const bfm_handle *h, double *ms)
+{
+    if (!h || !ms) return BFM_EINVAL;
+    *ms = h->e.lastRunMs;
+    return BFM_OK;
+}
+
+int bfm_get_last_run_launches(const bfm_handle *h, uint64_t *launches)
+{
+    if (!h || !launches) return BFM_EINVAL;
+    *launches = h->e.lastLaunches;
+    return BFM_OK;
+}
+
+int bfm_set_launch_mode(bfm_handle *h, int mode)
+{
+    GUARD(h, {
+        if (mode < 0 || mode > 1) throw InvalidArgument("launch mode must be 0 (graphs) or 1 (direct)");
+        h->e.launchMode = mode;
+    });
+}
+
+int bfm_color_graph(uint32_t n, const uint8_t *deg, const uint32_t *nbr8, int uniform, uint32_t *colors, uint32_t *ncolors)
+{
+    if ((n && (!deg || !nbr8 || !colors)) || !ncolors) return BFM_EINVAL;
+    try {
+        for (uint32_t i = 0; i < n; ++i) {
+            if (deg[i] > 8) return BFM_EINVAL;
+            for (uint32_t j = 0; j < deg[i]; ++j)
+                if (nbr8[(size_t)i * 8 + j] >= n) return BFM_EINVAL;
+        }
+        const std::vector<uint32_t> c = color_graph(n, deg, nbr8, uniform != 0);
+        uint32_t k = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            colors[i] = c[i];
+            k = std::max(k, c[i] + 1);
+        }
+        *ncolors = k;
+        return BFM_OK;
+    } catch (...) {
+        return BFM_ERUNTIME;
+    }
+}
+
+int bfm_r250_seed(uint64_t seed)
+{
+    std::lock_guard<std::mutex> lock(g_r250_mutex);
+    global_r250().seed_u64(seed);
+    return BFM_OK;
+}
+
+int bfm_r250_seed_words(const uint32_t *words, size_t n)
+{
+    if (!words || n < 250) return BFM_EINVAL;
+    std::lock_guard<std::mutex> lock(g_r250_mutex);
+    global_r250().seed_words(words);
+    return BFM_OK;
+}
+
+int bfm_r250_get_state(uint32_t state251[251])
+{
+    if (!state251) return BFM_EINVAL;
+    std::lock_guard<std::mutex> lock(g_r250_mutex);
+    std::memcpy(state251, global_r250().buf, 250 * sizeof(uint32_t));
+    state251[250] = global_r250().idx;
+    return BFM_OK;
+}
+
+int bfm_r250_set_state(const uint32_t state251[251])
+{
+    if (!state251 || state251[250] >= 250) return BFM_EINVAL;
+    std::lock_guard<std::mutex> lock(g_r250_mutex);
+    std::memcpy(global_r250().buf, state251, 250 * sizeof(uint32_t));
+    global_r250().idx = state251[250];
+    return BFM_OK;
+}
+
+uint32_t bfm_r250_rand32(void)
+{
+    std::lock_guard<std::mutex> lock(g_r250_mutex);
+    return global_r250().next();
+}
+
+} /* extern "C" */

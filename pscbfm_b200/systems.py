@@ -1,0 +1,327 @@
+"""Synthetic BFM systems: the standard bond set and seeded polymer generators.
+
+The reference ships no input systems for this path (its golden
+``tests/*.bfm`` files are absent), so every benchmark and test system is
+generated here from a seed:
+
+* ``saw_chains``      linear chains grown as self-avoiding walks (dilute
+                      melts, e.g. 128 chains x 64 on 128^3);
+* ``ordered_melt``    a dense volume-fraction-0.5 melt built as a serpentine
+                      crystal (e.g. 4096 chains x 256 on 256^3) that the
+                      sweep itself melts;
+* ``star_comb``       3-arm stars with side chains (branched, >2 colours
+                      possible after cross-links);
+* ``add_crosslinks``  extra bonds between close monomers, giving odd cycles
+                      and therefore 3 or more colours.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from itertools import permutations, product
+
+import numpy as np
+
+
+def bond_vectors_108() -> np.ndarray:
+    """The 108 bond vectors of the standard BFM bond set: all permutations
+    and sign changes of (2,0,0), (2,1,0), (2,1,1), (3,0,0), (3,1,0), (2,2,1)."""
+    vecs = set()
+    for base in [(2, 0, 0), (2, 1, 0), (2, 1, 1), (3, 0, 0), (3, 1, 0), (2, 2, 1)]:
+        for perm in permutations(base):
+            for signs in product((1, -1), repeat=3):
+                vecs.add(tuple(int(p * s) for p, s in zip(perm, signs)))
+    out = np.array(sorted(vecs), dtype=np.int32)
+    assert out.shape == (108, 3)
+    return out
+
+
+def allowed_table(vectors: np.ndarray) -> np.ndarray:
+    """512-entry table, index (dx&7)|(dy&7)<<3|(dz&7)<<6 (the reference's
+    linearizeBondVectorIndex, UpdaterGPUScBFM_AB_Type.cu:871-889)."""
+    t = np.zeros(512, dtype=bool)
+    for dx, dy, dz in vectors:
+        t[(dx & 7) | ((dy & 7) << 3) | ((dz & 7) << 6)] = True
+    return t
+
+
+BONDS_108 = bond_vectors_108()
+ALLOWED_108 = allowed_table(BONDS_108)
+
+_CUBE = np.array([(a, b, c) for c in (0, 1) for b in (0, 1) for a in (0, 1)], dtype=np.int64)
+
+
+@dataclass
+class System:
+    box: tuple
+    pos: np.ndarray                  # (n,3) int32 absolute (unfolded) corner positions
+    deg: np.ndarray                  # (n,) uint8
+    nbr: np.ndarray                  # (n,8) uint32
+    allowed: np.ndarray = field(default_factory=lambda: ALLOWED_108.copy())
+    chains: list = field(default_factory=list)   # (first id, length) of linear chains
+    attributes: np.ndarray | None = None
+    name: str = ""
+
+    @property
+    def n(self) -> int:
+        return int(self.pos.shape[0])
+
+    def volume_fraction(self) -> float:
+        return 8.0 * self.n / float(np.prod(self.box))
+
+    def bonds(self):
+        """Undirected bond list (i < j)."""
+        out = []
+        for i in range(self.n):
+            for j in self.nbr[i, : self.deg[i]]:
+                if i < j:
+                    out.append((i, int(j)))
+        return out
+
+    def mean_degree(self) -> float:
+        return float(self.deg.mean()) if self.n else 0.0
+
+
+def _empty_topology(n):
+    return np.zeros(n, np.uint8), np.zeros((n, 8), np.uint32)
+
+
+def _connect(deg, nbr, i, j):
+    if deg[i] >= 8 or deg[j] >= 8:
+        raise ValueError("more than 8 bonds on a monomer")
+    nbr[i, deg[i]] = j
+    deg[i] += 1
+    nbr[j, deg[j]] = i
+    deg[j] += 1
+
+
+class _Occupancy:
+    """2x2x2 cube occupation on a periodic box, for growing walks."""
+
+    def __init__(self, box):
+        self.box = np.array(box, dtype=np.int64)
+        self.cells = np.zeros(tuple(box), dtype=bool)
+
+    def _idx(self, p):
+        c = (np.asarray(p, dtype=np.int64)[None, :] + _CUBE) % self.box
+        return c[:, 0], c[:, 1], c[:, 2]
+
+    def free(self, p) -> bool:
+        return not self.cells[self._idx(p)].any()
+
+    def set(self, p, v=True):
+        self.cells[self._idx(p)] = v
+
+
+def saw_chains(n_chains: int, chain_len: int, box=(128, 128, 128), seed: int = 12345, max_tries: int = 200,
+               alternate_ab: bool = True) -> System:
+    """Linear chains grown monomer by monomer as self-avoiding walks with
+    bonds drawn uniformly from the 108-vector set; a chain that gets stuck is
+    removed and regrown from a new random start."""
+    rng = np.random.default_rng(seed)
+    occ = _Occupancy(box)
+    n = n_chains * chain_len
+    pos = np.zeros((n, 3), np.int64)
+    deg, nbr = _empty_topology(n)
+    bvec = BONDS_108.astype(np.int64)
+    for c in range(n_chains):
+        first = c * chain_len
+        for _ in range(max_tries):
+            start = rng.integers(0, box, size=3)
+            if not occ.free(start):
+                continue
+            occ.set(start)
+            pos[first] = start
+            ok = True
+            for k in range(1, chain_len):
+                prev = pos[first + k - 1]
+                placed = False
+                for b in rng.permutation(108):
+                    cand = prev + bvec[b]
+                    if occ.free(cand):
+                        occ.set(cand)
+                        pos[first + k] = cand
+                        placed = True
+                        break
+                if not placed:
+                    for q in range(k):
+                        occ.set(pos[first + q], False)
+                    ok = False
+                    break
+            if ok:
+                break
+        else:
+            raise RuntimeError("could not place chain %d" % c)
+        for k in range(1, chain_len):
+            _connect(deg, nbr, first + k - 1, first + k)
+    attrs = None
+    if alternate_ab:
+        attrs = np.array([1 + (i // chain_len) % 2 for i in range(n)], dtype=np.int32)
+    return System(tuple(int(b) for b in box), pos.astype(np.int32), deg, nbr,
+                  chains=[(c * chain_len, chain_len) for c in range(n_chains)], attributes=attrs,
+                  name=f"saw_{n_chains}x{chain_len}_L{box[0]}")
+
+
+def ordered_melt(L: int = 256, chain_len: int | None = None) -> System:
+    """Volume fraction 0.5 on an L^3 box: monomers on the sites (2i, 2j, 4k),
+    chains run along x with (2,0,0) bonds and turn into the next row with a
+    (0,2,0) bond (a serpentine of chain_len / (L/2) rows).  For L = 256 and
+    chain_len = 256 this is 4096 chains x 256 = 1,048,576 monomers."""
+    per_row = L // 2
+    if chain_len is None:
+        chain_len = 2 * per_row
+    if chain_len % per_row:
+        raise ValueError("chain_len must be a multiple of L/2")
+    rows_per_chain = chain_len // per_row
+    rows_per_layer = L // 2
+    if rows_per_layer % rows_per_chain:
+        raise ValueError("L/2 rows per layer must be divisible by the rows per chain")
+    layers = L // 4
+    n_rows = rows_per_layer * layers
+    n_chains = n_rows // rows_per_chain
+    n = n_chains * chain_len
+    # row r -> (j, k); monomer index = chain*chain_len + local
+    chain = np.repeat(np.arange(n_chains), chain_len)
+    local = np.tile(np.arange(chain_len), n_chains)
+    row_in_chain = local // per_row
+    idx_in_row = local % per_row
+    row = chain * rows_per_chain + row_in_chain
+    j = row % rows_per_layer
+    k = row // rows_per_layer
+    x_idx = np.where(row_in_chain % 2 == 0, idx_in_row, per_row - 1 - idx_in_row)
+    pos = np.stack([2 * x_idx, 2 * j, 4 * k], axis=1).astype(np.int32)
+    deg = np.zeros(n, np.uint8)
+    nbr = np.zeros((n, 8), np.uint32)
+    ids = np.arange(n)
+    inner = local < chain_len - 1
+    a = ids[inner]
+    b = a + 1
+    # neighbour order: previous first, then next (the order LeMonADE lists a linear chain)
+    has_prev = local > 0
+    nbr[has_prev, 0] = (ids - 1)[has_prev]
+    deg[has_prev] = 1
+    nbr[a, deg[a]] = b
+    deg[a] += 1
+    return System((L, L, L), pos, deg, nbr, chains=[(c * chain_len, chain_len) for c in range(n_chains)],
+                  attributes=(1 + (chain % 2)).astype(np.int32), name=f"melt_{n_chains}x{chain_len}_L{L}")
+
+
+def star_comb(n_stars: int, arm_len: int = 64, side_every: int = 8, side_len: int = 16, box=(128, 128, 128),
+              seed: int = 7, max_tries: int = 200) -> System:
+    """3-arm stars (a core monomer plus three arms of arm_len) carrying a side
+    chain of side_len on every side_every-th backbone monomer, grown as
+    self-avoiding walks.  Attribute 1 (A) backbone, 2 (B) side chains."""
+    rng = np.random.default_rng(seed)
+    occ = _Occupancy(box)
+    bvec = BONDS_108.astype(np.int64)
+    pos_l, attr_l, bonds = [], [], []
+
+    def grow_from(parent_id, length, attr, placed):
+        ids = []
+        prev = parent_id
+        for _ in range(length):
+            for b in rng.permutation(108):
+                cand = pos_l[prev] + bvec[b]
+                if occ.free(cand):
+                    occ.set(cand)
+                    pos_l.append(cand)
+                    attr_l.append(attr)
+                    me = len(pos_l) - 1
+                    bonds.append((prev, me))
+                    placed.append(me)
+                    ids.append(me)
+                    prev = me
+                    break
+            else:
+                return None
+        return ids
+
+    for s in range(n_stars):
+        for _ in range(max_tries):
+            mark = (len(pos_l), len(bonds))
+            placed = []
+            core = rng.integers(0, box, size=3)
+            if not occ.free(core):
+                continue
+            occ.set(core)
+            pos_l.append(core)
+            attr_l.append(1)
+            placed.append(len(pos_l) - 1)
+            ok = True
+            core_id = len(pos_l) - 1
+            for _arm in range(3):
+                arm = grow_from(core_id, arm_len, 1, placed)
+                if arm is None:
+                    ok = False
+                    break
+                for q, mid in enumerate(arm):
+                    if (q + 1) % side_every == 0:
+                        if grow_from(mid, side_len, 2, placed) is None:
+                            ok = False
+                            break
+                if not ok:
+                    break
+            if ok:
+                break
+            for p in placed:
+                occ.set(pos_l[p], False)
+            del pos_l[mark[0]:]
+            del attr_l[mark[0]:]
+            del bonds[mark[1]:]
+        else:
+            raise RuntimeError("could not place star %d" % s)
+    n = len(pos_l)
+    deg, nbr = _empty_topology(n)
+    for a, b in bonds:
+        _connect(deg, nbr, a, b)
+    return System(tuple(int(b) for b in box), np.array(pos_l, dtype=np.int32), deg, nbr,
+                  attributes=np.array(attr_l, dtype=np.int32), name=f"starcomb_{n_stars}_L{box[0]}")
+
+
+def add_crosslinks(sys: System, n_links: int, seed: int = 3) -> System:
+    """Add up to n_links bonds between monomers that are not yet bonded but
+    whose separation is already a valid bond vector (this closes cycles, so
+    the colouring may need 3 or more colours)."""
+    rng = np.random.default_rng(seed)
+    pos = sys.pos.astype(np.int64)
+    box = np.array(sys.box)
+    wrapped = pos % box
+    lookup = {tuple(p): i for i, p in enumerate(wrapped)}
+    deg = sys.deg.copy()
+    nbr = sys.nbr.copy()
+    added = 0
+    for i in rng.permutation(sys.n):
+        if added >= n_links:
+            break
+        if deg[i] >= 8:
+            continue
+        for b in rng.permutation(108):
+            q = tuple((wrapped[i] + BONDS_108[b]) % box)
+            j = lookup.get(q)
+            if j is None or j == i or deg[j] >= 8 or j in set(nbr[i, : deg[i]].tolist()):
+                continue
+            d = pos[j] - pos[i]
+            d = (d + box // 2) % box - box // 2  # minimum image
+            if not sys.allowed[(d[0] & 7) | ((d[1] & 7) << 3) | ((d[2] & 7) << 6)]:
+                continue
+            if np.any(np.abs(d) > 3):
+                continue
+            # unfold j next to i so the stored bond is the short one
+            if not np.array_equal(pos[j] - pos[i], d):
+                continue
+            _connect(deg, nbr, int(i), int(j))
+            added += 1
+            break
+    return System(sys.box, sys.pos.copy(), deg, nbr, sys.allowed.copy(), list(sys.chains), sys.attributes,
+                  sys.name + f"_x{added}")
+
+
+def chain_observables(pos: np.ndarray, chains) -> tuple[float, float]:
+    """Mean squared end-to-end distance R_e^2 and radius of gyration R_g^2
+    over linear chains (first id, length) of unfolded positions."""
+    p = np.asarray(pos, dtype=np.float64)
+    re2, rg2 = [], []
+    for first, length in chains:
+        c = p[first:first + length]
+        re2.append(float(((c[-1] - c[0]) ** 2).sum()))
+        rg2.append(float(((c - c.mean(axis=0)) ** 2).sum(axis=1).mean()))
+    return float(np.mean(re2)), float(np.mean(rg2))

@@ -1,0 +1,273 @@
+"""Host-side mirror of the reference's ``UpdaterGPUScBFM_AB_Type<T>``.
+
+Same method names, argument meaning, dependency order and exception types as
+src/pscbfm/UpdaterGPUScBFM_AB_Type.h:453-514 of lgh0504/pscbfm, forwarding
+to the C ABI of ``libpscbfm_b200.so`` (include/pscbfm_b200.h).  The
+reference's ``std::invalid_argument`` becomes ``ValueError`` and its
+``std::runtime_error`` becomes ``RuntimeError``; CUDA failures, which the
+reference answers with ``exit()`` (cudacommon.hpp:36-51), raise
+:class:`CudaError`.
+
+The template parameter of the reference (the device coordinate type) has no
+counterpart: positions are always kept as 32-bit Z-order codes plus image
+counters on the device.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+
+import numpy as np
+
+from . import _native
+
+
+class CudaError(RuntimeError):
+    """A CUDA runtime call failed inside the library."""
+
+
+class DeviceTimeout(TimeoutError):
+    """A bounded device-side wait gave up."""
+
+
+class Rng(enum.IntEnum):
+    """``UpdaterGPUScBFM_AB_Type::Rng`` (UpdaterGPUScBFM_AB_Type.h:413-420)."""
+
+    IntHash = 1
+    Saru = 2
+    Philox = 3
+    Pcg = 4
+    Xorwow = 5
+
+
+def _raise(status: int, msg: str):
+    if status == _native.BFM_OK:
+        return
+    if status == _native.BFM_EINVAL:
+        raise ValueError(msg)
+    if status == _native.BFM_ECUDA:
+        raise CudaError(msg)
+    if status == _native.BFM_ETIMEOUT:
+        raise DeviceTimeout(msg)
+    raise RuntimeError(msg)
+
+
+class UpdaterGPUScBFM_AB_Type:
+    """One simulated BFM system on one GPU (see module docstring)."""
+
+    Rng = Rng
+
+    def __init__(self):
+        self._lib = _native.lib()
+        h = ctypes.c_void_p()
+        _raise(self._lib.bfm_create(ctypes.byref(h)), "bfm_create failed")
+        self._h = h
+        self._n = 0
+        self._steps_between_sortings = 5000
+
+    # ------------------------------------------------------------ plumbing
+    def _check(self, status: int):
+        if status != _native.BFM_OK:
+            msg = self._lib.bfm_last_error(self._h)
+            _raise(status, msg.decode() if msg else f"status {status}")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.bfm_destroy(h)
+            self._h = None
+
+    def destruct(self):
+        """Free every resource (``destruct``, UpdaterGPUScBFM_AB_Type.h:455)."""
+        self._check(self._lib.bfm_cleanup(self._h))
+
+    # ------------------------------------------------------------ setters
+    def setGpu(self, iGpuToUse: int):
+        self._check(self._lib.bfm_set_gpu(self._h, int(iGpuToUse)))
+
+    def copyBondSet(self, dx: int, dy: int, dz: int, bondForbidden: bool):
+        self._check(self._lib.bfm_copy_bond_set(self._h, int(dx), int(dy), int(dz), 1 if bondForbidden else 0))
+
+    def setNrOfAllMonomers(self, nAllMonomers: int):
+        self._check(self._lib.bfm_set_nr_of_all_monomers(self._h, int(nAllMonomers)))
+        self._n = int(nAllMonomers)
+
+    def setAttribute(self, i: int, attribute: int):
+        self._check(self._lib.bfm_set_attribute(self._h, int(i), int(attribute)))
+
+    def setMonomerCoordinates(self, i: int, x: int, y: int, z: int):
+        self._check(self._lib.bfm_set_monomer_coordinates(self._h, int(i), int(x), int(y), int(z)))
+
+    def setConnectivity(self, monoidx1: int, monoidx2: int):
+        self._check(self._lib.bfm_set_connectivity(self._h, int(monoidx1), int(monoidx2)))
+
+    def setLatticeSize(self, boxX: int, boxY: int, boxZ: int):
+        self._check(self._lib.bfm_set_lattice_size(self._h, int(boxX), int(boxY), int(boxZ)))
+
+    def setPeriodicity(self, isPeriodicX: bool, isPeriodicY: bool, isPeriodicZ: bool):
+        self._check(self._lib.bfm_set_periodicity(self._h, int(bool(isPeriodicX)), int(bool(isPeriodicY)), int(bool(isPeriodicZ))))
+
+    def setAge(self, rAge: int):
+        self._check(self._lib.bfm_set_age(self._h, int(rAge)))
+
+    def getAge(self) -> int:
+        v = ctypes.c_int64()
+        self._check(self._lib.bfm_get_age(self._h, ctypes.byref(v)))
+        return v.value
+
+    def setRng(self, x):
+        self._check(self._lib.bfm_set_rng(self._h, int(x)))
+
+    def getRng(self) -> Rng:
+        v = ctypes.c_int()
+        self._check(self._lib.bfm_get_rng(self._h, ctypes.byref(v)))
+        return Rng(v.value)
+
+    def setStepsBetweenSortings(self, rnStepsBetweenSortings: int):
+        self._check(self._lib.bfm_set_steps_between_sortings(self._h, int(rnStepsBetweenSortings)))
+        self._steps_between_sortings = int(rnStepsBetweenSortings)
+
+    def getStepsBetweenSortings(self) -> int:
+        return self._steps_between_sortings
+
+    # ------------------------------------------------------------ life cycle
+    def initialize(self):
+        self._check(self._lib.bfm_initialize(self._h))
+
+    def execute(self) -> bool:
+        return True
+
+    def runSimulationOnGPU(self, nrMCS_per_Call: int):
+        self._check(self._lib.bfm_run(self._h, int(nrMCS_per_Call)))
+
+    def cleanup(self):
+        self._check(self._lib.bfm_cleanup(self._h))
+        self._n = 0
+
+    # ------------------------------------------------------------ getters
+    def _pos(self, i: int):
+        x, y, z = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        self._check(self._lib.bfm_get_monomer_position(self._h, int(i), ctypes.byref(x), ctypes.byref(y), ctypes.byref(z)))
+        return x.value, y.value, z.value
+
+    def getMonomerPositionInX(self, i: int) -> int:
+        return self._pos(i)[0]
+
+    def getMonomerPositionInY(self, i: int) -> int:
+        return self._pos(i)[1]
+
+    def getMonomerPositionInZ(self, i: int) -> int:
+        return self._pos(i)[2]
+
+    # ------------------------------------------------------------ bulk API
+    def setAllMonomerCoordinates(self, xyz):
+        a = np.ascontiguousarray(xyz, dtype=np.int32).reshape(-1, 3)
+        self._check(self._lib.bfm_set_all_coordinates(self._h, a.ctypes.data, a.shape[0]))
+
+    def setAllConnectivity(self, deg, nbr8):
+        d = np.ascontiguousarray(deg, dtype=np.uint8)
+        b = np.ascontiguousarray(nbr8, dtype=np.uint32).reshape(-1, 8)
+        self._check(self._lib.bfm_set_all_connectivity(self._h, d.ctypes.data, b.ctypes.data, d.shape[0]))
+
+    def setBondSet(self, allowed512):
+        """allowed512[(dx&7)|(dy&7)<<3|(dz&7)<<6] for dx,dy,dz in [-4,3], the
+        loop of the LeMonADE adapter (GPUScBFM_AB_Type.h:168-175)."""
+        allowed = np.asarray(allowed512, dtype=bool)
+        for dx in range(-4, 4):
+            for dy in range(-4, 4):
+                for dz in range(-4, 4):
+                    self.copyBondSet(dx, dy, dz, not allowed[(dx & 7) | ((dy & 7) << 3) | ((dz & 7) << 6)])
+
+    def getAllMonomerPositions(self) -> np.ndarray:
+        out = np.empty((self._n, 3), dtype=np.int32)
+        self._check(self._lib.bfm_get_positions(self._h, out.ctypes.data, self._n))
+        return out
+
+    def getLattice(self) -> np.ndarray:
+        nw = ctypes.c_size_t()
+        self._check(self._lib.bfm_get_lattice_words(self._h, ctypes.byref(nw)))
+        out = np.empty(nw.value, dtype=np.uint32)
+        self._check(self._lib.bfm_get_lattice(self._h, out.ctypes.data, nw.value))
+        return out
+
+    def getNSpecies(self) -> int:
+        v = ctypes.c_uint32()
+        self._check(self._lib.bfm_get_nspecies(self._h, ctypes.byref(v)))
+        return v.value
+
+    def getColors(self) -> np.ndarray:
+        out = np.empty(self._n, dtype=np.uint32)
+        self._check(self._lib.bfm_get_colors(self._h, out.ctypes.data, self._n))
+        return out
+
+    def getSpeciesOrder(self, sp: int) -> np.ndarray:
+        cnt = ctypes.c_size_t()
+        self._check(self._lib.bfm_get_species_order(self._h, int(sp), None, 0, ctypes.byref(cnt)))
+        out = np.empty(cnt.value, dtype=np.uint32)
+        self._check(self._lib.bfm_get_species_order(self._h, int(sp), out.ctypes.data, cnt.value, ctypes.byref(cnt)))
+        return out
+
+    def getCounters(self):
+        """(attempted moves, candidates after the check phase, accepted moves)."""
+        out = np.zeros(3, dtype=np.uint64)
+        self._check(self._lib.bfm_get_counters(self._h, out.ctypes.data))
+        return int(out[0]), int(out[1]), int(out[2])
+
+    def getLastRunMs(self) -> float:
+        v = ctypes.c_double()
+        self._check(self._lib.bfm_get_last_run_ms(self._h, ctypes.byref(v)))
+        return v.value
+
+    def getLastRunLaunches(self) -> int:
+        v = ctypes.c_uint64()
+        self._check(self._lib.bfm_get_last_run_launches(self._h, ctypes.byref(v)))
+        return v.value
+
+    def setLaunchMode(self, mode: int):
+        self._check(self._lib.bfm_set_launch_mode(self._h, int(mode)))
+
+    # ------------------------------------------------------------ convenience
+    def setup(self, system, *, gpu: int = 0, rng=Rng.Saru, age: int = 0, steps_between_sortings: int = 5000):
+        """All setters of the LeMonADE adapter (GPUScBFM_AB_Type.h:121-184) for
+        a :class:`pscbfm_b200.systems.System`, then ``initialize``."""
+        self.setGpu(gpu)
+        self.setRng(rng)
+        self.setAge(age)
+        self.setStepsBetweenSortings(steps_between_sortings)
+        self.setPeriodicity(True, True, True)
+        self.setLatticeSize(*system.box)
+        self.setNrOfAllMonomers(system.n)
+        self.setAllMonomerCoordinates(system.pos)
+        self.setAllConnectivity(system.deg, system.nbr)
+        self.setBondSet(system.allowed)
+        self.initialize()
+        return self
+
+
+# process-global R250 colour/seed generator (LeMonADE's RandomNumberGenerators)
+def r250_seed(seed: int):
+    _native.lib().bfm_r250_seed(int(seed))
+
+
+def r250_seed_words(words):
+    w = np.ascontiguousarray(words, dtype=np.uint32)
+    if w.size < 250:
+        raise ValueError("R250 needs at least 250 seed words")
+    _native.lib().bfm_r250_seed_words(w.ctypes.data, w.size)
+
+
+def r250_get_state() -> np.ndarray:
+    out = np.zeros(251, dtype=np.uint32)
+    _native.lib().bfm_r250_get_state(out.ctypes.data)
+    return out
+
+
+def r250_set_state(state):
+    s = np.ascontiguousarray(state, dtype=np.uint32)
+    if s.size != 251 or s[250] >= 250:
+        raise ValueError("R250 state must be 250 words + an index below 250")
+    _native.lib().bfm_r250_set_state(s.ctypes.data)
+
+
+def r250_rand32() -> int:
+    return int(_native.lib().bfm_r250_rand32())

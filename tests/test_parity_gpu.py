@@ -1,0 +1,135 @@
+"""GPU parity: the CUDA sweep (through the C ABI) against the CPU oracle and
+against the reference's own updater built for sm_100a, bit for bit on final
+positions and on the occupation lattice."""
+import numpy as np
+import pytest
+
+import pscbfm_b200 as pb
+from oracle import oracle
+from pscbfm_b200 import systems
+
+pytestmark = pytest.mark.gpu
+
+
+def _systems():
+    return {
+        "dilute_chains": systems.saw_chains(40, 24, box=(64, 64, 64), seed=21),
+        "dense_chains": systems.saw_chains(60, 32, box=(32, 32, 32), seed=22),
+        "star_comb": systems.star_comb(6, arm_len=20, side_every=5, side_len=4, box=(32, 32, 32), seed=23),
+        "crosslinked": systems.add_crosslinks(systems.saw_chains(40, 20, box=(32, 32, 32), seed=24), 60, seed=2),
+        "melt_L32": systems.ordered_melt(32),
+        "lone_monomers": systems.saw_chains(50, 1, box=(16, 16, 16), seed=25),
+    }
+
+
+SYSTEMS = _systems()
+
+
+def run_pair(s, rng, age, sort_every, calls, r250_seed=1234, mode=0):
+    pb.r250_seed(r250_seed)
+    st = pb.r250_get_state()
+    u = pb.UpdaterGPUScBFM_AB_Type()
+    u.setLaunchMode(mode)
+    u.setup(s, gpu=0, rng=rng, age=age, steps_between_sortings=sort_every)
+    o = oracle.Sweep(s, rng=int(rng), age=age, sort_every=sort_every, threads=4)
+    for nmcs in calls:
+        u.runSimulationOnGPU(nmcs)
+        o.run(nmcs, st)
+        got, want = u.getAllMonomerPositions(), o.positions()
+        assert np.array_equal(got, want), f"{int((got != want).any(axis=1).sum())} monomers differ after {nmcs} MCS"
+        assert np.array_equal(u.getLattice(), oracle.lattice_words(got, s.box))
+    assert np.array_equal(pb.r250_get_state(), st)
+    assert u.getAge() == o.age()
+    return u, o
+
+
+@pytest.mark.parametrize("name", list(SYSTEMS))
+@pytest.mark.parametrize("rng", [pb.Rng.Saru, pb.Rng.IntHash])
+def test_sweep_matches_oracle(name, rng):
+    s = SYSTEMS[name]
+    u, o = run_pair(s, rng, age=0, sort_every=13, calls=[1, 30, 17])
+    assert np.array_equal(u.getColors(), o.colors())
+    for sp in range(u.getNSpecies()):
+        assert np.array_equal(u.getSpeciesOrder(sp), o.slab(sp))
+    att, cand, acc = u.getCounters()
+    oatt, ocand, oacc = o.stats()
+    assert (att, cand, acc) == (oatt, ocand, oacc)
+
+
+@pytest.mark.parametrize("age,sort_every", [(4999, 5000), (12345, 7), (3, 1), (0, 5000)])
+def test_age_and_sorting_cadence(age, sort_every):
+    run_pair(SYSTEMS["dense_chains"], pb.Rng.Saru, age=age, sort_every=sort_every, calls=[9, 1, 25])
+
+
+def test_launch_modes_agree():
+    s = SYSTEMS["crosslinked"]
+    a, _ = run_pair(s, pb.Rng.Saru, 0, 50, [200], mode=0)
+    b, _ = run_pair(s, pb.Rng.Saru, 0, 50, [200], mode=1)
+    assert np.array_equal(a.getAllMonomerPositions(), b.getAllMonomerPositions())
+
+
+def test_three_colours_present():
+    u, _ = run_pair(SYSTEMS["crosslinked"], pb.Rng.Saru, 0, 5000, [3])
+    assert u.getNSpecies() >= 3
+
+
+def test_wrapping_and_image_counters():
+    """Long dilute run: monomers cross the periodic box many times; the
+    unfolded positions still match the oracle."""
+    s = systems.saw_chains(8, 4, box=(8, 8, 8), seed=5)
+    u, o = run_pair(s, pb.Rng.Saru, 0, 100, [500, 500])
+    pos = u.getAllMonomerPositions()
+    assert (np.abs(pos) >= 8).any()
+
+
+REF_CASES = [
+    ("dilute_chains", 0), ("dense_chains", 0), ("crosslinked", 0), ("melt_L32", 0), ("star_comb", 1),
+    ("dense_chains", 1),
+]
+
+
+@pytest.mark.parametrize("name,ctype", REF_CASES)
+@pytest.mark.parametrize("rng", [pb.Rng.Saru, pb.Rng.IntHash])
+def test_sweep_matches_reference_build(name, ctype, rng):
+    """The reference's own UpdaterGPUScBFM_AB_Type<T> (oracle/_ref), driven
+    with the same R250 stream: positions after each call must be identical
+    to the product's and to the oracle's."""
+    if oracle.ref_gpu() is None:
+        pytest.skip("oracle/_ref/libref_pscbfm.so not built")
+    s = SYSTEMS[name]
+    pb.r250_seed(77)
+    st_ref = pb.r250_get_state()
+    u, o = run_pair(s, rng, age=0, sort_every=11, calls=[5, 20], r250_seed=77)
+    ref = oracle.RefUpdater(s, rng=int(rng), age=0, sort_every=11, ctype=ctype)
+    ref.run(5, st_ref)
+    ref.run(20, st_ref)
+    assert np.array_equal(ref.positions(), o.positions())
+    assert np.array_equal(ref.positions(), u.getAllMonomerPositions())
+
+
+def test_full_size_melt_properties():
+    """The 256^3 melt (1,048,576 monomers): size-independent properties after
+    a short run -- lattice equals the positions' lattice, bonds stay in the
+    set, no two corners coincide, a second identical run is identical."""
+    s = systems.ordered_melt(256)
+    outs = []
+    for _ in range(2):
+        pb.r250_seed(9)
+        u = pb.UpdaterGPUScBFM_AB_Type().setup(s, rng=pb.Rng.Saru)
+        u.runSimulationOnGPU(200)
+        pos = u.getAllMonomerPositions()
+        outs.append(pos)
+        assert np.array_equal(u.getLattice(), oracle.lattice_words(pos, s.box))
+        att, cand, acc = u.getCounters()
+        assert att == 200 * s.n and acc > 0
+    assert np.array_equal(outs[0], outs[1])
+    pos = outs[0].astype(np.int64)
+    ids = np.arange(s.n)
+    for j in range(2):
+        has = s.deg > j
+        d = pos[s.nbr[has, j]] - pos[ids[has]]
+        assert np.all(np.abs(d) <= 3)
+        assert s.allowed[(d[:, 0] & 7) | ((d[:, 1] & 7) << 3) | ((d[:, 2] & 7) << 6)].all()
+    w = pos % 256
+    codes = w[:, 0] * 65536 + w[:, 1] * 256 + w[:, 2]
+    assert np.unique(codes).size == s.n
