@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""Throughput of the colored BFM sweep: attempted moves per second on one B200.
+
+Workload: dense linear melt, 4096 chains x N=256 (1,048,576 monomers) on a
+256^3 periodic lattice, volume fraction 0.5, standard 108-vector bond set,
+two colours (bipartite chains), Saru RNG.  The start is a serpentine crystal
+melted by the sweep itself before warm-up.  A "step" is --mcs-per-step
+Monte-Carlo steps (default 1000; 100 steps = the 100,000 MCS run).
+
+  value  attempted moves/s from CUDA events around each step's kernels on the
+         library stream, state resident in HBM (L2 flushed before each step)
+  e2e    the same through the public C ABI with host buffers: each step is
+         runSimulationOnGPU (host-drawn colour/seed schedule copied H2D from
+         pinned memory) plus the read-back of all positions (D2H)
+
+Multi-GPU (torchrun): independent replicas, one system per rank, no
+collective on the data path ("weak" scaling); times are the max over ranks.
+
+--impl reference runs the reference's own UpdaterGPUScBFM_AB_Type (built for
+sm_100a from its sources into oracle/_ref/) on the same workload through its
+own API; without that library it times the CPU oracle port on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+import numpy as np  # noqa: E402
+
+WORKLOAD = ("dense linear melt: 4096 chains x N=256 (1,048,576 monomers), 256^3 periodic lattice, "
+            "volume fraction 0.5, 108-vector bond set, 2 colours, Saru RNG")
+METRIC = "attempted moves/s on 1 B200; batched+surrogate vs plain at equal R_e² error"
+UNIT = "attempted moves/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--mcs-per-step", type=int, default=1000)
+    p.add_argument("--melt-mcs", type=int, default=2000)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    return p.parse_args()
+
+
+# ------------------------------------------------------------------ ranks
+class Ranks:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        hi = max(sm)
+        loaded = [v for v in sm if v >= 0.5 * hi] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def flush_l2(buf):
+    """Write a buffer larger than the 126 MB L2 (torch, current stream)."""
+    import torch
+    buf.zero_()
+    torch.cuda.synchronize()
+
+
+def peaks():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------- workload
+def make_workload():
+    from pscbfm_b200 import systems
+    return systems.ordered_melt(256)
+
+
+def algorithmic_bytes(c: float, a: float, kbar: float, C: int = 4):
+    """Bytes per attempted move of the check and perform kernels: own
+    coordinate C, bond count 1, per bond a 4-byte id and an 8-byte coordinate
+    gather, nine 4-byte lattice probes, the target bit for candidates (c);
+    perform: nine probes of the target lattice for candidates, coordinate
+    write and two lattice bit updates for accepted moves (a)."""
+    check = C + 1 + 12 * kbar + 36 + 4 * c
+    perform = 36 * c + C * a + 8 * a
+    return check, perform
+
+
+def cpu_baseline(system, pos_now, seconds: float):
+    """The oracle (CPU restatement of the colored sweep, OpenMP over the
+    monomers of a colour) on a bounded sample: as many MCS of the same melt
+    as fit in about `seconds` of host time, on all host cores; plus the
+    serial random-sequential BFM on one core."""
+    from oracle import oracle
+    from pscbfm_b200.systems import System
+    s = System(system.box, pos_now.copy(), system.deg, system.nbr, system.allowed, system.chains)
+    cores = os.cpu_count() or 1
+    sw = oracle.Sweep(s, rng=2, age=0, sort_every=5000, threads=cores)
+    st = oracle.r250_state(5)
+    t = time.perf_counter()
+    sw.run(1, st)
+    one = max(time.perf_counter() - t, 1e-3)
+    m = max(1, min(200, int(seconds / one)))
+    t = time.perf_counter()
+    sw.run(m, st)
+    dt = time.perf_counter() - t
+    colored = s.n * m / dt
+    pos = pos_now.copy()
+    t = time.perf_counter()
+    oracle.serial_run(s, pos, 1, seed=3)
+    dts = time.perf_counter() - t
+    serial = s.n / dts
+    return {"value": colored, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{m} MCS of the same 256^3 melt ({s.n * m:.3g} attempted moves), colored two-phase "
+                      f"algorithm, OpenMP over the monomers of a colour",
+            "serial_1core": {"value": serial, "unit": UNIT, "cores": 1,
+                             "sample": "1 MCS random-sequential Metropolis BFM on the same melt"}}
+
+
+# ------------------------------------------------------------------- arms
+def run_b200(args, ranks):
+    import torch
+
+    import pscbfm_b200 as pb
+    gpu = ranks.local
+    torch.cuda.set_device(gpu)
+    system = make_workload()
+    pb.r250_seed(1000 + ranks.rank)
+    u = pb.UpdaterGPUScBFM_AB_Type().setup(system, gpu=gpu, rng=pb.Rng.Saru)
+    S = args.mcs_per_step
+    u.runSimulationOnGPU(args.melt_mcs)        # melt the serpentine crystal (untimed)
+    flushbuf = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{gpu}")
+    for _ in range(args.warmup):
+        flush_l2(flushbuf)
+        u.runSimulationOnGPU(S)
+        u.getAllMonomerPositions()
+
+    # live per-kernel timing for the roofline (same kernels, direct launches)
+    a0, c0, s0 = u.getCounters()
+    kmcs = min(S, 200)
+    ms_check, ms_perf, nl = u.timeKernels(kmcs)
+    a1, c1, s1 = u.getCounters()
+    cand = (c1 - c0) / max(a1 - a0, 1)
+    acc = (s1 - s0) / max(a1 - a0, 1)
+
+    clocks = Clocks(gpu)
+    torch.cuda.synchronize()
+    ranks.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_begin = time.perf_counter()
+    dev_ms, e2e_s, launches = 0.0, 0.0, 0
+    step_ms = []
+    acnt0 = u.getCounters()
+    for _ in range(args.steps):
+        flush_l2(flushbuf)
+        t0 = time.perf_counter()
+        u.runSimulationOnGPU(S)
+        pos = u.getAllMonomerPositions()
+        e2e_s += time.perf_counter() - t0
+        ms = u.getLastRunMs()
+        dev_ms += ms
+        step_ms.append(ms)
+        launches += u.getLastRunLaunches() + 1    # + the read-back unpack kernel
+    torch.cuda.synchronize()
+    ranks.barrier()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t_begin
+    clk = clocks.stop()
+    acnt1 = u.getCounters()
+
+    attempts = acnt1[0] - acnt0[0]
+    dev_s = ranks.max(dev_ms / 1e3)
+    e2e_s = ranks.max(e2e_s)
+    total_attempts = attempts * ranks.world
+    value = total_attempts / dev_s
+    e2e = total_attempts / e2e_s
+
+    kbar = float(system.deg.mean())
+    b_check, b_perf = algorithmic_bytes(cand, acc, kbar)
+    nspec = u.getNSpecies()
+    per_launch_attempts = system.n / nspec
+    t_check = ms_check / max(nl, 1) / 1e3
+    t_perf = ms_perf / max(nl, 1) / 1e3
+    hbm, hbm_kind = peaks()
+    dominant = "k_check" if t_check >= t_perf else "k_perform"
+    bytes_dom = (b_check if dominant == "k_check" else b_perf) * per_launch_attempts
+    t_dom = t_check if dominant == "k_check" else t_perf
+    achieved = bytes_dom / t_dom / 1e9
+    traffic = None
+    prof = os.path.join(HERE, "profiles", "k_check_melt256_traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    whole_bytes = (b_check + b_perf) * total_attempts / ranks.world
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": ranks.world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": dev_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u32",
+        "data": "synthetic (seeded serpentine melt of the stated shape, melted in place before warm-up)",
+        "config": {"workload": WORKLOAD, "mcs_per_step": S, "monomers": system.n, "box": list(system.box),
+                   "colours": nspec, "replicas": ranks.world,
+                   "l2": "flushed before every step (256 MiB write); the 19 MiB state is L2-resident within a step",
+                   "launch": "one check + one perform kernel per colour substep, CUDA graphs of 64 substeps"},
+        "e2e": {"value": e2e, "unit": UNIT,
+                "h2d_bytes_per_step": S * nspec * 16,
+                "d2h_bytes_per_step": system.n * 12},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": traffic, "kernel": dominant, "peak_source": f"{hbm_kind} hbm_gbs",
+                     "bytes_per_attempt": {"k_check": b_check, "k_perform": b_perf},
+                     "attempts_per_launch": per_launch_attempts,
+                     "launch_ms": {"k_check": t_check * 1e3, "k_perform": t_perf * 1e3},
+                     "candidate_fraction": cand, "accept_fraction": acc,
+                     "whole_step_gbs": whole_bytes / (dev_ms / 1e3) / 1e9},
+        "clocks": clk,
+        "wall_s": wall,
+    }
+    if ranks.rank == 0 and ranks.world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(system, pos, args.cpu_seconds)
+    if ranks.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_reference(args, ranks):
+    if ranks.rank != 0:
+        return
+    from oracle import oracle
+    system = make_workload()
+    S = args.mcs_per_step
+    if oracle.ref_gpu() is not None:
+        import torch
+        ref = oracle.RefUpdater(system, rng=2, age=0, sort_every=5000, ctype=1, gpu=ranks.local)
+        st = oracle.r250_state(7)
+        ref.run(args.melt_mcs, st)
+        flushbuf = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{ranks.local}")
+        for _ in range(args.warmup):
+            flush_l2(flushbuf)
+            ref.run(S, st)
+            ref.positions()
+        clocks = Clocks(ranks.local)
+        torch.cuda.synchronize()
+        clocks.start()
+        tot = 0.0
+        for _ in range(args.steps):
+            flush_l2(flushbuf)
+            t0 = time.perf_counter()
+            ref.run(S, st)            # synchronous, ends with its own copy-back
+            ref.positions()
+            tot += time.perf_counter() - t0
+        clk = clocks.stop()
+        value = system.n * S * args.steps / tot
+        desc = {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": f"{args.steps} x {S} MCS of the same melt through the reference's "
+                          f"UpdaterGPUScBFM_AB_Type<uint8_t> (its own CUDA kernels, built for sm_100a), "
+                          f"one host thread driving the B200"}
+    else:
+        clk = None
+        c = cpu_baseline(system, system.pos, args.cpu_seconds)
+        value = c["value"]
+        desc = {k: c[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        tot = None
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": (tot / args.steps * 1e3) if tot else None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "mcs_per_step": S},
+            "cpu_baseline": desc,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ranks = Ranks()
+    try:
+        if args.impl == "reference":
+            run_reference(args, ranks)
+        else:
+            run_b200(args, ranks)
+    finally:
+        ranks.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -105,6 +105,11 @@ int bfm_get_counters(bfm_handle *h, uint64_t out3[3]);
 int bfm_get_last_run_ms(const bfm_handle *h, double *ms);
 /* kernel launches issued by the last bfm_run */
 int bfm_get_last_run_launches(const bfm_handle *h, uint64_t *launches);
+/* runs nmcs Monte-Carlo steps like bfm_run (same trajectory) with every kernel
+ * launched directly and bracketed by CUDA events on the handle's stream;
+ * returns the summed device time of the check and of the perform kernels and
+ * the number of launches of each */
+int bfm_time_kernels(bfm_handle *h, uint32_t nmcs, double *ms_check, double *ms_perform, uint64_t *launches_each);
 /* launch path: 0 = one check + one perform kernel per colour substep, captured
  * in CUDA graphs; 1 = same kernels launched one by one */
 int bfm_set_launch_mode(bfm_handle *h, int mode);

@@ -46,9 +46,14 @@ RefBase *make(int gpu, uint32_t Lx, uint32_t Ly, uint32_t Lz, uint32_t n, const 
               const uint32_t *nnbr, const uint32_t *nbr8, const uint8_t *allowed512, int rng, int64_t age,
               int64_t sortEvery)
 {
+    /* The adapter calls setGpu() first (GPUScBFM_AB_Type.h:131).  On this GPU
+     * it throws: setGpu prints the device table, and getCudaCodeName
+     * (cudacommon.hpp:1032-1043) returns 0 into a std::string for every
+     * compute capability above 7.  The device is therefore selected with
+     * cudaSetDevice; initialize() queries it itself (.cu:2535-2536). */
+    if (cudaSetDevice(gpu) != cudaSuccess) throw std::runtime_error("cudaSetDevice failed");
     auto *r = new Ref<T>();
     auto &u = r->u;
-    u.setGpu(gpu);
     u.setRng((typename UpdaterGPUScBFM_AB_Type<T>::Rng)rng);
     u.setAge(age);
     u.setStepsBetweenSortings(sortEvery);

@@ -93,6 +93,7 @@ _SIGS = {
     "bfm_get_last_run_ms": (_c.c_int, [_P, _c.POINTER(_c.c_double)]),
     "bfm_get_last_run_launches": (_c.c_int, [_P, _c.POINTER(_c.c_uint64)]),
     "bfm_set_launch_mode": (_c.c_int, [_P, _c.c_int]),
+    "bfm_time_kernels": (_c.c_int, [_P, _c.c_uint32, _c.POINTER(_c.c_double), _c.POINTER(_c.c_double), _c.POINTER(_c.c_uint64)]),
     "bfm_color_graph": (_c.c_int, [_c.c_uint32, _P, _P, _c.c_int, _P, _P]),
     "bfm_r250_seed": (_c.c_int, [_c.c_uint64]),
     "bfm_r250_seed_words": (_c.c_int, [_P, _c.c_size_t]),

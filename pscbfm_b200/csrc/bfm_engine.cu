@@ -375,6 +375,8 @@ struct Engine {
         }
         if (h_out) cudaFreeHost(h_out);
         h_out = nullptr;
+        for (auto e : profEvents) cudaEventDestroy(e);
+        profEvents.clear();
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         ev0 = ev1 = nullptr;
@@ -611,14 +613,67 @@ struct Engine {
     }
     int performBlocks() const { return (int)std::max<uint32_t>(1, std::min<uint32_t>((nmax + kThreads - 1) / kThreads, 148u * 64u)); }
 
+    /* per-kernel event pairs when profiling (direct launches only) */
+    bool profiling = false;
+    std::vector<cudaEvent_t> profEvents;
+    size_t profUsed = 0;
+    cudaEvent_t profEvent()
+    {
+        if (profUsed == profEvents.size()) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            profEvents.push_back(e);
+        }
+        return profEvents[profUsed++];
+    }
+
     void launchSubstep(const Substep *sched, uint32_t k)
     {
         const Sys s = sys();
+        cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
+        if (profiling) {
+            e0 = profEvent();
+            e1 = profEvent();
+            e2 = profEvent();
+            CK(cudaEventRecord(e0, stream));
+        }
         if (rng == BFM_RNG_SARU)
             k_check<RNG_SARU><<<checkBlocks(), kThreads, 0, stream>>>(s, sched, k);
         else
             k_check<RNG_INTHASH><<<checkBlocks(), kThreads, 0, stream>>>(s, sched, k);
+        if (profiling) CK(cudaEventRecord(e1, stream));
         k_perform<<<performBlocks(), kThreads, 0, stream>>>(s, sched, k);
+        if (profiling) CK(cudaEventRecord(e2, stream));
+    }
+
+    /* run nMCS with every kernel bracketed by CUDA events on the launching
+     * stream; returns the summed durations of the check and perform kernels */
+    void timeKernels(uint32_t nMCS, double *msCheck, double *msPerform, uint64_t *launchesEach)
+    {
+        const int saved = launchMode;
+        launchMode = 1;
+        profiling = true;
+        profUsed = 0;
+        try {
+            run(nMCS);
+        } catch (...) {
+            profiling = false;
+            launchMode = saved;
+            throw;
+        }
+        profiling = false;
+        launchMode = saved;
+        double c = 0, p = 0;
+        for (size_t i = 0; i + 2 < profUsed; i += 3) {
+            float a = 0, b = 0;
+            CK(cudaEventElapsedTime(&a, profEvents[i], profEvents[i + 1]));
+            CK(cudaEventElapsedTime(&b, profEvents[i + 1], profEvents[i + 2]));
+            c += a;
+            p += b;
+        }
+        *msCheck = c;
+        *msPerform = p;
+        *launchesEach = profUsed / 3;
     }
 
     /* substeps per captured graph: a whole number of MCS */
@@ -1034,6 +1089,15 @@ int bfm_get_last_run_launches(const bfm_handle *h, uint64_t *launches)
     if (!h || !launches) return BFM_EINVAL;
     *launches = h->e.lastLaunches;
     return BFM_OK;
+}
+
+int bfm_time_kernels(bfm_handle *h, uint32_t nmcs, double *ms_check, double *ms_perform, uint64_t *launches_each)
+{
+    if (h && !h->e.initialized) return BFM_ENOTINIT;
+    GUARD(h, {
+        if (!ms_check || !ms_perform || !launches_each) throw InvalidArgument("null output pointer");
+        h->e.timeKernels(nmcs, ms_check, ms_perform, launches_each);
+    });
 }
 
 int bfm_set_launch_mode(bfm_handle *h, int mode)

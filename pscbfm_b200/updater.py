@@ -223,6 +223,13 @@ class UpdaterGPUScBFM_AB_Type:
         self._check(self._lib.bfm_get_last_run_launches(self._h, ctypes.byref(v)))
         return v.value
 
+    def timeKernels(self, nmcs: int):
+        """Run nmcs MCS with per-kernel CUDA events; returns (check ms, perform
+        ms, launches of each) summed over the run."""
+        c, p, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_uint64()
+        self._check(self._lib.bfm_time_kernels(self._h, int(nmcs), ctypes.byref(c), ctypes.byref(p), ctypes.byref(n)))
+        return c.value, p.value, n.value
+
     def setLaunchMode(self, mode: int):
         self._check(self._lib.bfm_set_launch_mode(self._h, int(mode)))
 
