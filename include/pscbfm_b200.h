@@ -33,7 +33,8 @@ enum {
     BFM_ECUDA = 3,       /* a CUDA call failed (the reference exit()s, cudacommon.hpp:36-51) */
     BFM_ETIMEOUT = 4,    /* a bounded device-side wait gave up */
     BFM_ENOTINIT = 5,    /* call needs bfm_initialize first */
-    BFM_EUNSUPPORTED = 6 /* feature not provided by this build */
+    BFM_EUNSUPPORTED = 6, /* feature not provided by this build */
+    BFM_ETOOLARGE = 7     /* size beyond the fixed maximum of bfm_substep_noalloc */
 };
 
 /* random number generators, numbering of the reference's enum class Rng
@@ -120,6 +121,32 @@ int bfm_set_launch_mode(bfm_handle *h, int mode);
  * colors[n] receives the colours, *ncolors their number. */
 int bfm_color_graph(uint32_t n, const uint8_t *deg, const uint32_t *nbr8, int uniform, uint32_t *colors,
                     uint32_t *ncolors);
+
+/* One colour substep (check + perform) on device arrays the caller owns,
+ * without allocating any device memory.  No counterpart in the reference:
+ * it is for callers that cannot call cudaMalloc while they step a system --
+ * e.g. a host simulation that hands the library slices of one device pool
+ * it manages itself, or runs under a fixed device-memory budget, where the
+ * allocation calls (which may also synchronize the device) are not allowed.
+ * The library's own scratch for this call (target bit lattice and
+ * check/perform flags) is a fixed 512 KiB static device array, held by every
+ * GPU that loads the library until the process exits.
+ *   pos       device, npad Z-order codes (bit 3k: x_k, 3k+1: y_k, 3k+2: z_k)
+ *   img       device int32[3][npad] image counters, or NULL
+ *   nbr, deg  device neighbour slot ids (row j at nbr + j*npad) and counts
+ *   lattice   device occupation bits, Z-order, 32-bit words, max(L)^3/32 words
+ *   allowed512 host table, index (dx&7)|(dy&7)<<3|(dz&7)<<6, 108 entries set
+ *   slot_offset, count: the colour's slab; local index = RNG subsequence
+ *   seed, iteration, rng: as drawn per substep by runSimulationOnGPU
+ *   stream    cudaStream_t to enqueue on (asynchronous; NULL = legacy stream)
+ * Limits: max(L)^3 <= 128^3 sites and count <= 262144, else BFM_ETOOLARGE.
+ * The first call on a device looks up the scratch array's address (one
+ * cudaGetSymbolAddress, no allocation); make that first call before any
+ * stream capture.  All calls share the one scratch array, so calls that
+ * overlap on the GPU (concurrent streams, several host threads) race. */
+int bfm_substep_noalloc(uint32_t *pos, int32_t *img, const uint32_t *nbr, const uint8_t *deg, uint32_t npad,
+                        uint32_t *lattice, uint32_t box_x, uint32_t box_y, uint32_t box_z, const uint8_t *allowed512,
+                        uint32_t slot_offset, uint32_t count, uint32_t seed, uint32_t iteration, int rng, void *stream);
 
 /* Process-global R250 colour/seed generator, the counterpart of LeMonADE's
  * RandomNumberGenerators whose r250_rand32() the reference calls

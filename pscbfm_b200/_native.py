@@ -56,7 +56,7 @@ _lock = threading.Lock()
 _lib = None
 
 # status codes of include/pscbfm_b200.h
-BFM_OK, BFM_EINVAL, BFM_ERUNTIME, BFM_ECUDA, BFM_ETIMEOUT, BFM_ENOTINIT, BFM_EUNSUPPORTED = range(7)
+BFM_OK, BFM_EINVAL, BFM_ERUNTIME, BFM_ECUDA, BFM_ETIMEOUT, BFM_ENOTINIT, BFM_EUNSUPPORTED, BFM_ETOOLARGE = range(8)
 
 _c = ctypes
 _P = _c.c_void_p
@@ -95,6 +95,8 @@ _SIGS = {
     "bfm_set_launch_mode": (_c.c_int, [_P, _c.c_int]),
     "bfm_time_kernels": (_c.c_int, [_P, _c.c_uint32, _c.POINTER(_c.c_double), _c.POINTER(_c.c_double), _c.POINTER(_c.c_uint64)]),
     "bfm_color_graph": (_c.c_int, [_c.c_uint32, _P, _P, _c.c_int, _P, _P]),
+    "bfm_substep_noalloc": (_c.c_int, [_P, _P, _P, _P, _c.c_uint32, _P, _c.c_uint32, _c.c_uint32, _c.c_uint32, _P,
+                                       _c.c_uint32, _c.c_uint32, _c.c_uint32, _c.c_uint32, _c.c_int, _P]),
     "bfm_r250_seed": (_c.c_int, [_c.c_uint64]),
     "bfm_r250_seed_words": (_c.c_int, [_P, _c.c_size_t]),
     "bfm_r250_get_state": (_c.c_int, [_P]),

@@ -771,6 +771,98 @@ struct Engine {
     }
 };
 
+/* ------------------------------------------- no-allocation colour substep
+ *
+ * bfm_substep_noalloc runs one colour substep on device arrays owned by the
+ * caller.  Its only scratch -- the target bit lattice and the per-monomer
+ * check/perform hand-over flags -- lives in the file-scope device array
+ * below, so the call allocates nothing.  The array is sized for lattices of
+ * up to 128^3 sites and up to 262,144 monomers per substep (512 KiB, held by
+ * every GPU that loads the library until the process exits).
+ */
+constexpr uint32_t kNoAllocMaxSites = 1u << 21;                   /* 128^3 */
+constexpr uint32_t kNoAllocMaxCount = 1u << 18;                   /* monomers per call */
+constexpr size_t kNoAllocTmpWords = kNoAllocMaxSites / 32;        /* 256 KiB of target bits */
+constexpr size_t kNoAllocFlagWords = kNoAllocMaxCount / 4;        /* 256 KiB of flags */
+
+template <int RNG>
+__global__ void __launch_bounds__(kThreads) k_check_na(const uint32_t *__restrict__ pos, const uint32_t *__restrict__ nbr,
+                                                       const uint8_t *__restrict__ deg, uint32_t npad,
+                                                       const uint32_t *__restrict__ lat, uint32_t *tmp,
+                                                       uint8_t *__restrict__ flags, uint32_t off, uint32_t n,
+                                                       uint32_t seed, uint32_t iter, Geometry g, Bondset bonds)
+{
+    __shared__ uint32_t forbid[16];
+    if (threadIdx.x < 16) forbid[threadIdx.x] = bonds.forbidden[threadIdx.x];
+    __syncthreads();
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = off + i;
+        const uint32_t r0 = pos[slot];
+        const int dir = direction(draw<RNG>(seed, iter, i));
+        const uint32_t r1 = zstep(r0, dir, g);
+        bool ok = true;
+        for (uint32_t j = 0; j < deg[slot]; ++j) {
+            const uint32_t code = zbond(pos[nbr[(size_t)j * npad + slot]], r1);
+            if ((forbid[code >> 5] >> (code & 31u)) & 1u) {
+                ok = false;
+                break;
+            }
+        }
+        if (ok) ok = !face_occupied(lat, r0, dir, g);
+        if (ok) atomicOr(tmp + (r1 >> 5), 1u << (r1 & 31u));
+        flags[i] = ok ? (uint8_t)(dir | 8) : (uint8_t)0;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_perform_na(uint32_t *__restrict__ pos, int32_t *__restrict__ img, uint32_t npad,
+                                                         uint32_t *lat, const uint32_t *__restrict__ tmp,
+                                                         const uint8_t *__restrict__ flags, uint32_t off, uint32_t n,
+                                                         Geometry g)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint8_t f = flags[i];
+        if (!(f & 8)) continue;
+        const uint32_t slot = off + i;
+        const uint32_t r0 = pos[slot];
+        const int dir = f & 7;
+        if (face_occupied(tmp, r0, dir, g)) continue;
+        const uint32_t r1 = zstep(r0, dir, g);
+        atomicXor(lat + (r0 >> 5), 1u << (r0 & 31u));
+        atomicXor(lat + (r1 >> 5), 1u << (r1 & 31u));
+        pos[slot] = r1;
+        if (img) {
+            const int ax = dir >> 1;
+            const bool wrapped = (dir & 1) ? ((r1 & g.m[ax]) == 0) : ((r0 & g.m[ax]) == 0);
+            if (wrapped) img[(size_t)ax * npad + slot] += (dir & 1) ? 1 : -1;
+        }
+    }
+}
+
+} // namespace
+
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocTmpWords + kNoAllocFlagWords];
+
+namespace {
+std::mutex g_noalloc_mutex;
+void *g_noalloc_ptr[256] = {};
+
+/* Device address of g_noalloc_scratch on the current device.  Host code
+ * cannot use the array's name: on the host it is only a stand-in symbol, so
+ * the address is looked up once per device, with that device current. */
+int noalloc_scratch(uint32_t **out)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return BFM_ECUDA;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return BFM_ECUDA;
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = static_cast<uint32_t *>(g_noalloc_ptr[dev]);
+    return BFM_OK;
+}
+
 } // namespace
 
 struct bfm_handle {
@@ -1128,6 +1220,55 @@ int bfm_color_graph(uint32_t n, const uint8_t *deg, const uint32_t *nbr8, int un
     } catch (...) {
         return BFM_ERUNTIME;
     }
+}
+
+int bfm_substep_noalloc(uint32_t *pos, int32_t *img, const uint32_t *nbr, const uint8_t *deg, uint32_t npad,
+                        uint32_t *lattice, uint32_t box_x, uint32_t box_y, uint32_t box_z, const uint8_t *allowed512,
+                        uint32_t slot_offset, uint32_t count, uint32_t seed, uint32_t iteration, int rng, void *stream)
+{
+    if (!pos || !nbr || !deg || !lattice || !allowed512) return BFM_EINVAL;
+    if (rng != BFM_RNG_INTHASH && rng != BFM_RNG_SARU) return BFM_EINVAL;
+    const uint32_t b[3] = {box_x, box_y, box_z};
+    uint32_t Lm = 0;
+    for (int a = 0; a < 3; ++a) {
+        if (b[a] < 8 || (b[a] & (b[a] - 1))) return BFM_EINVAL;
+        Lm = std::max(Lm, b[a]);
+    }
+    if ((uint64_t)Lm * Lm * Lm > kNoAllocMaxSites || count > kNoAllocMaxCount) return BFM_ETOOLARGE;
+    if ((uint64_t)slot_offset + count > npad) return BFM_EINVAL;
+    unsigned nAllowed = 0;
+    Bondset bonds;
+    std::memset(&bonds, 0, sizeof(bonds));
+    for (uint32_t dz = 0; dz < 8; ++dz)
+        for (uint32_t dy = 0; dy < 8; ++dy)
+            for (uint32_t dx = 0; dx < 8; ++dx) {
+                if (allowed512[dx | (dy << 3) | (dz << 6)]) {
+                    ++nAllowed;
+                } else {
+                    const uint32_t code = zcode(dx, dy, dz);
+                    bonds.forbidden[code >> 5] |= 1u << (code & 31);
+                }
+            }
+    if (nAllowed != 108) return BFM_ERUNTIME;
+    Geometry g;
+    for (int a = 0; a < 3; ++a) g.m[a] = dilate3(b[a] - 1) << a;
+    uint32_t *scratch = nullptr;
+    const int st = noalloc_scratch(&scratch);
+    if (st != BFM_OK) return st;
+    uint32_t *tmp = scratch;
+    uint8_t *flags = reinterpret_cast<uint8_t *>(scratch + kNoAllocTmpWords);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t words = (size_t)Lm * Lm * Lm / 32;
+    if (cudaMemsetAsync(tmp, 0, words * sizeof(uint32_t), s) != cudaSuccess) return BFM_ECUDA;
+    if (count) {
+        const int blocks = (int)std::min<uint32_t>((count + kThreads - 1) / kThreads, 148u * 16u);
+        if (rng == BFM_RNG_SARU)
+            k_check_na<RNG_SARU><<<blocks, kThreads, 0, s>>>(pos, nbr, deg, npad, lattice, tmp, flags, slot_offset, count, seed, iteration, g, bonds);
+        else
+            k_check_na<RNG_INTHASH><<<blocks, kThreads, 0, s>>>(pos, nbr, deg, npad, lattice, tmp, flags, slot_offset, count, seed, iteration, g, bonds);
+        k_perform_na<<<blocks, kThreads, 0, s>>>(pos, img, npad, lattice, tmp, flags, slot_offset, count, g);
+    }
+    return cudaGetLastError() == cudaSuccess ? BFM_OK : BFM_ECUDA;
 }
 
 int bfm_r250_seed(uint64_t seed)
