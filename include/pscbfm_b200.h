@@ -106,14 +106,28 @@ int bfm_get_counters(bfm_handle *h, uint64_t out3[3]);
 int bfm_get_last_run_ms(const bfm_handle *h, double *ms);
 /* kernel launches issued by the last bfm_run */
 int bfm_get_last_run_launches(const bfm_handle *h, uint64_t *launches);
-/* runs nmcs Monte-Carlo steps like bfm_run (same trajectory) with every kernel
- * launched directly and bracketed by CUDA events on the handle's stream;
- * returns the summed device time of the check and of the perform kernels and
- * the number of launches of each */
-int bfm_time_kernels(bfm_handle *h, uint32_t nmcs, double *ms_check, double *ms_perform, uint64_t *launches_each);
-/* launch path: 0 = one check + one perform kernel per colour substep, captured
- * in CUDA graphs; 1 = same kernels launched one by one */
+/* runs nmcs Monte-Carlo steps like bfm_run (same trajectory) with CUDA
+ * events on the handle's stream around every sweep-kernel launch (CUDA
+ * graphs replaced by direct launches): summed device time in ms, number of
+ * launches and attempted moves covered */
+int bfm_time_kernels(bfm_handle *h, uint32_t nmcs, double *ms, uint64_t *launches, uint64_t *attempts);
+/* launch path: 0 = one persistent cooperative kernel per schedule chunk
+ * (default); 1 = one check + one perform kernel per colour substep, captured
+ * in CUDA graphs; 2 = the same kernels launched one by one */
 int bfm_set_launch_mode(bfm_handle *h, int mode);
+/* bound of every grid-barrier wait in the persistent kernel (default 2000 ms);
+ * a wait that runs out ends the launch and bfm_run returns BFM_ETIMEOUT */
+int bfm_set_barrier_timeout_ms(bfm_handle *h, uint32_t ms);
+/* Failure-detection check of the bounded grid barrier: `rounds` barriers of
+ * a cooperative kernel with one CTA per SM that expects extra_arrivals more
+ * CTAs than exist.  extra_arrivals = 0 returns BFM_OK; > 0 makes every wait
+ * run into timeout_ms and returns BFM_ETIMEOUT, with the context intact. */
+int bfm_barrier_selftest(int gpu, uint32_t timeout_ms, uint32_t extra_arrivals, uint32_t rounds, double *elapsed_ms);
+/* the same with a choice of barrier (counting = 1: monotone counter with
+ * release reductions, the one the sweep uses; 0: generation barrier) and of
+ * CTAs per SM; also measures the cost of one barrier (elapsed / rounds) */
+int bfm_barrier_selftest_variant(int gpu, uint32_t timeout_ms, uint32_t extra_arrivals, uint32_t rounds, int counting,
+                                 uint32_t ctas_per_sm, double *elapsed_ms);
 
 /* The species colouring initialize() uses (the reference's graphColoring,
  * graphColoring.tpp:103-439, with uniform rebalancing as called at

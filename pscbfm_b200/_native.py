@@ -19,7 +19,7 @@ LIBPATH = os.path.join(HERE, LIBNAME)
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 SOURCES = ["bfm_engine.cu"]
-HEADERS = ["bfm_device.cuh", "bfm_host.hpp", "../../include/pscbfm_b200.h"]
+HEADERS = ["bfm_device.cuh", "bfm_host.hpp", "bfm_sweep.cuh", "../../include/pscbfm_b200.h"]
 
 NVCC_FLAGS = [
     "-std=c++17",
@@ -93,7 +93,11 @@ _SIGS = {
     "bfm_get_last_run_ms": (_c.c_int, [_P, _c.POINTER(_c.c_double)]),
     "bfm_get_last_run_launches": (_c.c_int, [_P, _c.POINTER(_c.c_uint64)]),
     "bfm_set_launch_mode": (_c.c_int, [_P, _c.c_int]),
-    "bfm_time_kernels": (_c.c_int, [_P, _c.c_uint32, _c.POINTER(_c.c_double), _c.POINTER(_c.c_double), _c.POINTER(_c.c_uint64)]),
+    "bfm_time_kernels": (_c.c_int, [_P, _c.c_uint32, _c.POINTER(_c.c_double), _c.POINTER(_c.c_uint64), _c.POINTER(_c.c_uint64)]),
+    "bfm_set_barrier_timeout_ms": (_c.c_int, [_P, _c.c_uint32]),
+    "bfm_barrier_selftest": (_c.c_int, [_c.c_int, _c.c_uint32, _c.c_uint32, _c.c_uint32, _c.POINTER(_c.c_double)]),
+    "bfm_barrier_selftest_variant": (_c.c_int, [_c.c_int, _c.c_uint32, _c.c_uint32, _c.c_uint32, _c.c_int, _c.c_uint32,
+                                                _c.POINTER(_c.c_double)]),
     "bfm_color_graph": (_c.c_int, [_c.c_uint32, _P, _P, _c.c_int, _P, _P]),
     "bfm_substep_noalloc": (_c.c_int, [_P, _P, _P, _P, _c.c_uint32, _P, _c.c_uint32, _c.c_uint32, _c.c_uint32, _P,
                                        _c.c_uint32, _c.c_uint32, _c.c_uint32, _c.c_uint32, _c.c_int, _P]),

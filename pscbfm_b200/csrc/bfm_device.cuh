@@ -49,6 +49,13 @@ __host__ __device__ inline uint32_t zcode(uint32_t x, uint32_t y, uint32_t z)
     return dilate3(x) | (dilate3(y) << 1) | (dilate3(z) << 2);
 }
 
+/* the payload mask of axis ax, selected without indexing (an indexed
+ * parameter array would live in local memory) */
+__host__ __device__ inline uint32_t axis_mask(const Geometry &g, int ax)
+{
+    return ax == 0 ? g.m[0] : (ax == 1 ? g.m[1] : g.m[2]);
+}
+
 /* +1 / -1 along one axis with periodic wrap (mask = that axis' payload) */
 __host__ __device__ inline uint32_t zinc(uint32_t a, uint32_t mask, uint32_t unit)
 {
@@ -64,7 +71,8 @@ __host__ __device__ inline uint32_t zstep(uint32_t a, int dir, const Geometry &g
 {
     const int ax = dir >> 1;
     const uint32_t unit = 1u << ax;
-    return (dir & 1) ? zinc(a, g.m[ax], unit) : zdec(a, g.m[ax], unit);
+    const uint32_t m = axis_mask(g, ax);
+    return (dir & 1) ? zinc(a, m, unit) : zdec(a, m, unit);
 }
 
 /* Interleaved 9-bit code of the bond vector (b - a) mod 8 per axis.  The
@@ -93,9 +101,9 @@ __host__ __device__ inline Face zface(uint32_t r0, int dir, const Geometry &g)
     const int bx = (ax == 0) ? 1 : 0;
     const int cx = (ax == 2) ? 1 : 2;
     const uint32_t unit = 1u << ax;
-    uint32_t p = (dir & 1) ? zinc(zinc(r0, g.m[ax], unit), g.m[ax], unit)
-                           : zdec(zdec(r0, g.m[ax], unit), g.m[ax], unit);
-    const uint32_t mb = g.m[bx], mc = g.m[cx];
+    const uint32_t ma = axis_mask(g, ax);
+    uint32_t p = (dir & 1) ? zinc(zinc(r0, ma, unit), ma, unit) : zdec(zdec(r0, ma, unit), ma, unit);
+    const uint32_t mb = axis_mask(g, bx), mc = axis_mask(g, cx);
     const uint32_t ub = 1u << bx, uc = 1u << cx;
     Face f;
     f.base = p & ~(mb | mc);

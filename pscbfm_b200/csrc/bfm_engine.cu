@@ -36,6 +36,7 @@
 
 #include "bfm_device.cuh"
 #include "bfm_host.hpp"
+#include "bfm_sweep.cuh"
 #include "../../include/pscbfm_b200.h"
 
 using namespace bfm;
@@ -47,6 +48,8 @@ constexpr uint32_t kSlabAlign = 128;
 constexpr uint32_t kNoId = 0xFFFFFFFFu;
 constexpr uint32_t kChunk = 4096;       /* substeps per uploaded schedule chunk */
 constexpr uint32_t kGraphSubsteps = 64; /* substeps per captured CUDA graph */
+constexpr int kSweepThreads = 1024;     /* threads per CTA of the persistent kernel */
+constexpr uint32_t kSweepSmemListMax = 48u * 1024u; /* candidate list bytes kept in shared memory */
 
 struct Species {
     uint32_t off, n;
@@ -69,6 +72,8 @@ struct Sys {
     int32_t *img;
     const uint32_t *nbr;
     const uint8_t *deg;
+    uint16_t *bcode;      /* bond codes zbond(partner, self), row per bond (stored-bond path) */
+    const uint8_t *rev;   /* for bond row j of a monomer: the row of the partner that points back */
     uint8_t *flags;
     uint32_t *lat;
     uint32_t *tmp;
@@ -179,7 +184,7 @@ __global__ void __launch_bounds__(kThreads) k_perform(Sys s, const Substep *__re
                     }
                     s.pos[slot] = r1;
                     const int ax = dir >> 1;
-                    const bool wrapped = (dir & 1) ? ((r1 & s.g.m[ax]) == 0) : ((r0 & s.g.m[ax]) == 0);
+                    const bool wrapped = (dir & 1) ? ((r1 & axis_mask(s.g, ax)) == 0) : ((r0 & axis_mask(s.g, ax)) == 0);
                     if (wrapped) s.img[(size_t)ax * s.npad + slot] += (dir & 1) ? 1 : -1;
                     acc = 1;
                 }
@@ -188,6 +193,281 @@ __global__ void __launch_bounds__(kThreads) k_perform(Sys s, const Substep *__re
         nAcc += __syncthreads_count(acc);
     }
     if (threadIdx.x == 0 && nAcc && s.counters) atomicAdd(s.counters + 1, (unsigned long long)nAcc);
+}
+
+/* 9-bit bond code minus / plus one unit along axis ax (per-axis modulo 8) */
+__device__ __forceinline__ uint32_t bcode_dec(uint32_t c, uint32_t ax)
+{
+    const uint32_t m = 0x49u << ax;
+    return (c & ~m) | (((c & m) - (1u << ax)) & m);
+}
+__device__ __forceinline__ uint32_t bcode_inc(uint32_t c, uint32_t ax)
+{
+    const uint32_t m = 0x49u << ax;
+    return (c & ~m) | (((c | ~m) + (1u << ax)) & m);
+}
+
+/* per-axis negation modulo 8 of a 9-bit bond code: the code of the bond
+ * seen from the partner */
+__device__ __forceinline__ uint32_t bcode_neg(uint32_t c)
+{
+    return ((0u - (c & 0x049u)) & 0x049u) | ((0u - (c & 0x092u)) & 0x092u) | ((0u - (c & 0x124u)) & 0x124u);
+}
+
+/* bond code of every stored bond from the current positions */
+__global__ void k_bondcodes(const uint32_t *__restrict__ pos, const uint32_t *__restrict__ nbr, const uint8_t *__restrict__ deg,
+                            uint16_t *__restrict__ bcode, uint32_t npad)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npad; i += gridDim.x * blockDim.x) {
+        const uint32_t r = pos[i];
+        for (uint32_t j = 0; j < deg[i]; ++j)
+            bcode[(size_t)j * npad + i] = (uint16_t)zbond(pos[nbr[(size_t)j * npad + i]], r);
+    }
+}
+
+/* The persistent sweep kernel (see bfm_sweep.cuh): substeps [k0, k1) of
+ * the schedule, check / barrier / perform / barrier per substep.  Each CTA
+ * owns one contiguous range of every colour slab (equal work per SM, a
+ * compact Z-order region per CTA).  STORED: bonds are tested from their
+ * stored codes (bond vector mod 8, updated by the movers), otherwise from the
+ * partners' positions. */
+template <int RNG, bool STORED>
+__global__ void __launch_bounds__(kSweepThreads, 1)
+    k_sweep(Sys s, const Substep *__restrict__ sched, uint32_t k0, uint32_t k1, GridBarrier *bar, uint2 *glist,
+            uint32_t cap, unsigned long long timeoutNs, uint32_t maxdeg)
+{
+    extern __shared__ uint2 s_dyn[];
+    __shared__ __align__(16) unsigned long long s_table[kFaceTableA];
+    __shared__ __align__(16) DirConst s_dir[6];
+    __shared__ uint32_t s_forbid[16];
+    __shared__ uint32_t s_after[6 * 16]; /* forbidden after a move in dir: bit (code) of row dir */
+    __shared__ unsigned int s_count;
+
+    uint2 *list = glist ? glist + (size_t)blockIdx.x * cap : s_dyn;
+    build_face_table_a(s_table);
+    build_dir_table(s_dir, s.g);
+    if (threadIdx.x < 16) s_forbid[threadIdx.x] = s.bonds.forbidden[threadIdx.x];
+    if (threadIdx.x < 96) {
+        const uint32_t dir = threadIdx.x >> 4, w = threadIdx.x & 15u, ax = dir >> 1;
+        uint32_t bits = 0;
+        for (uint32_t b = 0; b < 32; ++b) {
+            const uint32_t c = w * 32u + b;
+            const uint32_t nc = (dir & 1u) ? bcode_dec(c, ax) : bcode_inc(c, ax); /* (q - r0) - D */
+            bits |= ((s.bonds.forbidden[nc >> 5] >> (nc & 31u)) & 1u) << b;
+        }
+        s_after[threadIdx.x] = bits;
+    }
+    if (threadIdx.x == 0) s_count = 0;
+    unsigned int target = 0; /* counting barrier: arrivals expected so far */
+    __syncthreads();
+
+    unsigned long long *lat = reinterpret_cast<unsigned long long *>(s.lat);
+    unsigned long long *tmp = reinterpret_cast<unsigned long long *>(s.tmp);
+    const uint32_t words = s.latWords >> 1;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t npad = s.npad;
+    const uint32_t *__restrict__ nbr = s.nbr;
+    const uint8_t *__restrict__ deg = s.deg;
+    uint16_t *bcode = s.bcode;
+    uint32_t *pos = s.pos;
+    unsigned int nCand = 0, nAcc = 0;
+    uint32_t prevBuf = 0;
+    bool havePrev = false;
+    bool alive = true;
+
+    for (uint32_t k = k0; k < k1; ++k) {
+        const Substep d = sched[k];
+        const Species sp = s.spec[d.species];
+        /* zero the target words this CTA's candidates set in the previous substep */
+        if (havePrev) {
+            unsigned long long *tp = tmp + (size_t)prevBuf * words;
+            const unsigned int cnt = s_count;
+            for (uint32_t j = threadIdx.x; j < cnt; j += blockDim.x) {
+                const uint2 e = list[j];
+                const int dir = (int)(e.x >> 28);
+                tp[dstep(e.y, dir, s_dir[dir]) >> 6] = 0ull;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_count = 0;
+        __syncthreads();
+
+        /* phase A: check this CTA's contiguous range [lo, hi) of the slab */
+        unsigned long long *tb = tmp + (size_t)d.buf * words;
+        const uint32_t lo = (uint32_t)(((uint64_t)sp.n * blockIdx.x) / gridDim.x);
+        const uint32_t hi = (uint32_t)(((uint64_t)sp.n * (blockIdx.x + 1)) / gridDim.x);
+        uint32_t i = lo + threadIdx.x;
+        uint32_t nr0 = 0, ndg = 0, na = 0, nb = 0;
+        if (i < hi) {
+            const uint32_t slot = sp.off + i;
+            nr0 = pos[slot];
+            ndg = deg[slot];
+            if (STORED) {
+                na = maxdeg > 0 ? bcode[slot] : 0u;
+                nb = maxdeg > 1 ? bcode[(size_t)npad + slot] : 0u;
+            } else {
+                na = maxdeg > 0 ? nbr[slot] : 0u;
+                nb = maxdeg > 1 ? nbr[(size_t)npad + slot] : 0u;
+            }
+        }
+        for (uint32_t base = lo; base < hi; base += blockDim.x, i += blockDim.x) {
+            const uint32_t r0 = nr0, dg = ndg, ea = na, eb = nb;
+            const bool valid = i < hi;
+            const uint32_t inext = i + blockDim.x;
+            if (inext < hi) {
+                const uint32_t slot = sp.off + inext;
+                nr0 = pos[slot];
+                ndg = deg[slot];
+                if (STORED) {
+                    na = maxdeg > 0 ? bcode[slot] : 0u;
+                    nb = maxdeg > 1 ? bcode[(size_t)npad + slot] : 0u;
+                } else {
+                    na = maxdeg > 0 ? nbr[slot] : 0u;
+                    nb = maxdeg > 1 ? nbr[(size_t)npad + slot] : 0u;
+                }
+            }
+            bool ok = false;
+            int dir = 0;
+            if (valid) {
+                dir = direction(draw<RNG>(d.seed, d.iter, i));
+                const DirConst dc = s_dir[dir];
+                const Face4 f = face4d(r0, dir, dc, s_table);
+                const uint32_t r1 = dstep(r0, dir, dc);
+                if (STORED) {
+                    const uint32_t *after = s_after + dir * 16;
+                    ok = !face4_occupied(lat, f);
+                    if (dg > 0) ok = ok && !((after[ea >> 5] >> (ea & 31u)) & 1u);
+                    if (dg > 1) ok = ok && !((after[eb >> 5] >> (eb & 31u)) & 1u);
+                    for (uint32_t j = 2; j < dg; ++j) {
+                        const uint32_t c = bcode[(size_t)j * npad + sp.off + i];
+                        if ((after[c >> 5] >> (c & 31u)) & 1u) ok = false;
+                    }
+                } else {
+                    const uint32_t p0 = pos[ea];
+                    const uint32_t p1 = pos[eb];
+                    ok = !face4_occupied(lat, f);
+                    if (dg > 0) {
+                        const uint32_t c = zbond(p0, r1);
+                        ok = ok && !((s_forbid[c >> 5] >> (c & 31u)) & 1u);
+                    }
+                    if (dg > 1) {
+                        const uint32_t c = zbond(p1, r1);
+                        ok = ok && !((s_forbid[c >> 5] >> (c & 31u)) & 1u);
+                    }
+                    for (uint32_t j = 2; j < dg; ++j) {
+                        const uint32_t c = zbond(pos[nbr[(size_t)j * npad + sp.off + i]], r1);
+                        if ((s_forbid[c >> 5] >> (c & 31u)) & 1u) ok = false;
+                    }
+                }
+                if (ok) atomicOr(tb + (r1 >> 6), 1ull << (r1 & 63u));
+            }
+            const unsigned int m = __ballot_sync(0xFFFFFFFFu, ok);
+            if (m) {
+                const int leader = __ffs(m) - 1;
+                unsigned int at = 0;
+                if ((int)lane == leader) at = atomicAdd(&s_count, (unsigned int)__popc(m));
+                at = __shfl_sync(0xFFFFFFFFu, at, leader);
+                if (ok) list[at + __popc(m & ((1u << lane) - 1u))] = make_uint2((sp.off + i) | ((uint32_t)dir << 28), r0);
+            }
+            nCand += ok ? 1u : 0u;
+        }
+        if (!grid_barrier_count(bar, target, gridDim.x, timeoutNs)) {
+            alive = false;
+            break;
+        }
+
+        /* phase B: perform, this CTA's candidates only */
+        {
+            const unsigned long long *tr = tmp + (size_t)d.buf * words;
+            const unsigned int cnt = s_count;
+            for (uint32_t j = threadIdx.x; j < cnt; j += blockDim.x) {
+                const uint2 e = list[j];
+                const int dir = (int)(e.x >> 28);
+                const uint32_t slot = e.x & 0x0FFFFFFFu;
+                const uint32_t r0 = e.y;
+                const DirConst dc = s_dir[dir];
+                const Face4 f = face4d(r0, dir, dc, s_table);
+                if (face4_occupied(tr, f)) continue;
+                const uint32_t r1 = dstep(r0, dir, dc);
+                const uint32_t w0 = r0 >> 6, w1 = r1 >> 6;
+                const unsigned long long b0 = 1ull << (r0 & 63u), b1 = 1ull << (r1 & 63u);
+                if (w0 == w1) {
+                    atomicXor(lat + w0, b0 | b1);
+                } else {
+                    atomicXor(lat + w0, b0);
+                    atomicXor(lat + w1, b1);
+                }
+                pos[slot] = r1;
+                const uint32_t ax = (uint32_t)(dir >> 1);
+                const bool wrapped = (dir & 1) ? ((r1 & dc.ma) == 0) : ((r0 & dc.ma) == 0);
+                if (wrapped) s.img[(size_t)ax * npad + slot] += (dir & 1) ? 1 : -1;
+                if (STORED) {
+                    /* own bonds: (q - r0) -> (q - r1); the partner's bond back is
+                     * always the per-axis negation, so it is written, not read */
+                    const uint32_t dg = deg[slot];
+                    const size_t o0 = slot, o1 = (size_t)npad + slot;
+                    const uint32_t q0 = maxdeg > 0 ? nbr[o0] : 0u, q1 = maxdeg > 1 ? nbr[o1] : 0u;
+                    const uint32_t v0 = maxdeg > 0 ? s.rev[o0] : 0u, v1 = maxdeg > 1 ? s.rev[o1] : 0u;
+                    const uint32_t c0 = maxdeg > 0 ? bcode[o0] : 0u, c1 = maxdeg > 1 ? bcode[o1] : 0u;
+                    if (dg > 0) {
+                        const uint32_t nc = (dir & 1) ? bcode_dec(c0, ax) : bcode_inc(c0, ax);
+                        bcode[o0] = (uint16_t)nc;
+                        bcode[(size_t)v0 * npad + q0] = (uint16_t)bcode_neg(nc);
+                    }
+                    if (dg > 1) {
+                        const uint32_t nc = (dir & 1) ? bcode_dec(c1, ax) : bcode_inc(c1, ax);
+                        bcode[o1] = (uint16_t)nc;
+                        bcode[(size_t)v1 * npad + q1] = (uint16_t)bcode_neg(nc);
+                    }
+                    for (uint32_t b = 2; b < dg; ++b) {
+                        const size_t own = (size_t)b * npad + slot;
+                        const uint32_t nc = (dir & 1) ? bcode_dec(bcode[own], ax) : bcode_inc(bcode[own], ax);
+                        bcode[own] = (uint16_t)nc;
+                        bcode[(size_t)s.rev[own] * npad + nbr[own]] = (uint16_t)bcode_neg(nc);
+                    }
+                }
+                ++nAcc;
+            }
+        }
+        if (!grid_barrier_count(bar, target, gridDim.x, timeoutNs)) {
+            alive = false;
+            break;
+        }
+        prevBuf = d.buf;
+        havePrev = true;
+    }
+    /* every CTA has passed the last barrier: zero the last targets so the
+     * next launch starts from clean target lattices */
+    if (alive && havePrev) {
+        unsigned long long *tp = tmp + (size_t)prevBuf * words;
+        const unsigned int cnt = s_count;
+        for (uint32_t j = threadIdx.x; j < cnt; j += blockDim.x) {
+            const uint2 e = list[j];
+            const int dir = (int)(e.x >> 28);
+            tp[dstep(e.y, dir, s_dir[dir]) >> 6] = 0ull;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        nCand += __shfl_down_sync(0xFFFFFFFFu, nCand, o);
+        nAcc += __shfl_down_sync(0xFFFFFFFFu, nAcc, o);
+    }
+    if (lane == 0 && s.counters) {
+        if (nCand) atomicAdd(s.counters + 0, (unsigned long long)nCand);
+        if (nAcc) atomicAdd(s.counters + 1, (unsigned long long)nAcc);
+    }
+}
+
+/* rounds grid barriers expecting `expected` CTAs; with expected > gridDim.x
+ * no barrier can complete and every wait runs into its bound */
+__global__ void k_barrier_selftest(GridBarrier *bar, unsigned int expected, unsigned long long timeoutNs, unsigned int rounds,
+                                   int counting)
+{
+    unsigned int gen = 0;
+    if (threadIdx.x == 0) gen = counting ? 0u : ld_acquire_gpu(&bar->gen);
+    for (unsigned int r = 0; r < rounds; ++r) {
+        const bool ok = counting ? grid_barrier_count(bar, gen, expected, timeoutNs) : grid_barrier(bar, expected, gen, timeoutNs);
+        if (!ok) return;
+    }
 }
 
 /* spatial re-sort support: inv[perm[i]] = i */
@@ -200,8 +480,9 @@ __global__ void k_invert(const uint32_t *__restrict__ perm, uint32_t *__restrict
 __global__ void k_permute(const uint32_t *__restrict__ perm, const uint32_t *__restrict__ inv, uint32_t npad,
                           uint32_t maxdeg, const uint32_t *__restrict__ pos, const int32_t *__restrict__ img,
                           const uint32_t *__restrict__ nbr, const uint8_t *__restrict__ deg,
-                          const uint32_t *__restrict__ s2o, uint32_t *__restrict__ pos2, int32_t *__restrict__ img2,
-                          uint32_t *__restrict__ nbr2, uint8_t *__restrict__ deg2, uint32_t *__restrict__ s2o2,
+                          const uint32_t *__restrict__ s2o, const uint8_t *__restrict__ rev,
+                          uint32_t *__restrict__ pos2, int32_t *__restrict__ img2, uint32_t *__restrict__ nbr2,
+                          uint8_t *__restrict__ deg2, uint32_t *__restrict__ s2o2, uint8_t *__restrict__ rev2,
                           uint32_t *__restrict__ o2s)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npad; i += gridDim.x * blockDim.x) {
@@ -212,8 +493,10 @@ __global__ void k_permute(const uint32_t *__restrict__ perm, const uint32_t *__r
         img2[2 * (size_t)npad + i] = img[2 * (size_t)npad + p];
         const uint8_t dg = deg[p];
         deg2[i] = dg;
-        for (uint32_t j = 0; j < maxdeg; ++j)
+        for (uint32_t j = 0; j < maxdeg; ++j) {
             nbr2[(size_t)j * npad + i] = j < dg ? inv[nbr[(size_t)j * npad + p]] : 0u;
+            rev2[(size_t)j * npad + i] = rev[(size_t)j * npad + p];
+        }
         const uint32_t o = s2o[p];
         s2o2[i] = o;
         if (o != kNoId) o2s[o] = i;
@@ -242,6 +525,9 @@ struct CudaError : std::runtime_error {
 };
 struct InvalidArgument : std::invalid_argument {
     using std::invalid_argument::invalid_argument;
+};
+struct DeviceTimeout : std::runtime_error {
+    using std::runtime_error::runtime_error;
 };
 
 #define CK(call)                                                                                          \
@@ -316,6 +602,9 @@ struct Engine {
     int32_t *d_img = nullptr, *d_img2 = nullptr;
     uint32_t *d_nbr = nullptr, *d_nbr2 = nullptr;
     uint8_t *d_deg = nullptr, *d_deg2 = nullptr;
+    uint8_t *d_rev = nullptr, *d_rev2 = nullptr;
+    uint16_t *d_bcode = nullptr;
+    bool storedBonds = false; /* every bond has a partner entry pointing back */
     uint32_t *d_s2o = nullptr, *d_s2o2 = nullptr, *d_o2s = nullptr;
     uint8_t *d_flags = nullptr;
     uint32_t *d_lat = nullptr, *d_tmp = nullptr;
@@ -329,7 +618,16 @@ struct Engine {
     size_t cubBytes = 0;
     int32_t *d_out = nullptr;
     int32_t *h_out = nullptr;
+    unsigned int *h_flag = nullptr;
     bool hostPosValid = false;
+
+    /* persistent kernel */
+    GridBarrier *d_bar = nullptr;
+    uint2 *d_glist = nullptr;
+    int sweepGrid = 0;
+    uint32_t sweepCap = 0;
+    size_t sweepSmem = 0;
+    unsigned long long timeoutNs = 2000000000ull;
 
     /* graphs: [schedule buffer][rng kind index] */
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -361,9 +659,9 @@ struct Engine {
             }
         graphRng = -1;
         dfree(d_pos); dfree(d_pos2); dfree(d_img); dfree(d_img2); dfree(d_nbr); dfree(d_nbr2);
-        dfree(d_deg); dfree(d_deg2); dfree(d_s2o); dfree(d_s2o2); dfree(d_o2s); dfree(d_flags);
+        dfree(d_deg); dfree(d_deg2); dfree(d_rev); dfree(d_rev2); dfree(d_bcode); dfree(d_s2o); dfree(d_s2o2); dfree(d_o2s); dfree(d_flags);
         dfree(d_lat); dfree(d_tmp); dfree(d_spec); dfree(d_counters); dfree(d_perm); dfree(d_inv);
-        dfree(d_iota); dfree(d_keys); dfree(d_out);
+        dfree(d_iota); dfree(d_keys); dfree(d_out); dfree(d_bar); dfree(d_glist);
         if (d_cub) cudaFree(d_cub);
         d_cub = nullptr;
         for (int b = 0; b < 2; ++b) {
@@ -375,6 +673,8 @@ struct Engine {
         }
         if (h_out) cudaFreeHost(h_out);
         h_out = nullptr;
+        if (h_flag) cudaFreeHost(h_flag);
+        h_flag = nullptr;
         for (auto e : profEvents) cudaEventDestroy(e);
         profEvents.clear();
         if (ev0) cudaEventDestroy(ev0);
@@ -393,6 +693,8 @@ struct Engine {
         s.img = d_img;
         s.nbr = d_nbr;
         s.deg = d_deg;
+        s.bcode = d_bcode;
+        s.rev = d_rev;
         s.flags = d_flags;
         s.lat = d_lat;
         s.tmp = d_tmp;
@@ -520,6 +822,26 @@ struct Engine {
             hdeg[slot] = deg[i];
             for (uint32_t j = 0; j < deg[i]; ++j) hnbr[(size_t)j * npad + slot] = o2s[nbr[(size_t)i * 8 + j]];
         }
+        /* reverse rows: the m-th bond of i to k pairs with the m-th bond of k to i */
+        std::vector<uint8_t> hrev((size_t)std::max(maxdeg, 1u) * npad, 0);
+        storedBonds = true;
+        for (uint32_t i = 0; i < n && storedBonds; ++i)
+            for (uint32_t j = 0; j < deg[i]; ++j) {
+                const uint32_t k = nbr[(size_t)i * 8 + j];
+                uint32_t occ = 0;
+                for (uint32_t t = 0; t < j; ++t) occ += nbr[(size_t)i * 8 + t] == k;
+                int r = -1;
+                for (uint32_t t = 0, seen = 0; t < deg[k]; ++t)
+                    if (nbr[(size_t)k * 8 + t] == i && seen++ == occ) {
+                        r = (int)t;
+                        break;
+                    }
+                if (r < 0 || k == i) {
+                    storedBonds = false;
+                    break;
+                }
+                hrev[(size_t)j * npad + o2s[i]] = (uint8_t)r;
+            }
 
         CK(cudaSetDevice(gpu));
         CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
@@ -530,6 +852,8 @@ struct Engine {
         dalloc(d_img, 3 * (size_t)npad); dalloc(d_img2, 3 * (size_t)npad);
         dalloc(d_nbr, nbrRows * npad); dalloc(d_nbr2, nbrRows * npad);
         dalloc(d_deg, npad); dalloc(d_deg2, npad);
+        dalloc(d_rev, nbrRows * npad); dalloc(d_rev2, nbrRows * npad);
+        dalloc(d_bcode, nbrRows * npad);
         dalloc(d_s2o, npad); dalloc(d_s2o2, npad); dalloc(d_o2s, n);
         dalloc(d_flags, npad);
         dalloc(d_lat, latWords);
@@ -544,6 +868,8 @@ struct Engine {
             CK(cudaEventCreateWithFlags(&schedFree[b], cudaEventDisableTiming));
         }
         CK(cudaMallocHost((void **)&h_out, 3 * (size_t)n * sizeof(int32_t)));
+        CK(cudaMallocHost((void **)&h_flag, sizeof(unsigned int)));
+        *h_flag = 0;
         {
             cub::DeviceRadixSort::SortPairs(nullptr, cubBytes, d_pos, d_keys, d_iota, d_perm, (int)nmax, 0, (int)keyBits, stream);
             CK(cudaMalloc(&d_cub, std::max<size_t>(cubBytes, 16)));
@@ -554,6 +880,8 @@ struct Engine {
         CK(cudaMemcpyAsync(d_img, himg.data(), himg.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
         CK(cudaMemcpyAsync(d_nbr, hnbr.data(), hnbr.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
         CK(cudaMemcpyAsync(d_deg, hdeg.data(), npad, cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_rev, hrev.data(), hrev.size(), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemsetAsync(d_bcode, 0, nbrRows * npad * sizeof(uint16_t), stream));
         CK(cudaMemcpyAsync(d_s2o, s2o.data(), npad * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
         CK(cudaMemcpyAsync(d_o2s, o2s.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
         CK(cudaMemcpyAsync(d_lat, hlat.data(), latWords * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
@@ -563,6 +891,9 @@ struct Engine {
         CK(cudaMemsetAsync(d_tmp, 0, 2 * latWords * sizeof(uint32_t), stream));
         CK(cudaMemsetAsync(d_flags, 0, npad, stream));
         CK(cudaMemsetAsync(d_counters, 0, 4 * sizeof(unsigned long long), stream));
+        dalloc(d_bar, 1);
+        CK(cudaMemsetAsync(d_bar, 0, sizeof(GridBarrier), stream));
+        configureSweep();
         CK(cudaStreamSynchronize(stream));
         substepCounter = 0;
         nAttempts = 0;
@@ -574,6 +905,72 @@ struct Engine {
          * same slot order before the first substep. */
         spatialSort();
         hostPosValid = false;
+    }
+
+    /* recompute the stored bond codes from the positions (after set-up, a
+     * re-sort, or a run of the per-substep kernels, which do not keep them) */
+    void refreshBondCodes()
+    {
+        if (maxdeg == 0) return;
+        const int blocks = (int)std::min<uint32_t>((npad + kThreads - 1) / kThreads, 148 * 16);
+        k_bondcodes<<<blocks, kThreads, 0, stream>>>(d_pos, d_nbr, d_deg, d_bcode, npad);
+        CK(cudaGetLastError());
+    }
+
+    /* Persistent-kernel launch shape: as many CTAs as can be co-resident (a
+     * cooperative launch needs them all resident); each CTA's candidate
+     * list holds its worst case (every monomer it checks is a candidate),
+     * in shared memory when that fits. */
+    template <int RNG, bool STORED>
+    void configureFor(int smCount)
+    {
+        int blocks = 0;
+        size_t smem = 0;
+        uint32_t cap = 0;
+        for (int pass = 0; pass < 2; ++pass) {
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_sweep<RNG, STORED>, kSweepThreads, smem));
+            if (blocks < 1) throw std::runtime_error("persistent sweep kernel does not fit on an SM");
+            const uint32_t grid = (uint32_t)(blocks * smCount);
+            cap = std::max<uint32_t>(32u, (nmax + grid - 1) / grid + 1u);
+            const size_t want = cap * sizeof(uint2) <= kSweepSmemListMax ? cap * sizeof(uint2) : 0;
+            if (want == smem) break;
+            smem = want;
+        }
+        sweepGrid = blocks * smCount;
+        sweepCap = cap;
+        sweepSmem = smem;
+        if (smem > 0)
+            CK(cudaFuncSetAttribute(k_sweep<RNG, STORED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+
+    void configureSweep()
+    {
+        int dev = 0, sms = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        if (npad >= (1u << 28)) throw std::runtime_error("more than 2^28 monomer slots are not supported");
+        if (rng == BFM_RNG_SARU)
+            storedBonds ? configureFor<RNG_SARU, true>(sms) : configureFor<RNG_SARU, false>(sms);
+        else
+            storedBonds ? configureFor<RNG_INTHASH, true>(sms) : configureFor<RNG_INTHASH, false>(sms);
+        dfree(d_glist);
+        if (sweepSmem == 0) dalloc(d_glist, (size_t)sweepGrid * sweepCap);
+    }
+
+    void launchSweep(const Substep *sched, uint32_t k0, uint32_t k1)
+    {
+        Sys s = sys();
+        uint2 *gl = sweepSmem ? nullptr : d_glist;
+        uint32_t cap = sweepCap;
+        GridBarrier *bar = d_bar;
+        unsigned long long to = timeoutNs;
+        uint32_t md = maxdeg;
+        void *args[] = {&s, (void *)&sched, &k0, &k1, &bar, &gl, &cap, &to, &md};
+        CK(cudaMemsetAsync(d_bar, 0, sizeof(GridBarrier), stream)); /* the counting barrier starts at 0 */
+        const void *fn = rng == BFM_RNG_SARU
+                             ? (storedBonds ? (const void *)k_sweep<RNG_SARU, true> : (const void *)k_sweep<RNG_SARU, false>)
+                             : (storedBonds ? (const void *)k_sweep<RNG_INTHASH, true> : (const void *)k_sweep<RNG_INTHASH, false>);
+        CK(cudaLaunchCooperativeKernel(fn, dim3(sweepGrid), dim3(kSweepThreads), args, sweepSmem, stream));
     }
 
     /* doSpatialSorting (.cu:1835-1943): per species, order slots by the
@@ -588,13 +985,15 @@ struct Engine {
         }
         const int blocks = (int)std::min<uint32_t>((npad + kThreads - 1) / kThreads, 148 * 16);
         k_invert<<<blocks, kThreads, 0, stream>>>(d_perm, d_inv, npad);
-        k_permute<<<blocks, kThreads, 0, stream>>>(d_perm, d_inv, npad, maxdeg, d_pos, d_img, d_nbr, d_deg, d_s2o, d_pos2,
-                                                   d_img2, d_nbr2, d_deg2, d_s2o2, d_o2s);
+        k_permute<<<blocks, kThreads, 0, stream>>>(d_perm, d_inv, npad, maxdeg, d_pos, d_img, d_nbr, d_deg, d_s2o, d_rev,
+                                                   d_pos2, d_img2, d_nbr2, d_deg2, d_s2o2, d_rev2, d_o2s);
         CK(cudaGetLastError());
         std::swap(d_pos, d_pos2);
         std::swap(d_img, d_img2);
         std::swap(d_nbr, d_nbr2);
         std::swap(d_deg, d_deg2);
+        std::swap(d_rev, d_rev2);
+        refreshBondCodes();
         std::swap(d_s2o, d_s2o2);
         /* the captured graphs hold the old pointers */
         for (auto &ge : graph)
@@ -613,47 +1012,45 @@ struct Engine {
     }
     int performBlocks() const { return (int)std::max<uint32_t>(1, std::min<uint32_t>((nmax + kThreads - 1) / kThreads, 148u * 64u)); }
 
-    /* per-kernel event pairs when profiling (direct launches only) */
+    /* event pairs around every sweep-kernel launch when profiling */
     bool profiling = false;
     std::vector<cudaEvent_t> profEvents;
     size_t profUsed = 0;
-    cudaEvent_t profEvent()
+    void profMark()
     {
+        if (!profiling) return;
         if (profUsed == profEvents.size()) {
             cudaEvent_t e;
             CK(cudaEventCreate(&e));
             profEvents.push_back(e);
         }
-        return profEvents[profUsed++];
+        CK(cudaEventRecord(profEvents[profUsed++], stream));
     }
 
     void launchSubstep(const Substep *sched, uint32_t k)
     {
         const Sys s = sys();
-        cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
-        if (profiling) {
-            e0 = profEvent();
-            e1 = profEvent();
-            e2 = profEvent();
-            CK(cudaEventRecord(e0, stream));
-        }
+        profMark();
         if (rng == BFM_RNG_SARU)
             k_check<RNG_SARU><<<checkBlocks(), kThreads, 0, stream>>>(s, sched, k);
         else
             k_check<RNG_INTHASH><<<checkBlocks(), kThreads, 0, stream>>>(s, sched, k);
-        if (profiling) CK(cudaEventRecord(e1, stream));
+        profMark();
+        profMark();
         k_perform<<<performBlocks(), kThreads, 0, stream>>>(s, sched, k);
-        if (profiling) CK(cudaEventRecord(e2, stream));
+        profMark();
     }
 
-    /* run nMCS with every kernel bracketed by CUDA events on the launching
-     * stream; returns the summed durations of the check and perform kernels */
-    void timeKernels(uint32_t nMCS, double *msCheck, double *msPerform, uint64_t *launchesEach)
+    /* run nMCS in the current launch path (graphs replaced by direct
+     * launches) with CUDA events around every sweep-kernel launch on the
+     * handle's stream: summed device time, launches, attempted moves */
+    void timeKernels(uint32_t nMCS, double *ms, uint64_t *launches, uint64_t *attempts)
     {
         const int saved = launchMode;
-        launchMode = 1;
+        if (launchMode == 1) launchMode = 2;
         profiling = true;
         profUsed = 0;
+        const uint64_t a0 = nAttempts;
         try {
             run(nMCS);
         } catch (...) {
@@ -663,17 +1060,15 @@ struct Engine {
         }
         profiling = false;
         launchMode = saved;
-        double c = 0, p = 0;
-        for (size_t i = 0; i + 2 < profUsed; i += 3) {
-            float a = 0, b = 0;
+        double t = 0;
+        for (size_t i = 0; i + 1 < profUsed; i += 2) {
+            float a = 0;
             CK(cudaEventElapsedTime(&a, profEvents[i], profEvents[i + 1]));
-            CK(cudaEventElapsedTime(&b, profEvents[i + 1], profEvents[i + 2]));
-            c += a;
-            p += b;
+            t += a;
         }
-        *msCheck = c;
-        *msPerform = p;
-        *launchesEach = profUsed / 3;
+        *ms = t;
+        *launches = profUsed / 2;
+        *attempts = nAttempts - a0;
     }
 
     /* substeps per captured graph: a whole number of MCS */
@@ -708,7 +1103,7 @@ struct Engine {
         uint64_t launches = 0;
         uint32_t iStep = 0;
         int b = 0;
-        const uint32_t cap = launchMode == 0 ? graphSubsteps() : (kChunk / nSpecies) * nSpecies;
+        const uint32_t cap = launchMode == 1 ? graphSubsteps() : (kChunk / nSpecies) * nSpecies;
         while (iStep < nMCS) {
             /* one schedule chunk: whole MCS only, ending before a re-sort */
             CK(cudaEventSynchronize(schedFree[b]));
@@ -736,7 +1131,12 @@ struct Engine {
             if (sortFirst && !sortedFresh) spatialSort();
             CK(cudaMemcpyAsync(d_sched[b], hs, m * sizeof(Substep), cudaMemcpyHostToDevice, stream));
             CK(cudaEventRecord(schedFree[b], stream));
-            if (launchMode == 0 && m == cap) {
+            if (launchMode == 0) {
+                profMark();
+                launchSweep(d_sched[b], 0, m);
+                profMark();
+                launches += 1;
+            } else if (launchMode == 1 && m == cap) {
                 if (!graph[b]) buildGraph(b);
                 CK(cudaGraphLaunch(graph[b], stream));
                 launches += 2 * (uint64_t)m;
@@ -749,13 +1149,26 @@ struct Engine {
             b ^= 1;
         }
         age += nMCS;
+        /* the split kernels leave the target buffer of their last substep
+         * set; the persistent kernel clears its own before it returns */
+        if (launchMode != 0) {
+            CK(cudaMemsetAsync(d_tmp, 0, 2 * latWords * sizeof(uint32_t), stream));
+            refreshBondCodes();
+        }
         CK(cudaEventRecord(ev1, stream));
+        if (launchMode == 0) CK(cudaMemcpyAsync(h_flag, &d_bar->err, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream));
         CK(cudaEventSynchronize(ev1));
+        CK(cudaStreamSynchronize(stream));
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, ev0, ev1));
         lastRunMs = ms;
         lastLaunches = launches;
         CK(cudaGetLastError());
+        if (launchMode == 0 && *h_flag) {
+            CK(cudaMemsetAsync(d_bar, 0, sizeof(GridBarrier), stream));
+            CK(cudaStreamSynchronize(stream));
+            throw DeviceTimeout("a grid barrier of the persistent sweep kernel timed out; the positions of this run are not valid");
+        }
     }
 
     void readback()
@@ -832,7 +1245,7 @@ __global__ void __launch_bounds__(kThreads) k_perform_na(uint32_t *__restrict__ 
         pos[slot] = r1;
         if (img) {
             const int ax = dir >> 1;
-            const bool wrapped = (dir & 1) ? ((r1 & g.m[ax]) == 0) : ((r0 & g.m[ax]) == 0);
+            const bool wrapped = (dir & 1) ? ((r1 & axis_mask(g, ax)) == 0) : ((r0 & axis_mask(g, ax)) == 0);
             if (wrapped) img[(size_t)ax * npad + slot] += (dir & 1) ? 1 : -1;
         }
     }
@@ -880,6 +1293,9 @@ struct bfm_handle {
         } catch (CudaError const &ex) {                                \
             (h)->e.err = ex.what();                                    \
             return BFM_ECUDA;                                          \
+        } catch (DeviceTimeout const &ex) {                            \
+            (h)->e.err = ex.what();                                    \
+            return BFM_ETIMEOUT;                                       \
         } catch (std::invalid_argument const &ex) {                    \
             (h)->e.err = ex.what();                                    \
             return BFM_EINVAL;                                         \
@@ -890,6 +1306,9 @@ struct bfm_handle {
     } while (0)
 
 extern "C" {
+
+int bfm_barrier_selftest_variant(int gpu, uint32_t timeout_ms, uint32_t extra_arrivals, uint32_t rounds, int counting,
+                                 uint32_t ctas_per_sm, double *elapsed_ms);
 
 int bfm_create(bfm_handle **out)
 {
@@ -1183,19 +1602,76 @@ int bfm_get_last_run_launches(const bfm_handle *h, uint64_t *launches)
     return BFM_OK;
 }
 
-int bfm_time_kernels(bfm_handle *h, uint32_t nmcs, double *ms_check, double *ms_perform, uint64_t *launches_each)
+int bfm_time_kernels(bfm_handle *h, uint32_t nmcs, double *ms, uint64_t *launches, uint64_t *attempts)
 {
     if (h && !h->e.initialized) return BFM_ENOTINIT;
     GUARD(h, {
-        if (!ms_check || !ms_perform || !launches_each) throw InvalidArgument("null output pointer");
-        h->e.timeKernels(nmcs, ms_check, ms_perform, launches_each);
+        if (!ms || !launches || !attempts) throw InvalidArgument("null output pointer");
+        h->e.timeKernels(nmcs, ms, launches, attempts);
     });
+}
+
+int bfm_set_barrier_timeout_ms(bfm_handle *h, uint32_t ms)
+{
+    GUARD(h, {
+        if (ms == 0) throw InvalidArgument("barrier timeout must be positive");
+        h->e.timeoutNs = (unsigned long long)ms * 1000000ull;
+    });
+}
+
+int bfm_barrier_selftest(int gpu, uint32_t timeout_ms, uint32_t extra_arrivals, uint32_t rounds, double *elapsed_ms)
+{
+    return bfm_barrier_selftest_variant(gpu, timeout_ms, extra_arrivals, rounds, 1, 0, elapsed_ms);
+}
+
+int bfm_barrier_selftest_variant(int gpu, uint32_t timeout_ms, uint32_t extra_arrivals, uint32_t rounds, int counting,
+                                 uint32_t ctas_per_sm, double *elapsed_ms)
+{
+    GridBarrier *bar = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int status = BFM_OK;
+    do {
+        if (cudaSetDevice(gpu) != cudaSuccess) { status = BFM_ECUDA; break; }
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, gpu) != cudaSuccess) { status = BFM_ECUDA; break; }
+        if (cudaMalloc((void **)&bar, sizeof(GridBarrier)) != cudaSuccess) { status = BFM_ECUDA; break; }
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) { status = BFM_ECUDA; break; }
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaMemsetAsync(bar, 0, sizeof(GridBarrier), st);
+        const unsigned int grid = (unsigned int)sms * (ctas_per_sm ? ctas_per_sm : 1u);
+        unsigned int expected = grid + extra_arrivals;
+        unsigned long long to = (unsigned long long)timeout_ms * 1000000ull;
+        void *args[] = {&bar, &expected, &to, &rounds, &counting};
+        cudaEventRecord(e0, st);
+        if (cudaLaunchCooperativeKernel((const void *)k_barrier_selftest, dim3(grid), dim3(64), args, 0, st) != cudaSuccess) {
+            status = BFM_ECUDA;
+            break;
+        }
+        cudaEventRecord(e1, st);
+        GridBarrier hb;
+        if (cudaMemcpyAsync(&hb, bar, sizeof(hb), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            status = BFM_ECUDA;
+            break;
+        }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (elapsed_ms) *elapsed_ms = ms;
+        status = hb.err ? BFM_ETIMEOUT : BFM_OK;
+    } while (0);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (st) cudaStreamDestroy(st);
+    if (bar) cudaFree(bar);
+    return status;
 }
 
 int bfm_set_launch_mode(bfm_handle *h, int mode)
 {
     GUARD(h, {
-        if (mode < 0 || mode > 1) throw InvalidArgument("launch mode must be 0 (graphs) or 1 (direct)");
+        if (mode < 0 || mode > 2) throw InvalidArgument("launch mode must be 0 (persistent), 1 (graphs) or 2 (direct)");
         h->e.launchMode = mode;
     });
 }

@@ -1,0 +1,303 @@
+/*
+ * bfm_sweep.cuh -- the persistent colour-substep kernel.
+ *
+ * One cooperative launch runs a chunk of colour substeps.  Per substep:
+ *
+ *   phase A (check)    every monomer of the colour draws its move, tests its
+ *                      bonds and the leading face on the occupation lattice,
+ *                      and -- if both pass -- marks its target in the
+ *                      substep's target lattice and appends itself to its
+ *                      CTA's candidate list;
+ *   grid barrier
+ *   phase B (perform)  each CTA walks only its own candidates: a candidate
+ *                      moves unless another candidate's target lies in its
+ *                      leading face (the reference's deterministic two-phase
+ *                      rule, UpdaterGPUScBFM_AB_Type.cu:1148-1190);
+ *   grid barrier
+ *
+ * and at the start of the next substep each CTA zeroes the target words of
+ * its previous candidates (the target lattice is double buffered, so this
+ * never races with the marks of the running substep).  Lattices are read as
+ * 64-bit words: a word is a 4x4x4 brick of sites in Z-order, so the nine
+ * sites of a leading face lie in at most four words, whose masks come from a
+ * per-CTA table.
+ *
+ * Grid barriers wait with a bound: after `timeoutNs` of %globaltimer (or a
+ * fixed number of polls) a waiting CTA raises the error word and every CTA
+ * leaves the kernel, so a broken launch ends with BFM_ETIMEOUT instead of a
+ * hang.
+ */
+#pragma once
+#include <cstdint>
+
+#include "bfm_device.cuh"
+
+namespace bfm {
+
+struct GridBarrier {
+    unsigned int count; /* CTAs arrived at the current barrier */
+    unsigned int gen;   /* barrier generation, bumped by the last arrival */
+    unsigned int err;   /* non-zero: a wait timed out, leave the kernel */
+    unsigned int pad;
+};
+
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int *p)
+{
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+constexpr unsigned int kBarrierMaxPolls = 1u << 26;
+
+/* Grid-wide barrier for co-resident CTAs (cooperative launch).  `gen` is the
+ * generation the calling CTA expects (kept by thread 0).  Returns false on
+ * all threads of the CTA when the barrier failed (timeout here or elsewhere). */
+__device__ __forceinline__ bool grid_barrier(GridBarrier *bar, unsigned int nblocks, unsigned int &gen,
+                                             unsigned long long timeoutNs)
+{
+    __shared__ unsigned int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int ok = 1;
+        __threadfence();
+        const unsigned int arrived = atomicAdd(&bar->count, 1u);
+        if (arrived == nblocks - 1) {
+            atomicExch(&bar->count, 0u);
+            __threadfence();
+            atomicExch(&bar->gen, gen + 1u);
+        } else {
+            const unsigned long long t0 = global_ns();
+            unsigned int polls = 0;
+            while (ld_acquire_gpu(&bar->gen) == gen) {
+                if (ld_acquire_gpu(&bar->err)) {
+                    ok = 0;
+                    break;
+                }
+                if (++polls > kBarrierMaxPolls || global_ns() - t0 > timeoutNs) {
+                    atomicExch(&bar->err, 1u);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        gen += 1u;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+/* Counting grid barrier: the counter only grows.  Each CTA adds 1 with a
+ * release reduction (no return value, nothing to wait for) and then waits
+ * until the counter reaches `target` = (barriers passed so far + 1) x CTAs,
+ * reading it with acquire semantics.  The counter starts at 0 for every
+ * launch (the host clears it before the launch). */
+__device__ __forceinline__ void red_release_add(unsigned int *p, unsigned int v)
+{
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ bool grid_barrier_count(GridBarrier *bar, unsigned int &target, unsigned int nblocks,
+                                                   unsigned long long timeoutNs)
+{
+    __shared__ unsigned int s_ok2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int ok = 1;
+        target += nblocks;
+        red_release_add(&bar->count, 1u);
+        const unsigned long long t0 = global_ns();
+        unsigned int polls = 0;
+        while ((int)(ld_acquire_gpu(&bar->count) - target) < 0) {
+            if (ld_acquire_gpu(&bar->err)) {
+                ok = 0;
+                break;
+            }
+            if (++polls > kBarrierMaxPolls || global_ns() - t0 > timeoutNs) {
+                atomicExch(&bar->err, 1u);
+                ok = 0;
+                break;
+            }
+            __nanosleep(20);
+        }
+        s_ok2 = ok;
+    }
+    __syncthreads();
+    return s_ok2 != 0;
+}
+
+/* Face-mask table: for a move along axis a and the low two bits lb, lc of the
+ * first transverse values (b-1, c-1), the masks of the nine face sites in the
+ * (up to) four bricks, with the move axis' own bits still zero.  Entry
+ * ((a*4 + lb)*4 + lc)*4 + (gb | gc<<1). */
+constexpr int kFaceTable = 3 * 4 * 4 * 4;
+
+__device__ __forceinline__ void build_face_table(unsigned long long *t)
+{
+    for (int e = threadIdx.x; e < 48; e += blockDim.x) {
+        const int a = e >> 4, lb = (e >> 2) & 3, lc = e & 3;
+        const int bx = (a == 0) ? 1 : 0;
+        const int cx = (a == 2) ? 1 : 2;
+        unsigned long long m[4] = {0, 0, 0, 0};
+        for (int ib = 0; ib < 3; ++ib)
+            for (int ic = 0; ic < 3; ++ic) {
+                const int vb = lb + ib, vc = lc + ic;
+                const int g = (vb >= 4 ? 1 : 0) | (vc >= 4 ? 2 : 0);
+                const uint32_t ub = (uint32_t)(vb & 3), uc = (uint32_t)(vc & 3);
+                const uint32_t bit = (((ub & 1u) | ((ub & 2u) << 2)) << bx) | (((uc & 1u) | ((uc & 2u) << 2)) << cx);
+                m[g] |= 1ull << bit;
+            }
+        for (int g = 0; g < 4; ++g) t[e * 4 + g] = m[g];
+    }
+}
+
+struct Face4 {
+    uint32_t w[4];
+    unsigned long long m[4];
+};
+
+/* Face-mask table including the move axis' own two low bits la:
+ * entry (((ax*4 + la)*4 + lb)*4 + lc)*4 + (gb | gc<<1). 6 KiB. */
+constexpr int kFaceTableA = 3 * 4 * 4 * 4 * 4;
+
+__device__ __forceinline__ void build_face_table_a(unsigned long long *t)
+{
+    for (int e = threadIdx.x; e < 192; e += blockDim.x) {
+        const int a = e >> 6, la = (e >> 4) & 3, lb = (e >> 2) & 3, lc = e & 3;
+        const int bx = (a == 0) ? 1 : 0;
+        const int cx = (a == 2) ? 1 : 2;
+        const uint32_t abit = (((uint32_t)la & 1u) | (((uint32_t)la & 2u) << 2)) << a;
+        unsigned long long m0 = 0, m1 = 0, m2 = 0, m3 = 0;
+        for (int ib = 0; ib < 3; ++ib)
+            for (int ic = 0; ic < 3; ++ic) {
+                const int vb = lb + ib, vc = lc + ic;
+                const int g = (vb >= 4 ? 1 : 0) | (vc >= 4 ? 2 : 0);
+                const uint32_t ub = (uint32_t)(vb & 3), uc = (uint32_t)(vc & 3);
+                const uint32_t bit = abit | (((ub & 1u) | ((ub & 2u) << 2)) << bx) | (((uc & 1u) | ((uc & 2u) << 2)) << cx);
+                const unsigned long long v = 1ull << bit;
+                if (g == 0) m0 |= v;
+                else if (g == 1) m1 |= v;
+                else if (g == 2) m2 |= v;
+                else m3 |= v;
+            }
+        t[e * 4 + 0] = m0;
+        t[e * 4 + 1] = m1;
+        t[e * 4 + 2] = m2;
+        t[e * 4 + 3] = m3;
+    }
+}
+
+/* Per-direction constants: payload masks of the move axis and of the two
+ * transverse axes, their unit bits, and the bit position of the transverse
+ * axes (for extracting their two low coordinate bits). */
+struct DirConst {
+    uint32_t ma, mb, mc, ua;
+    uint32_t ub, uc, bx, cx;
+};
+
+__device__ __forceinline__ void build_dir_table(DirConst *t, const Geometry &g)
+{
+    if (threadIdx.x < 6) {
+        const int dir = threadIdx.x, ax = dir >> 1;
+        const int bx = (ax == 0) ? 1 : 0;
+        const int cx = (ax == 2) ? 1 : 2;
+        DirConst d;
+        d.ma = axis_mask(g, ax);
+        d.mb = axis_mask(g, bx);
+        d.mc = axis_mask(g, cx);
+        d.ua = 1u << ax;
+        d.ub = 1u << bx;
+        d.uc = 1u << cx;
+        d.bx = (uint32_t)bx;
+        d.cx = (uint32_t)cx;
+        t[dir] = d;
+    }
+}
+
+/* Unit step along the move axis of dir, using the per-direction constants. */
+__device__ __forceinline__ uint32_t dstep(uint32_t a, int dir, const DirConst &d)
+{
+    return (dir & 1) ? ((a & ~d.ma) | (((a | ~d.ma) + d.ua) & d.ma)) : ((a & ~d.ma) | (((a & d.ma) - d.ua) & d.ma));
+}
+
+/* The leading face as <= 4 (word, mask), from the direction constants and
+ * the table with the move axis' bits included. */
+__device__ __forceinline__ Face4 face4d(uint32_t r0, int dir, const DirConst &d, const unsigned long long *tableA)
+{
+    const uint32_t two = d.ua << 3; /* dilated 2 along the move axis */
+    const uint32_t pa = (dir & 1) ? (((r0 | ~d.ma) + two) & d.ma) : (((r0 & d.ma) - two) & d.ma);
+    const uint32_t b0 = ((r0 & d.mb) - d.ub) & d.mb;
+    const uint32_t b2 = ((r0 | ~d.mb) + d.ub) & d.mb;
+    const uint32_t c0 = ((r0 & d.mc) - d.uc) & d.mc;
+    const uint32_t c2 = ((r0 | ~d.mc) + d.uc) & d.mc;
+    const uint32_t ax = (uint32_t)(dir >> 1);
+    const uint32_t la = ((pa >> ax) & 1u) | ((pa >> (ax + 2)) & 2u);
+    const uint32_t lb = ((b0 >> d.bx) & 1u) | ((b0 >> (d.bx + 2)) & 2u);
+    const uint32_t lc = ((c0 >> d.cx) & 1u) | ((c0 >> (d.cx + 2)) & 2u);
+    const ulonglong2 *t = reinterpret_cast<const ulonglong2 *>(tableA + ((((ax * 4u + la) * 4u + lb) * 4u + lc) << 2));
+    const ulonglong2 t01 = t[0], t23 = t[1];
+    const uint32_t ha = pa >> 6, hb0 = b0 >> 6, hb2 = b2 >> 6, hc0 = c0 >> 6, hc2 = c2 >> 6;
+    Face4 f;
+    f.w[0] = ha | hb0 | hc0;
+    f.w[1] = ha | hb2 | hc0;
+    f.w[2] = ha | hb0 | hc2;
+    f.w[3] = ha | hb2 | hc2;
+    f.m[0] = t01.x;
+    f.m[1] = t01.y;
+    f.m[2] = t23.x;
+    f.m[3] = t23.y;
+    return f;
+}
+
+/* The leading face of a monomer at r0 moving in dir as <= 4 (word, mask). */
+__device__ __forceinline__ Face4 face4(uint32_t r0, int dir, const Geometry &g, const unsigned long long *table)
+{
+    const int ax = dir >> 1;
+    const int bx = (ax == 0) ? 1 : 0;
+    const int cx = (ax == 2) ? 1 : 2;
+    const uint32_t ua = 1u << ax;
+    const uint32_t ma = axis_mask(g, ax), mb = axis_mask(g, bx), mc = axis_mask(g, cx);
+    const uint32_t p = (dir & 1) ? zinc(zinc(r0, ma, ua), ma, ua) : zdec(zdec(r0, ma, ua), ma, ua);
+    const uint32_t pa = p & ma;
+    const uint32_t ub = 1u << bx, uc = 1u << cx;
+    const uint32_t b0 = ((p & mb) - ub) & mb;           /* dilated b-1 */
+    const uint32_t b2 = (((p & mb) | ~mb) + ub) & mb;   /* dilated b+1 */
+    const uint32_t c0 = ((p & mc) - uc) & mc;
+    const uint32_t c2 = (((p & mc) | ~mc) + uc) & mc;
+    const uint32_t lb = ((b0 >> bx) & 1u) | ((b0 >> (bx + 2)) & 2u);
+    const uint32_t lc = ((c0 >> cx) & 1u) | ((c0 >> (cx + 2)) & 2u);
+    const unsigned long long *t = table + (((ax * 4 + (int)lb) * 4 + (int)lc) << 2);
+    const uint32_t sh = pa & 63u; /* the move axis' low bits inside the word */
+    const uint32_t ha = pa >> 6, hb0 = b0 >> 6, hb2 = b2 >> 6, hc0 = c0 >> 6, hc2 = c2 >> 6;
+    Face4 f;
+    f.w[0] = ha | hb0 | hc0;
+    f.w[1] = ha | hb2 | hc0;
+    f.w[2] = ha | hb0 | hc2;
+    f.w[3] = ha | hb2 | hc2;
+    f.m[0] = t[0] << sh;
+    f.m[1] = t[1] << sh;
+    f.m[2] = t[2] << sh;
+    f.m[3] = t[3] << sh;
+    return f;
+}
+
+__device__ __forceinline__ bool face4_occupied(const unsigned long long *lat, const Face4 &f)
+{
+    unsigned long long o = lat[f.w[0]] & f.m[0];
+    if (f.m[1]) o |= lat[f.w[1]] & f.m[1];
+    if (f.m[2]) o |= lat[f.w[2]] & f.m[2];
+    if (f.m[3]) o |= lat[f.w[3]] & f.m[3];
+    return o != 0ull;
+}
+
+} // namespace bfm

@@ -224,11 +224,14 @@ class UpdaterGPUScBFM_AB_Type:
         return v.value
 
     def timeKernels(self, nmcs: int):
-        """Run nmcs MCS with per-kernel CUDA events; returns (check ms, perform
-        ms, launches of each) summed over the run."""
-        c, p, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_uint64()
-        self._check(self._lib.bfm_time_kernels(self._h, int(nmcs), ctypes.byref(c), ctypes.byref(p), ctypes.byref(n)))
-        return c.value, p.value, n.value
+        """Run nmcs MCS with CUDA events around every sweep-kernel launch;
+        returns (device ms, launches, attempted moves) summed over the run."""
+        ms, n, a = ctypes.c_double(), ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(self._lib.bfm_time_kernels(self._h, int(nmcs), ctypes.byref(ms), ctypes.byref(n), ctypes.byref(a)))
+        return ms.value, n.value, a.value
+
+    def setBarrierTimeoutMs(self, ms: int):
+        self._check(self._lib.bfm_set_barrier_timeout_ms(self._h, int(ms)))
 
     def setLaunchMode(self, mode: int):
         self._check(self._lib.bfm_set_launch_mode(self._h, int(mode)))

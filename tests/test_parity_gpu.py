@@ -11,6 +11,19 @@ from pscbfm_b200 import systems
 pytestmark = pytest.mark.gpu
 
 
+def _directed(base):
+    """Drop the back-pointer of a few bonds: the reference's setConnectivity
+    is directed (UpdaterGPUScBFM_AB_Type.cu:2616-2634), so a bond may be
+    listed on one side only; it then constrains only that side."""
+    s = systems.System(base.box, base.pos.copy(), base.deg.copy(), base.nbr.copy(), base.allowed.copy())
+    for i in (5, 40, 77):
+        j = int(s.nbr[i, s.deg[i] - 1])
+        s.deg[i] -= 1
+        s.nbr[i, s.deg[i]] = 0
+        assert j != i
+    return s
+
+
 def _systems():
     return {
         "dilute_chains": systems.saw_chains(40, 24, box=(64, 64, 64), seed=21),
@@ -19,6 +32,7 @@ def _systems():
         "crosslinked": systems.add_crosslinks(systems.saw_chains(40, 20, box=(32, 32, 32), seed=24), 60, seed=2),
         "melt_L32": systems.ordered_melt(32),
         "lone_monomers": systems.saw_chains(50, 1, box=(16, 16, 16), seed=25),
+        "directed_bonds": _directed(systems.saw_chains(60, 32, box=(32, 32, 32), seed=26)),
     }
 
 
@@ -61,11 +75,59 @@ def test_age_and_sorting_cadence(age, sort_every):
     run_pair(SYSTEMS["dense_chains"], pb.Rng.Saru, age=age, sort_every=sort_every, calls=[9, 1, 25])
 
 
-def test_launch_modes_agree():
+@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("name", ["crosslinked", "melt_L32", "dilute_chains"])
+def test_split_kernel_paths_match_oracle(name, mode):
+    """The per-substep kernels (CUDA graphs, direct launches) give the same
+    trajectory as the persistent kernel and the oracle."""
+    run_pair(SYSTEMS[name], pb.Rng.Saru, 0, 50, [70, 130], mode=mode)
+
+
+def test_launch_paths_agree_and_can_be_switched():
     s = SYSTEMS["crosslinked"]
-    a, _ = run_pair(s, pb.Rng.Saru, 0, 50, [200], mode=0)
-    b, _ = run_pair(s, pb.Rng.Saru, 0, 50, [200], mode=1)
-    assert np.array_equal(a.getAllMonomerPositions(), b.getAllMonomerPositions())
+    out = []
+    for mode in (0, 1, 2):
+        a, _ = run_pair(s, pb.Rng.Saru, 0, 50, [200], mode=mode)
+        out.append(a.getAllMonomerPositions())
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
+    # switching paths between calls on one handle keeps the trajectory
+    pb.r250_seed(1234)
+    st = pb.r250_get_state()
+    u = pb.UpdaterGPUScBFM_AB_Type().setup(s, rng=pb.Rng.Saru, steps_between_sortings=50)
+    o = oracle.Sweep(s, rng=2, sort_every=50, threads=4)
+    for mode, nmcs in ((0, 30), (2, 20), (1, 70), (0, 45)):
+        u.setLaunchMode(mode)
+        u.runSimulationOnGPU(nmcs)
+        o.run(nmcs, st)
+        assert np.array_equal(u.getAllMonomerPositions(), o.positions())
+
+
+def test_timed_run_keeps_trajectory():
+    """bfm_time_kernels advances the system exactly like bfm_run."""
+    s = SYSTEMS["dense_chains"]
+    pb.r250_seed(3)
+    st = pb.r250_get_state()
+    u = pb.UpdaterGPUScBFM_AB_Type().setup(s, rng=pb.Rng.Saru)
+    o = oracle.Sweep(s, rng=2, threads=4)
+    ms, launches, attempts = u.timeKernels(40)
+    o.run(40, st)
+    assert np.array_equal(u.getAllMonomerPositions(), o.positions())
+    assert ms > 0 and launches >= 1 and attempts == 40 * s.n
+
+
+def test_barrier_wait_is_bounded_and_reported():
+    """Failure detection without a GPU fault: a grid barrier that expects one
+    CTA more than exists can never complete; every wait must give up after
+    its bound, the call must report BFM_ETIMEOUT, and the context must stay
+    usable (a normal sweep afterwards is still bit-exact)."""
+    import ctypes
+    from pscbfm_b200 import _native
+    lib = _native.lib()
+    ms = ctypes.c_double()
+    assert lib.bfm_barrier_selftest(0, 200, 0, 64, ctypes.byref(ms)) == _native.BFM_OK
+    assert lib.bfm_barrier_selftest(0, 100, 1, 4, ctypes.byref(ms)) == _native.BFM_ETIMEOUT
+    assert 50.0 < ms.value < 5000.0
+    run_pair(SYSTEMS["dense_chains"], pb.Rng.Saru, 0, 13, [10])
 
 
 def test_three_colours_present():
