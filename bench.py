@@ -220,6 +220,7 @@ def run_b200(args, ranks):
     u = pb.UpdaterGPUScBFM_AB_Type().setup(system, gpu=gpu, rng=pb.Rng.Saru)
     S = args.mcs_per_step
     u.runSimulationOnGPU(args.melt_mcs)        # melt the serpentine crystal (untimed)
+    launch_info = u.getLaunchInfo()
     flushbuf = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{gpu}")
     for _ in range(args.warmup):
         flush_l2(flushbuf)
@@ -298,7 +299,8 @@ def run_b200(args, ranks):
         "config": {"workload": WORKLOAD, "mcs_per_step": S, "monomers": system.n, "box": list(system.box),
                    "colours": nspec, "replicas": ranks.world,
                    "l2": "flushed before every step (256 MiB write); the 19 MiB state is L2-resident within a step",
-                   "launch": "one persistent cooperative kernel per chunk of up to 4096 colour substeps"},
+                   "launch": "one persistent cooperative kernel per chunk of up to 4096 colour substeps",
+                   "kernel_shape": launch_info},
         "e2e": {"value": e2e, "unit": UNIT,
                 "h2d_bytes_per_step": S * nspec * 16,
                 "d2h_bytes_per_step": system.n * 12},

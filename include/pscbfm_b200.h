@@ -115,6 +115,12 @@ int bfm_time_kernels(bfm_handle *h, uint32_t nmcs, double *ms, uint64_t *launche
  * (default); 1 = one check + one perform kernel per colour substep, captured
  * in CUDA graphs; 2 = the same kernels launched one by one */
 int bfm_set_launch_mode(bfm_handle *h, int mode);
+/* shape of the persistent kernel chosen at initialize: mode 0 = bonds tested
+ * from the partners' positions, 1 = from stored bond codes, 2 = stored codes
+ * with the CTA's slab segments staged in shared memory by bulk copies
+ * (negative: -launch path of the per-substep kernels); CTAs, threads per CTA
+ * and dynamic shared memory per CTA */
+int bfm_get_launch_info(const bfm_handle *h, int *mode, int *grid, int *threads, size_t *smem_bytes);
 /* bound of every grid-barrier wait in the persistent kernel (default 2000 ms);
  * a wait that runs out ends the launch and bfm_run returns BFM_ETIMEOUT */
 int bfm_set_barrier_timeout_ms(bfm_handle *h, uint32_t ms);

@@ -95,6 +95,8 @@ _SIGS = {
     "bfm_set_launch_mode": (_c.c_int, [_P, _c.c_int]),
     "bfm_time_kernels": (_c.c_int, [_P, _c.c_uint32, _c.POINTER(_c.c_double), _c.POINTER(_c.c_uint64), _c.POINTER(_c.c_uint64)]),
     "bfm_set_barrier_timeout_ms": (_c.c_int, [_P, _c.c_uint32]),
+    "bfm_get_launch_info": (_c.c_int, [_P, _c.POINTER(_c.c_int), _c.POINTER(_c.c_int), _c.POINTER(_c.c_int),
+                                       _c.POINTER(_c.c_size_t)]),
     "bfm_barrier_selftest": (_c.c_int, [_c.c_int, _c.c_uint32, _c.c_uint32, _c.c_uint32, _c.POINTER(_c.c_double)]),
     "bfm_barrier_selftest_variant": (_c.c_int, [_c.c_int, _c.c_uint32, _c.c_uint32, _c.c_uint32, _c.c_int, _c.c_uint32,
                                                 _c.POINTER(_c.c_double)]),

@@ -225,25 +225,54 @@ __global__ void k_bondcodes(const uint32_t *__restrict__ pos, const uint32_t *__
     }
 }
 
+/* Bond modes of the persistent kernel */
+enum SweepMode {
+    SWEEP_GATHER = 0, /* bonds tested from the partners' positions */
+    SWEEP_STORED = 1, /* bonds tested from stored codes (bond vector mod 8) */
+    SWEEP_STAGED = 2  /* stored codes; a CTA's slab segments staged in shared memory by bulk copies */
+};
+
+/* Shared-memory layout of the staged mode for a window of W items (W a
+ * multiple of 16): positions (4 B), bond codes rows 0 and 1 (2 B each), bond
+ * count and direction (1 B each), then the candidate list. */
+struct StageLayout {
+    uint32_t W;
+    __host__ __device__ size_t pos() const { return 0; }
+    __host__ __device__ size_t bc0() const { return (size_t)W * 4; }
+    __host__ __device__ size_t bc1() const { return (size_t)W * 6; }
+    __host__ __device__ size_t dg() const { return (size_t)W * 8; }
+    __host__ __device__ size_t dirs() const { return (size_t)W * 9; }
+    __host__ __device__ size_t list() const { return (size_t)W * 10; }
+    __host__ __device__ size_t bytes(uint32_t cap) const { return list() + (size_t)cap * 8; }
+};
+
 /* The persistent sweep kernel (see bfm_sweep.cuh): substeps [k0, k1) of
  * the schedule, check / barrier / perform / barrier per substep.  Each CTA
  * owns one contiguous range of every colour slab (equal work per SM, a
- * compact Z-order region per CTA).  STORED: bonds are tested from their
- * stored codes (bond vector mod 8, updated by the movers), otherwise from the
- * partners' positions. */
-template <int RNG, bool STORED>
+ * compact Z-order region per CTA). */
+template <int RNG, int MODE>
 __global__ void __launch_bounds__(kSweepThreads, 1)
     k_sweep(Sys s, const Substep *__restrict__ sched, uint32_t k0, uint32_t k1, GridBarrier *bar, uint2 *glist,
-            uint32_t cap, unsigned long long timeoutNs, uint32_t maxdeg)
+            uint32_t cap, unsigned long long timeoutNs, uint32_t maxdeg, uint32_t window)
 {
-    extern __shared__ uint2 s_dyn[];
+    constexpr bool STORED = MODE != SWEEP_GATHER;
+    constexpr bool STAGE = MODE == SWEEP_STAGED;
+    extern __shared__ __align__(16) unsigned char s_dyn[];
     __shared__ __align__(16) unsigned long long s_table[kFaceTableA];
     __shared__ __align__(16) DirConst s_dir[6];
     __shared__ uint32_t s_forbid[16];
     __shared__ uint32_t s_after[6 * 16]; /* forbidden after a move in dir: bit (code) of row dir */
-    __shared__ unsigned int s_count;
+    __shared__ unsigned int s_cnt[2];     /* candidate count of the even / odd substep */
+    __shared__ __align__(8) unsigned long long s_mbar;
 
-    uint2 *list = glist ? glist + (size_t)blockIdx.x * cap : s_dyn;
+    const StageLayout lay{window};
+    uint32_t *st_pos = reinterpret_cast<uint32_t *>(s_dyn + lay.pos());
+    uint16_t *st_bc0 = reinterpret_cast<uint16_t *>(s_dyn + lay.bc0());
+    uint16_t *st_bc1 = reinterpret_cast<uint16_t *>(s_dyn + lay.bc1());
+    uint8_t *st_dg = s_dyn + lay.dg();
+    uint8_t *st_dir = s_dyn + lay.dirs();
+    uint2 *list = glist ? glist + (size_t)blockIdx.x * cap : reinterpret_cast<uint2 *>(s_dyn + (STAGE ? lay.list() : 0));
+
     build_face_table_a(s_table);
     build_dir_table(s_dir, s.g);
     if (threadIdx.x < 16) s_forbid[threadIdx.x] = s.bonds.forbidden[threadIdx.x];
@@ -257,8 +286,15 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
         }
         s_after[threadIdx.x] = bits;
     }
-    if (threadIdx.x == 0) s_count = 0;
+    if (threadIdx.x == 0) {
+        s_cnt[0] = s_cnt[1] = 0;
+        if (STAGE) {
+            mbar_init(&s_mbar, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+    }
     unsigned int target = 0; /* counting barrier: arrivals expected so far */
+    uint32_t mphase = 0;      /* parity of the staging mbarrier */
     __syncthreads();
 
     unsigned long long *lat = reinterpret_cast<unsigned long long *>(s.lat);
@@ -278,27 +314,49 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
     for (uint32_t k = k0; k < k1; ++k) {
         const Substep d = sched[k];
         const Species sp = s.spec[d.species];
+        const uint32_t lo = (uint32_t)(((uint64_t)sp.n * blockIdx.x) / gridDim.x);
+        const uint32_t hi = (uint32_t)(((uint64_t)sp.n * (blockIdx.x + 1)) / gridDim.x);
+        const uint32_t wlo = lo & ~15u;
+        unsigned int &cnt = s_cnt[k & 1u];
+
+        if (STAGE && threadIdx.x == 0) {
+            /* stage this CTA's segments of the slab: all copies in flight at once */
+            const uint32_t wn = ((hi + 15u) & ~15u) - wlo;
+            const uint32_t rows = maxdeg < 2 ? maxdeg : 2u;
+            fence_proxy_async();
+            mbar_arrive_expect_tx(&s_mbar, wn * (4u + 1u + 2u * rows));
+            bulk_g2s(st_pos, pos + sp.off + wlo, wn * 4u, &s_mbar);
+            bulk_g2s(st_dg, deg + sp.off + wlo, wn, &s_mbar);
+            if (rows > 0) bulk_g2s(st_bc0, bcode + sp.off + wlo, wn * 2u, &s_mbar);
+            if (rows > 1) bulk_g2s(st_bc1, bcode + (size_t)npad + sp.off + wlo, wn * 2u, &s_mbar);
+        }
         /* zero the target words this CTA's candidates set in the previous substep */
         if (havePrev) {
             unsigned long long *tp = tmp + (size_t)prevBuf * words;
-            const unsigned int cnt = s_count;
-            for (uint32_t j = threadIdx.x; j < cnt; j += blockDim.x) {
+            const unsigned int pc = s_cnt[(k - 1u) & 1u];
+            for (uint32_t j = threadIdx.x; j < pc; j += blockDim.x) {
                 const uint2 e = list[j];
                 const int dir = (int)(e.x >> 28);
                 tp[dstep(e.y, dir, s_dir[dir]) >> 6] = 0ull;
             }
         }
+        if (STAGE) {
+            /* directions of all items while the copies are in flight */
+            for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x)
+                st_dir[i - wlo] = (uint8_t)direction(draw<RNG>(d.seed, d.iter, i));
+        }
+        if (threadIdx.x == 0) cnt = 0;
         __syncthreads();
-        if (threadIdx.x == 0) s_count = 0;
-        __syncthreads();
+        if (STAGE) {
+            if (!mbar_wait_bounded(&s_mbar, mphase, timeoutNs)) atomicExch(&bar->err, 1u);
+            mphase ^= 1u;
+        }
 
         /* phase A: check this CTA's contiguous range [lo, hi) of the slab */
         unsigned long long *tb = tmp + (size_t)d.buf * words;
-        const uint32_t lo = (uint32_t)(((uint64_t)sp.n * blockIdx.x) / gridDim.x);
-        const uint32_t hi = (uint32_t)(((uint64_t)sp.n * (blockIdx.x + 1)) / gridDim.x);
         uint32_t i = lo + threadIdx.x;
         uint32_t nr0 = 0, ndg = 0, na = 0, nb = 0;
-        if (i < hi) {
+        if (!STAGE && i < hi) {
             const uint32_t slot = sp.off + i;
             nr0 = pos[slot];
             ndg = deg[slot];
@@ -311,25 +369,38 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
             }
         }
         for (uint32_t base = lo; base < hi; base += blockDim.x, i += blockDim.x) {
-            const uint32_t r0 = nr0, dg = ndg, ea = na, eb = nb;
             const bool valid = i < hi;
-            const uint32_t inext = i + blockDim.x;
-            if (inext < hi) {
-                const uint32_t slot = sp.off + inext;
-                nr0 = pos[slot];
-                ndg = deg[slot];
-                if (STORED) {
-                    na = maxdeg > 0 ? bcode[slot] : 0u;
-                    nb = maxdeg > 1 ? bcode[(size_t)npad + slot] : 0u;
-                } else {
-                    na = maxdeg > 0 ? nbr[slot] : 0u;
-                    nb = maxdeg > 1 ? nbr[(size_t)npad + slot] : 0u;
+            uint32_t r0, dg, ea, eb;
+            int dir = 0;
+            if (STAGE) {
+                const uint32_t w = valid ? i - wlo : 0u;
+                r0 = st_pos[w];
+                dg = st_dg[w];
+                ea = maxdeg > 0 ? st_bc0[w] : 0u;
+                eb = maxdeg > 1 ? st_bc1[w] : 0u;
+                dir = st_dir[w];
+            } else {
+                r0 = nr0;
+                dg = ndg;
+                ea = na;
+                eb = nb;
+                const uint32_t inext = i + blockDim.x;
+                if (inext < hi) {
+                    const uint32_t slot = sp.off + inext;
+                    nr0 = pos[slot];
+                    ndg = deg[slot];
+                    if (STORED) {
+                        na = maxdeg > 0 ? bcode[slot] : 0u;
+                        nb = maxdeg > 1 ? bcode[(size_t)npad + slot] : 0u;
+                    } else {
+                        na = maxdeg > 0 ? nbr[slot] : 0u;
+                        nb = maxdeg > 1 ? nbr[(size_t)npad + slot] : 0u;
+                    }
                 }
             }
             bool ok = false;
-            int dir = 0;
             if (valid) {
-                dir = direction(draw<RNG>(d.seed, d.iter, i));
+                if (!STAGE) dir = direction(draw<RNG>(d.seed, d.iter, i));
                 const DirConst dc = s_dir[dir];
                 const Face4 f = face4d(r0, dir, dc, s_table);
                 const uint32_t r1 = dstep(r0, dir, dc);
@@ -365,7 +436,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
             if (m) {
                 const int leader = __ffs(m) - 1;
                 unsigned int at = 0;
-                if ((int)lane == leader) at = atomicAdd(&s_count, (unsigned int)__popc(m));
+                if ((int)lane == leader) at = atomicAdd(&cnt, (unsigned int)__popc(m));
                 at = __shfl_sync(0xFFFFFFFFu, at, leader);
                 if (ok) list[at + __popc(m & ((1u << lane) - 1u))] = make_uint2((sp.off + i) | ((uint32_t)dir << 28), r0);
             }
@@ -379,14 +450,29 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
         /* phase B: perform, this CTA's candidates only */
         {
             const unsigned long long *tr = tmp + (size_t)d.buf * words;
-            const unsigned int cnt = s_count;
-            for (uint32_t j = threadIdx.x; j < cnt; j += blockDim.x) {
+            const unsigned int cc = cnt;
+            for (uint32_t j = threadIdx.x; j < cc; j += blockDim.x) {
                 const uint2 e = list[j];
                 const int dir = (int)(e.x >> 28);
                 const uint32_t slot = e.x & 0x0FFFFFFFu;
                 const uint32_t r0 = e.y;
                 const DirConst dc = s_dir[dir];
                 const Face4 f = face4d(r0, dir, dc, s_table);
+                /* bond data of a possible move, loaded together with the probe */
+                uint32_t dgm = 0, q0 = 0, q1 = 0, v0 = 0, v1 = 0, c0 = 0, c1 = 0;
+                if (STORED) {
+                    dgm = deg[slot];
+                    if (maxdeg > 0) {
+                        q0 = nbr[slot];
+                        v0 = s.rev[slot];
+                        c0 = bcode[slot];
+                    }
+                    if (maxdeg > 1) {
+                        q1 = nbr[(size_t)npad + slot];
+                        v1 = s.rev[(size_t)npad + slot];
+                        c1 = bcode[(size_t)npad + slot];
+                    }
+                }
                 if (face4_occupied(tr, f)) continue;
                 const uint32_t r1 = dstep(r0, dir, dc);
                 const uint32_t w0 = r0 >> 6, w1 = r1 >> 6;
@@ -404,22 +490,17 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
                 if (STORED) {
                     /* own bonds: (q - r0) -> (q - r1); the partner's bond back is
                      * always the per-axis negation, so it is written, not read */
-                    const uint32_t dg = deg[slot];
-                    const size_t o0 = slot, o1 = (size_t)npad + slot;
-                    const uint32_t q0 = maxdeg > 0 ? nbr[o0] : 0u, q1 = maxdeg > 1 ? nbr[o1] : 0u;
-                    const uint32_t v0 = maxdeg > 0 ? s.rev[o0] : 0u, v1 = maxdeg > 1 ? s.rev[o1] : 0u;
-                    const uint32_t c0 = maxdeg > 0 ? bcode[o0] : 0u, c1 = maxdeg > 1 ? bcode[o1] : 0u;
-                    if (dg > 0) {
+                    if (dgm > 0) {
                         const uint32_t nc = (dir & 1) ? bcode_dec(c0, ax) : bcode_inc(c0, ax);
-                        bcode[o0] = (uint16_t)nc;
+                        bcode[slot] = (uint16_t)nc;
                         bcode[(size_t)v0 * npad + q0] = (uint16_t)bcode_neg(nc);
                     }
-                    if (dg > 1) {
+                    if (dgm > 1) {
                         const uint32_t nc = (dir & 1) ? bcode_dec(c1, ax) : bcode_inc(c1, ax);
-                        bcode[o1] = (uint16_t)nc;
+                        bcode[(size_t)npad + slot] = (uint16_t)nc;
                         bcode[(size_t)v1 * npad + q1] = (uint16_t)bcode_neg(nc);
                     }
-                    for (uint32_t b = 2; b < dg; ++b) {
+                    for (uint32_t b = 2; b < dgm; ++b) {
                         const size_t own = (size_t)b * npad + slot;
                         const uint32_t nc = (dir & 1) ? bcode_dec(bcode[own], ax) : bcode_inc(bcode[own], ax);
                         bcode[own] = (uint16_t)nc;
@@ -440,8 +521,8 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
      * next launch starts from clean target lattices */
     if (alive && havePrev) {
         unsigned long long *tp = tmp + (size_t)prevBuf * words;
-        const unsigned int cnt = s_count;
-        for (uint32_t j = threadIdx.x; j < cnt; j += blockDim.x) {
+        const unsigned int pc = s_cnt[(k1 - 1u) & 1u];
+        for (uint32_t j = threadIdx.x; j < pc; j += blockDim.x) {
             const uint2 e = list[j];
             const int dir = (int)(e.x >> 28);
             tp[dstep(e.y, dir, s_dir[dir]) >> 6] = 0ull;
@@ -921,38 +1002,65 @@ struct Engine {
      * cooperative launch needs them all resident); each CTA's candidate
      * list holds its worst case (every monomer it checks is a candidate),
      * in shared memory when that fits. */
-    template <int RNG, bool STORED>
-    void configureFor(int smCount)
+    int sweepMode = 0;
+    uint32_t sweepWindow = 0;
+
+    /* Persistent-kernel launch shape: one CTA per SM (cooperative launch,
+     * all CTAs resident); each CTA owns 1/grid of every colour slab.  The
+     * candidate list holds the CTA's worst case (every monomer a candidate).
+     * Staged mode when the CTA's segments and list fit in shared memory. */
+    template <int RNG, int MODE>
+    bool configureFor(int smCount, size_t smemLimit)
     {
         int blocks = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_sweep<RNG, MODE>, kSweepThreads, 0));
+        if (blocks < 1) throw std::runtime_error("persistent sweep kernel does not fit on an SM");
+        const uint32_t grid = (uint32_t)smCount; /* one CTA per SM */
+        const uint32_t per = (nmax + grid - 1) / grid + 1u;
+        const uint32_t cap = std::max<uint32_t>(32u, per);
+        const uint32_t W = ((per + 15u) & ~15u) + 32u;
         size_t smem = 0;
-        uint32_t cap = 0;
-        for (int pass = 0; pass < 2; ++pass) {
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_sweep<RNG, STORED>, kSweepThreads, smem));
-            if (blocks < 1) throw std::runtime_error("persistent sweep kernel does not fit on an SM");
-            const uint32_t grid = (uint32_t)(blocks * smCount);
-            cap = std::max<uint32_t>(32u, (nmax + grid - 1) / grid + 1u);
-            const size_t want = cap * sizeof(uint2) <= kSweepSmemListMax ? cap * sizeof(uint2) : 0;
-            if (want == smem) break;
-            smem = want;
+        if (MODE == SWEEP_STAGED) {
+            smem = StageLayout{W}.bytes(cap);
+            if (smem > smemLimit) return false;
+        } else {
+            smem = (size_t)cap * sizeof(uint2) <= kSweepSmemListMax ? (size_t)cap * sizeof(uint2) : 0;
         }
-        sweepGrid = blocks * smCount;
+        if (smem > 0) CK(cudaFuncSetAttribute(k_sweep<RNG, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int fit = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k_sweep<RNG, MODE>, kSweepThreads, smem));
+        if (fit < 1) return false;
+        sweepGrid = (int)grid;
         sweepCap = cap;
         sweepSmem = smem;
-        if (smem > 0)
-            CK(cudaFuncSetAttribute(k_sweep<RNG, STORED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        sweepWindow = W;
+        sweepMode = MODE;
+        return true;
+    }
+
+    template <int RNG>
+    void configureRng(int smCount, size_t smemLimit)
+    {
+        if (storedBonds) {
+            if (configureFor<RNG, SWEEP_STAGED>(smCount, smemLimit)) return;
+            if (configureFor<RNG, SWEEP_STORED>(smCount, smemLimit)) return;
+        }
+        if (!configureFor<RNG, SWEEP_GATHER>(smCount, smemLimit))
+            throw std::runtime_error("persistent sweep kernel does not fit on an SM");
     }
 
     void configureSweep()
     {
-        int dev = 0, sms = 0;
+        int dev = 0, sms = 0, optin = 0;
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
         if (npad >= (1u << 28)) throw std::runtime_error("more than 2^28 monomer slots are not supported");
+        const size_t limit = (size_t)optin > 16384 ? (size_t)optin - 16384 : (size_t)optin; /* room for the static tables */
         if (rng == BFM_RNG_SARU)
-            storedBonds ? configureFor<RNG_SARU, true>(sms) : configureFor<RNG_SARU, false>(sms);
+            configureRng<RNG_SARU>(sms, limit);
         else
-            storedBonds ? configureFor<RNG_INTHASH, true>(sms) : configureFor<RNG_INTHASH, false>(sms);
+            configureRng<RNG_INTHASH>(sms, limit);
         dfree(d_glist);
         if (sweepSmem == 0) dalloc(d_glist, (size_t)sweepGrid * sweepCap);
     }
@@ -965,11 +1073,18 @@ struct Engine {
         GridBarrier *bar = d_bar;
         unsigned long long to = timeoutNs;
         uint32_t md = maxdeg;
-        void *args[] = {&s, (void *)&sched, &k0, &k1, &bar, &gl, &cap, &to, &md};
+        uint32_t win = sweepWindow;
+        void *args[] = {&s, (void *)&sched, &k0, &k1, &bar, &gl, &cap, &to, &md, &win};
         CK(cudaMemsetAsync(d_bar, 0, sizeof(GridBarrier), stream)); /* the counting barrier starts at 0 */
-        const void *fn = rng == BFM_RNG_SARU
-                             ? (storedBonds ? (const void *)k_sweep<RNG_SARU, true> : (const void *)k_sweep<RNG_SARU, false>)
-                             : (storedBonds ? (const void *)k_sweep<RNG_INTHASH, true> : (const void *)k_sweep<RNG_INTHASH, false>);
+        const void *fn = nullptr;
+        if (rng == BFM_RNG_SARU)
+            fn = sweepMode == SWEEP_STAGED ? (const void *)k_sweep<RNG_SARU, SWEEP_STAGED>
+                 : sweepMode == SWEEP_STORED ? (const void *)k_sweep<RNG_SARU, SWEEP_STORED>
+                                             : (const void *)k_sweep<RNG_SARU, SWEEP_GATHER>;
+        else
+            fn = sweepMode == SWEEP_STAGED ? (const void *)k_sweep<RNG_INTHASH, SWEEP_STAGED>
+                 : sweepMode == SWEEP_STORED ? (const void *)k_sweep<RNG_INTHASH, SWEEP_STORED>
+                                             : (const void *)k_sweep<RNG_INTHASH, SWEEP_GATHER>;
         CK(cudaLaunchCooperativeKernel(fn, dim3(sweepGrid), dim3(kSweepThreads), args, sweepSmem, stream));
     }
 
@@ -1609,6 +1724,17 @@ int bfm_time_kernels(bfm_handle *h, uint32_t nmcs, double *ms, uint64_t *launche
         if (!ms || !launches || !attempts) throw InvalidArgument("null output pointer");
         h->e.timeKernels(nmcs, ms, launches, attempts);
     });
+}
+
+int bfm_get_launch_info(const bfm_handle *h, int *mode, int *grid, int *threads, size_t *smem_bytes)
+{
+    if (!h) return BFM_EINVAL;
+    if (!h->e.initialized) return BFM_ENOTINIT;
+    if (mode) *mode = h->e.launchMode == 0 ? h->e.sweepMode : -h->e.launchMode;
+    if (grid) *grid = h->e.sweepGrid;
+    if (threads) *threads = kSweepThreads;
+    if (smem_bytes) *smem_bytes = h->e.sweepSmem;
+    return BFM_OK;
 }
 
 int bfm_set_barrier_timeout_ms(bfm_handle *h, uint32_t ms)

@@ -136,6 +136,59 @@ __device__ __forceinline__ bool grid_barrier_count(GridBarrier *bar, unsigned in
     return s_ok2 != 0;
 }
 
+/* ---- bulk (TMA) copies global -> shared on an mbarrier ------------------ */
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+/* 1-D bulk copy: dst, src 16-byte aligned, bytes a multiple of 16 */
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, unsigned long long *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(done)
+                 : "r"(smem_addr(bar)), "r"(parity)
+                 : "memory");
+    return done != 0;
+}
+
+/* generic-proxy accesses before, async-proxy (bulk copy) accesses after */
+__device__ __forceinline__ void fence_proxy_async()
+{
+    asm volatile("fence.proxy.async;" ::: "memory");
+}
+
+/* wait for the phase `parity` of the mbarrier with a bound; false on timeout */
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, uint32_t parity, unsigned long long timeoutNs)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    for (unsigned int polls = 0; polls < kBarrierMaxPolls; ++polls) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > timeoutNs) return false;
+    }
+    return false;
+}
+
 /* Face-mask table: for a move along axis a and the low two bits lb, lc of the
  * first transverse values (b-1, c-1), the masks of the nine face sites in the
  * (up to) four bricks, with the move axis' own bits still zero.  Entry

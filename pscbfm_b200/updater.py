@@ -230,6 +230,13 @@ class UpdaterGPUScBFM_AB_Type:
         self._check(self._lib.bfm_time_kernels(self._h, int(nmcs), ctypes.byref(ms), ctypes.byref(n), ctypes.byref(a)))
         return ms.value, n.value, a.value
 
+    def getLaunchInfo(self) -> dict:
+        """Shape of the persistent kernel: bond mode (0 gather, 1 stored, 2 staged),
+        CTAs, threads per CTA, dynamic shared memory per CTA."""
+        m, g, t, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_size_t()
+        self._check(self._lib.bfm_get_launch_info(self._h, ctypes.byref(m), ctypes.byref(g), ctypes.byref(t), ctypes.byref(b)))
+        return {"mode": m.value, "ctas": g.value, "threads": t.value, "smem_bytes": b.value}
+
     def setBarrierTimeoutMs(self, ms: int):
         self._check(self._lib.bfm_set_barrier_timeout_ms(self._h, int(ms)))
 
