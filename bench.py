@@ -57,19 +57,28 @@ def parse():
 
 # ------------------------------------------------------------------ ranks
 class Ranks:
-    def __init__(self):
+    """One process per GPU (torchrun environment); NCCL on GPUs, gloo on CPU.
+    Only the timing reductions cross ranks: every replica is independent."""
+
+    def __init__(self, backend: str | None = None):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.device = None
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                    device_id=torch.device("cuda", self.local))
+            if backend is None:
+                backend = "nccl" if torch.cuda.is_available() else "gloo"
+            kw = {}
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+                self.device = torch.device("cuda", self.local)
+                kw["device_id"] = self.device
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120), **kw)
             self.pg = dist
 
     def barrier(self):
@@ -80,13 +89,22 @@ class Ranks:
         if not self.pg:
             return v
         import torch
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
+        t = torch.tensor([v], dtype=torch.float64, device=self.device or "cpu")
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
     def close(self):
         if self.pg:
             self.pg.destroy_process_group()
+
+
+def aggregate(ranks, attempts: int, dev_s: float, e2e_s: float):
+    """Whole-job throughput of independent replicas: the attempts of all
+    ranks over the slowest rank's time (device-timed and end-to-end)."""
+    dev = ranks.max(dev_s)
+    e2e = ranks.max(e2e_s)
+    total = attempts * ranks.world
+    return total / dev, total / e2e, total
 
 
 # ------------------------------------------------------------------ clocks
@@ -262,11 +280,7 @@ def run_b200(args, ranks):
     acnt1 = u.getCounters()
 
     attempts = acnt1[0] - acnt0[0]
-    dev_s = ranks.max(dev_ms / 1e3)
-    e2e_s = ranks.max(e2e_s)
-    total_attempts = attempts * ranks.world
-    value = total_attempts / dev_s
-    e2e = total_attempts / e2e_s
+    value, e2e, total_attempts = aggregate(ranks, attempts, dev_ms / 1e3, e2e_s)
 
     kbar = float(system.deg.mean())
     b_check, b_perf = algorithmic_bytes(cand, acc, kbar)

@@ -395,6 +395,8 @@ void *orc_sweep_create(uint32_t Lx, uint32_t Ly, uint32_t Lz, uint32_t n, const 
                        int nThreads)
 {
     try {
+        for (uint32_t L : {Lx, Ly, Lz})
+            if (L < 8 || L > 1024 || (L & (L - 1))) return nullptr; /* power-of-two boxes only */
         auto *s = new Sweep();
         s->Lx = Lx; s->Ly = Ly; s->Lz = Lz;
         s->mx = Lx - 1; s->my = Ly - 1; s->mz = Lz - 1;
@@ -492,6 +494,8 @@ static inline uint64_t xs_next(uint64_t &s)
 uint64_t orc_serial_run(uint32_t Lx, uint32_t Ly, uint32_t Lz, uint32_t n, int32_t *pos3, const uint32_t *nnbr,
                         const uint32_t *nbr8, const uint8_t *forbidden512, uint64_t nMCS, uint64_t seed)
 {
+    for (uint32_t L : {Lx, Ly, Lz})
+        if (L < 8 || L > 1024 || (L & (L - 1))) return 0; /* power-of-two boxes only */
     const uint32_t mx = Lx - 1, my = Ly - 1, mz = Lz - 1;
     const uint32_t Lm = std::max(Lx, std::max(Ly, Lz));
     std::vector<uint8_t> lat((size_t)Lm * Lm * Lm, 0);
