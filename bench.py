@@ -293,7 +293,9 @@ def run_b200(args, ranks):
     prof = os.path.join(HERE, "profiles", "k_sweep_melt256_traffic.json")
     if os.path.exists(prof):
         try:
-            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+            # DRAM bytes per attempted move from one ncu capture of a shorter
+            # launch, scaled to this launch's attempted moves
+            traffic = json.load(open(prof))["dram_bytes_per_attempt"] * k_attempts / max(k_launches, 1)
         except Exception:
             traffic = None
     whole_bytes = (b_check + b_perf) * total_attempts / ranks.world

@@ -41,14 +41,28 @@ def _stale() -> bool:
     return False
 
 
+CLI = os.path.join(HERE, "bin", "pscbfm")
+CLI_SOURCES = ["pscbfm_main.cpp", "bfm_io.hpp", "../../include/UpdaterGPUScBFM_AB_Type.h"]
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
-    """Compile the CUDA sources into the in-tree shared library."""
-    if not force and not _stale():
-        return LIBPATH
-    cmd = [NVCC, *NVCC_FLAGS, "-o", LIBPATH] + [os.path.join(CSRC, s) for s in SOURCES]
-    if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True, cwd=CSRC)
+    """Compile the CUDA sources into the in-tree shared library, and the
+    pscbfm command-line simulator against it."""
+    if force or _stale():
+        cmd = [NVCC, *NVCC_FLAGS, "-o", LIBPATH] + [os.path.join(CSRC, s) for s in SOURCES]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True, cwd=CSRC)
+    if force or not os.path.exists(CLI) or any(
+            os.path.getmtime(os.path.join(CSRC, f)) > os.path.getmtime(CLI) for f in CLI_SOURCES) or \
+            os.path.getmtime(LIBPATH) > os.path.getmtime(CLI):
+        os.makedirs(os.path.dirname(CLI), exist_ok=True)
+        cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(REPO, "include"), "-I", CSRC,
+               os.path.join(CSRC, "pscbfm_main.cpp"), "-o", CLI, "-L", HERE, "-lpscbfm_b200",
+               "-Wl,-rpath,$ORIGIN/.."]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True, cwd=CSRC)
     return LIBPATH
 
 
