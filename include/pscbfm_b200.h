@@ -68,7 +68,7 @@ int bfm_set_periodicity(bfm_handle *h, int px, int py, int pz);
 /* setAge / getAge (.h:506-507) */
 int bfm_set_age(bfm_handle *h, int64_t age);
 int bfm_get_age(const bfm_handle *h, int64_t *age);
-/* setRng / getRng (.h:508-509); IntHash (default, as .cu:1407) and Saru */
+/* setRng / getRng (.h:508-509); IntHash (default, as .cu:1407), Saru, Philox */
 int bfm_set_rng(bfm_handle *h, int rng);
 int bfm_get_rng(const bfm_handle *h, int *rng);
 /* setStepsBetweenSortings (.h:513), default 5000 (.cu:1379) */
@@ -121,6 +121,11 @@ int bfm_set_launch_mode(bfm_handle *h, int mode);
  * (negative: -launch path of the per-substep kernels); CTAs, threads per CTA
  * and dynamic shared memory per CTA */
 int bfm_get_launch_info(const bfm_handle *h, int *mode, int *grid, int *threads, size_t *smem_bytes);
+/* force a shape of the persistent kernel (tests, tuning): -1 automatic
+ * (default), 0 gather, 1 stored codes, 2 staged; 3..5 the same with the
+ * candidate lists in global instead of shared memory.  BFM_ERUNTIME when the
+ * shape does not fit this system. */
+int bfm_set_sweep_shape(bfm_handle *h, int shape);
 /* bound of every grid-barrier wait in the persistent kernel (default 2000 ms);
  * a wait that runs out ends the launch and bfm_run returns BFM_ETIMEOUT */
 int bfm_set_barrier_timeout_ms(bfm_handle *h, uint32_t ms);
@@ -167,6 +172,13 @@ int bfm_color_graph(uint32_t n, const uint8_t *deg, const uint32_t *nbr8, int un
 int bfm_substep_noalloc(uint32_t *pos, int32_t *img, const uint32_t *nbr, const uint8_t *deg, uint32_t npad,
                         uint32_t *lattice, uint32_t box_x, uint32_t box_y, uint32_t box_z, const uint8_t *allowed512,
                         uint32_t slot_offset, uint32_t count, uint32_t seed, uint32_t iteration, int rng, void *stream);
+
+/* Diagnostic: for k < n, out_pairs[2k] = the library's Philox4x32-10 word at
+ * (seed, subsequence, offset + k) and out_pairs[2k+1] = curand() after
+ * curand_init(seed, subsequence, offset + k) on the GPU, the generator the
+ * reference's Philox option uses (rngs/lemonade_philox.h:48-56). */
+int bfm_debug_philox_vs_curand(int gpu, uint64_t seed, uint64_t subsequence, uint64_t offset, uint32_t n,
+                               uint32_t *out_pairs);
 
 /* Process-global R250 colour/seed generator, the counterpart of LeMonADE's
  * RandomNumberGenerators whose r250_rand32() the reference calls

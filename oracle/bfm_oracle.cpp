@@ -82,6 +82,30 @@ static inline uint32_t hash_rng(uint32_t seed, uint32_t subseq)
 
 enum { RNG_INTHASH = 1, RNG_SARU = 2, RNG_PHILOX = 3 };
 
+/* Philox4x32-10 (Salmon et al., SC'11, the Random123 constants), the word
+ * curand() returns after curand_init(seed, subsequence, offset) -- the use
+ * in rngs/lemonade_philox.h:48-56: block counter (offset/4) + subsequence *
+ * 2^64, key = seed, word offset % 4.  Pinned against curand on the GPU. */
+static inline uint32_t philox4x32_10(uint64_t seed, uint64_t subsequence, uint64_t offset)
+{
+    const uint64_t blk = offset >> 2;
+    uint32_t c[4] = {(uint32_t)blk, (uint32_t)(blk >> 32), (uint32_t)subsequence, (uint32_t)(subsequence >> 32)};
+    uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0;
+        const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
+        c[0] = n0;
+        c[1] = (uint32_t)p1;
+        c[2] = n2;
+        c[3] = (uint32_t)p0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c[offset & 3];
+}
+
 /* ---------------------------------------------------------- Z-order index */
 
 /* 10-bit -> 30-bit dilation with two zero bits between payload bits.  Equal to
@@ -268,6 +292,7 @@ struct Sweep {
     uint32_t draw(uint32_t seed, uint64_t iteration, uint32_t local) const
     {
         if (rng == RNG_INTHASH) return hash_rng(seed, local);
+        if (rng == RNG_PHILOX) return philox4x32_10(seed, local, iteration);
         return saru_u32(seed, (uint32_t)iteration, local);
     }
 
@@ -346,6 +371,7 @@ extern "C" {
 
 uint32_t orc_saru(uint32_t seed, uint32_t iteration, uint32_t subseq) { return saru_u32(seed, iteration, subseq); }
 uint32_t orc_hash_rng(uint32_t seed, uint32_t subseq) { return hash_rng(seed, subseq); }
+uint32_t orc_philox(uint64_t seed, uint64_t subseq, uint64_t offset) { return philox4x32_10(seed, subseq, offset); }
 uint32_t orc_zindex(int64_t x, int64_t y, int64_t z, uint32_t mx, uint32_t my, uint32_t mz) { return zindex(x, y, z, mx, my, mz); }
 
 void orc_r250_seed_u64(uint32_t *state251, uint64_t seed)

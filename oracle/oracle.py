@@ -45,6 +45,8 @@ def orc() -> ctypes.CDLL:
         L.orc_saru.argtypes = [_c.c_uint32] * 3
         L.orc_hash_rng.restype = _c.c_uint32
         L.orc_hash_rng.argtypes = [_c.c_uint32] * 2
+        L.orc_philox.restype = _c.c_uint32
+        L.orc_philox.argtypes = [_c.c_uint64] * 3
         L.orc_zindex.restype = _c.c_uint32
         L.orc_zindex.argtypes = [_c.c_int64] * 3 + [_c.c_uint32] * 3
         L.orc_r250_seed_u64.argtypes = [_P, _c.c_uint64]

@@ -18,7 +18,7 @@ LIBNAME = "libpscbfm_b200.so"
 LIBPATH = os.path.join(HERE, LIBNAME)
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["bfm_engine.cu"]
+SOURCES = ["bfm_engine.cu", "bfm_diag.cu"]
 HEADERS = ["bfm_device.cuh", "bfm_host.hpp", "bfm_sweep.cuh", "../../include/pscbfm_b200.h"]
 
 NVCC_FLAGS = [
@@ -109,6 +109,7 @@ _SIGS = {
     "bfm_set_launch_mode": (_c.c_int, [_P, _c.c_int]),
     "bfm_time_kernels": (_c.c_int, [_P, _c.c_uint32, _c.POINTER(_c.c_double), _c.POINTER(_c.c_uint64), _c.POINTER(_c.c_uint64)]),
     "bfm_set_barrier_timeout_ms": (_c.c_int, [_P, _c.c_uint32]),
+    "bfm_set_sweep_shape": (_c.c_int, [_P, _c.c_int]),
     "bfm_get_launch_info": (_c.c_int, [_P, _c.POINTER(_c.c_int), _c.POINTER(_c.c_int), _c.POINTER(_c.c_int),
                                        _c.POINTER(_c.c_size_t)]),
     "bfm_barrier_selftest": (_c.c_int, [_c.c_int, _c.c_uint32, _c.c_uint32, _c.c_uint32, _c.POINTER(_c.c_double)]),
@@ -117,6 +118,7 @@ _SIGS = {
     "bfm_color_graph": (_c.c_int, [_c.c_uint32, _P, _P, _c.c_int, _P, _P]),
     "bfm_substep_noalloc": (_c.c_int, [_P, _P, _P, _P, _c.c_uint32, _P, _c.c_uint32, _c.c_uint32, _c.c_uint32, _P,
                                        _c.c_uint32, _c.c_uint32, _c.c_uint32, _c.c_uint32, _c.c_int, _P]),
+    "bfm_debug_philox_vs_curand": (_c.c_int, [_c.c_int, _c.c_uint64, _c.c_uint64, _c.c_uint64, _c.c_uint32, _P]),
     "bfm_r250_seed": (_c.c_int, [_c.c_uint64]),
     "bfm_r250_seed_words": (_c.c_int, [_P, _c.c_size_t]),
     "bfm_r250_get_state": (_c.c_int, [_P]),

@@ -199,10 +199,48 @@ __host__ __device__ inline uint32_t jhash(uint32_t a)
     return a;
 }
 
+/* 32x32 -> 64-bit product, high half */
+__host__ __device__ inline uint32_t mulhi32(uint32_t a, uint32_t b)
+{
+#ifdef __CUDA_ARCH__
+    return __umulhi(a, b);
+#else
+    return (uint32_t)(((uint64_t)a * b) >> 32);
+#endif
+}
+
+/* Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11): ten rounds of two
+ * 32x32 multiplications with the Weyl key schedule.  Output word
+ * (offset & 3) of the block at counter (offset / 4) + subsequence * 2^64 and
+ * key = seed, the stream position of a generator set up with
+ * curand_init(seed, subsequence, offset), as rngs/lemonade_philox.h:48-56 of
+ * the reference does (checked against curand's own outputs). */
+__host__ __device__ inline uint32_t philox_word(uint64_t seed, uint64_t subsequence, uint64_t offset)
+{
+    const uint64_t blk = offset >> 2;
+    uint32_t c0 = (uint32_t)blk, c1 = (uint32_t)(blk >> 32), c2 = (uint32_t)subsequence, c3 = (uint32_t)(subsequence >> 32);
+    uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t lo0 = 0xD2511F53u * c0, hi0 = mulhi32(0xD2511F53u, c0);
+        const uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = mulhi32(0xCD9E8D57u, c2);
+        const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0;
+        c1 = lo1;
+        c2 = n2;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    const uint32_t w = (uint32_t)(offset & 3u);
+    return w == 0 ? c0 : (w == 1 ? c1 : (w == 2 ? c2 : c3));
+}
+
 template <int RNG>
-__host__ __device__ inline uint32_t draw(uint32_t seed, uint32_t iteration, uint32_t local)
+__host__ __device__ inline uint32_t draw(uint32_t seed, uint32_t iteration, uint32_t local, uint32_t iterationHi = 0)
 {
     if (RNG == RNG_INTHASH) return jhash(jhash(local) ^ seed);
+    if (RNG == RNG_PHILOX) return philox_word(seed, local, ((uint64_t)iterationHi << 32) | iteration);
     return saru(seed, iteration, local);
 }
 

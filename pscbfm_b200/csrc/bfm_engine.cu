@@ -57,10 +57,11 @@ struct Species {
 
 /* one colour substep, as drawn by the host */
 struct Substep {
-    uint32_t species;
+    uint16_t species;
+    uint16_t buf;    /* temporary lattice buffer used by this substep */
     uint32_t seed;
-    uint32_t iter;   /* RNG iteration = currentAge truncated to 32 bit (.cu:3049) */
-    uint32_t buf;    /* temporary lattice buffer used by this substep */
+    uint32_t iter;   /* RNG iteration = currentAge (.cu:3049), low 32 bits (all Saru uses) */
+    uint32_t iterHi; /* high 32 bits, for Philox whose offset is the full 64-bit age */
 };
 
 struct Bondset {
@@ -128,7 +129,7 @@ __global__ void __launch_bounds__(kThreads) k_check(Sys s, const Substep *__rest
         if (i < sp.n) {
             const uint32_t slot = sp.off + i;
             const uint32_t r0 = s.pos[slot];
-            const int dir = direction(draw<RNG>(d.seed, d.iter, i));
+            const int dir = direction(draw<RNG>(d.seed, d.iter, i, d.iterHi));
             const uint32_t r1 = zstep(r0, dir, s.g);
             const uint32_t nb = s.deg[slot];
             bool ok = true;
@@ -343,7 +344,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
         if (STAGE) {
             /* directions of all items while the copies are in flight */
             for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x)
-                st_dir[i - wlo] = (uint8_t)direction(draw<RNG>(d.seed, d.iter, i));
+                st_dir[i - wlo] = (uint8_t)direction(draw<RNG>(d.seed, d.iter, i, d.iterHi));
         }
         if (threadIdx.x == 0) cnt = 0;
         __syncthreads();
@@ -400,7 +401,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
             }
             bool ok = false;
             if (valid) {
-                if (!STAGE) dir = direction(draw<RNG>(d.seed, d.iter, i));
+                if (!STAGE) dir = direction(draw<RNG>(d.seed, d.iter, i, d.iterHi));
                 const DirConst dc = s_dir[dir];
                 const Face4 f = face4d(r0, dir, dc, s_table);
                 const uint32_t r1 = dstep(r0, dir, dc);
@@ -798,8 +799,9 @@ struct Engine {
             if (L[a] == 0) throw std::runtime_error("setLatticeSize must be called before initialize");
             if (!periodic[a]) throw std::runtime_error("only fully periodic boxes are supported by this build");
         }
-        if (rng != BFM_RNG_INTHASH && rng != BFM_RNG_SARU)
-            throw std::runtime_error("random number generator " + std::to_string(rng) + " is not provided by this build (IntHash = 1, Saru = 2)");
+        if (rng != BFM_RNG_INTHASH && rng != BFM_RNG_SARU && rng != BFM_RNG_PHILOX)
+            throw std::runtime_error("random number generator " + std::to_string(rng) +
+                                     " is not provided by this build (IntHash = 1, Saru = 2, Philox = 3)");
         /* initializeBondTable (.cu:1516-1559): exactly 108 allowed bonds */
         unsigned nAllowed = 0;
         for (int i = 0; i < 512; ++i) nAllowed += forbidden[i] ? 0 : 1;
@@ -1004,6 +1006,7 @@ struct Engine {
      * in shared memory when that fits. */
     int sweepMode = 0;
     uint32_t sweepWindow = 0;
+    int forcedShape = -1; /* -1 automatic; 0..2 bond mode; +3: candidate lists in global memory */
 
     /* Persistent-kernel launch shape: one CTA per SM (cooperative launch,
      * all CTAs resident); each CTA owns 1/grid of every colour slab.  The
@@ -1020,11 +1023,13 @@ struct Engine {
         const uint32_t cap = std::max<uint32_t>(32u, per);
         const uint32_t W = ((per + 15u) & ~15u) + 32u;
         size_t smem = 0;
+        const bool globalList = forcedShape >= 3;
         if (MODE == SWEEP_STAGED) {
+            if (globalList) return false;
             smem = StageLayout{W}.bytes(cap);
             if (smem > smemLimit) return false;
         } else {
-            smem = (size_t)cap * sizeof(uint2) <= kSweepSmemListMax ? (size_t)cap * sizeof(uint2) : 0;
+            smem = !globalList && (size_t)cap * sizeof(uint2) <= kSweepSmemListMax ? (size_t)cap * sizeof(uint2) : 0;
         }
         if (smem > 0) CK(cudaFuncSetAttribute(k_sweep<RNG, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int fit = 0;
@@ -1041,6 +1046,15 @@ struct Engine {
     template <int RNG>
     void configureRng(int smCount, size_t smemLimit)
     {
+        if (forcedShape >= 0) {
+            const int m = forcedShape % 3;
+            bool ok = false;
+            if (m == SWEEP_STAGED && storedBonds) ok = configureFor<RNG, SWEEP_STAGED>(smCount, smemLimit);
+            else if (m == SWEEP_STORED && storedBonds) ok = configureFor<RNG, SWEEP_STORED>(smCount, smemLimit);
+            else if (m == SWEEP_GATHER) ok = configureFor<RNG, SWEEP_GATHER>(smCount, smemLimit);
+            if (!ok) throw std::runtime_error("the requested persistent-kernel shape is not available for this system");
+            return;
+        }
         if (storedBonds) {
             if (configureFor<RNG, SWEEP_STAGED>(smCount, smemLimit)) return;
             if (configureFor<RNG, SWEEP_STORED>(smCount, smemLimit)) return;
@@ -1059,6 +1073,8 @@ struct Engine {
         const size_t limit = (size_t)optin > 16384 ? (size_t)optin - 16384 : (size_t)optin; /* room for the static tables */
         if (rng == BFM_RNG_SARU)
             configureRng<RNG_SARU>(sms, limit);
+        else if (rng == BFM_RNG_PHILOX)
+            configureRng<RNG_PHILOX>(sms, limit);
         else
             configureRng<RNG_INTHASH>(sms, limit);
         dfree(d_glist);
@@ -1081,6 +1097,10 @@ struct Engine {
             fn = sweepMode == SWEEP_STAGED ? (const void *)k_sweep<RNG_SARU, SWEEP_STAGED>
                  : sweepMode == SWEEP_STORED ? (const void *)k_sweep<RNG_SARU, SWEEP_STORED>
                                              : (const void *)k_sweep<RNG_SARU, SWEEP_GATHER>;
+        else if (rng == BFM_RNG_PHILOX)
+            fn = sweepMode == SWEEP_STAGED ? (const void *)k_sweep<RNG_PHILOX, SWEEP_STAGED>
+                 : sweepMode == SWEEP_STORED ? (const void *)k_sweep<RNG_PHILOX, SWEEP_STORED>
+                                             : (const void *)k_sweep<RNG_PHILOX, SWEEP_GATHER>;
         else
             fn = sweepMode == SWEEP_STAGED ? (const void *)k_sweep<RNG_INTHASH, SWEEP_STAGED>
                  : sweepMode == SWEEP_STORED ? (const void *)k_sweep<RNG_INTHASH, SWEEP_STORED>
@@ -1148,6 +1168,8 @@ struct Engine {
         profMark();
         if (rng == BFM_RNG_SARU)
             k_check<RNG_SARU><<<checkBlocks(), kThreads, 0, stream>>>(s, sched, k);
+        else if (rng == BFM_RNG_PHILOX)
+            k_check<RNG_PHILOX><<<checkBlocks(), kThreads, 0, stream>>>(s, sched, k);
         else
             k_check<RNG_INTHASH><<<checkBlocks(), kThreads, 0, stream>>>(s, sched, k);
         profMark();
@@ -1235,10 +1257,11 @@ struct Engine {
                 for (uint32_t sub = 0; sub < nSpecies; ++sub) {
                     Substep &d = hs[m++];
                     const uint64_t currentAge = (uint64_t)a + (uint64_t)iStep * nSpecies + sub; /* .cu:3049 */
-                    d.species = (uint32_t)((uint64_t)r250.next() % nSpecies);                /* .cu:3065 */
+                    d.species = (uint16_t)((uint64_t)r250.next() % nSpecies);                /* .cu:3065 */
                     d.seed = r250.next();                                                    /* .cu:3066 */
                     d.iter = (uint32_t)currentAge;
-                    d.buf = (uint32_t)(substepCounter++ & 1u);
+                    d.iterHi = (uint32_t)(currentAge >> 32);
+                    d.buf = (uint16_t)(substepCounter++ & 1u);
                     nAttempts += spec[d.species].n;
                 }
                 ++iStep;
@@ -1723,6 +1746,15 @@ int bfm_time_kernels(bfm_handle *h, uint32_t nmcs, double *ms, uint64_t *launche
     GUARD(h, {
         if (!ms || !launches || !attempts) throw InvalidArgument("null output pointer");
         h->e.timeKernels(nmcs, ms, launches, attempts);
+    });
+}
+
+int bfm_set_sweep_shape(bfm_handle *h, int shape)
+{
+    GUARD(h, {
+        if (shape < -1 || shape > 5) throw InvalidArgument("sweep shape must be -1 (automatic) or 0..5");
+        h->e.forcedShape = shape;
+        if (h->e.initialized) h->e.configureSweep();
     });
 }
 

@@ -237,6 +237,10 @@ class UpdaterGPUScBFM_AB_Type:
         self._check(self._lib.bfm_get_launch_info(self._h, ctypes.byref(m), ctypes.byref(g), ctypes.byref(t), ctypes.byref(b)))
         return {"mode": m.value, "ctas": g.value, "threads": t.value, "smem_bytes": b.value}
 
+    def setSweepShape(self, shape: int):
+        """-1 automatic; 0 gather, 1 stored bond codes, 2 staged; +3 global candidate lists."""
+        self._check(self._lib.bfm_set_sweep_shape(self._h, int(shape)))
+
     def setBarrierTimeoutMs(self, ms: int):
         self._check(self._lib.bfm_set_barrier_timeout_ms(self._h, int(ms)))
 

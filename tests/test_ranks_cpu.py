@@ -33,7 +33,7 @@ def _worker(rank, world, port, out):
 def test_two_gloo_ranks_aggregate_weak_scaling():
     world = 2
     port = _free_port()
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
     for r in range(world):
