@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--melt-mcs", type=int, default=2000)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--sweep-shape", type=int, default=-1,
+                   help="persistent-kernel shape (-1 automatic; see bfm_set_sweep_shape)")
     return p.parse_args()
 
 
@@ -236,6 +238,8 @@ def run_b200(args, ranks):
     system = make_workload()
     pb.r250_seed(1000 + ranks.rank)
     u = pb.UpdaterGPUScBFM_AB_Type().setup(system, gpu=gpu, rng=pb.Rng.Saru)
+    if args.sweep_shape != -1:
+        u.setSweepShape(args.sweep_shape)
     S = args.mcs_per_step
     u.runSimulationOnGPU(args.melt_mcs)        # melt the serpentine crystal (untimed)
     launch_info = u.getLaunchInfo()

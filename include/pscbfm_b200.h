@@ -117,14 +117,16 @@ int bfm_time_kernels(bfm_handle *h, uint32_t nmcs, double *ms, uint64_t *launche
 int bfm_set_launch_mode(bfm_handle *h, int mode);
 /* shape of the persistent kernel chosen at initialize: mode 0 = bonds tested
  * from the partners' positions, 1 = from stored bond codes, 2 = stored codes
- * with the CTA's slab segments staged in shared memory by bulk copies
- * (negative: -launch path of the per-substep kernels); CTAs, threads per CTA
- * and dynamic shared memory per CTA */
+ * with the CTA's slab segments staged in shared memory by bulk copies, 6..8 =
+ * stored codes with the independent work of each substep done inside the
+ * grid-barrier waits (negative: -launch path of the per-substep kernels);
+ * CTAs, threads per CTA and dynamic shared memory per CTA */
 int bfm_get_launch_info(const bfm_handle *h, int *mode, int *grid, int *threads, size_t *smem_bytes);
 /* force a shape of the persistent kernel (tests, tuning): -1 automatic
  * (default), 0 gather, 1 stored codes, 2 staged; 3..5 the same with the
- * candidate lists in global instead of shared memory.  BFM_ERUNTIME when the
- * shape does not fit this system. */
+ * candidate lists in global instead of shared memory; 6..8 windowed
+ * (1024 threads x 1 item in flight, 1024 x 2, 512 x 4).
+ * BFM_ERUNTIME when the shape does not fit this system. */
 int bfm_set_sweep_shape(bfm_handle *h, int shape);
 /* bound of every grid-barrier wait in the persistent kernel (default 2000 ms);
  * a wait that runs out ends the launch and bfm_run returns BFM_ETIMEOUT */

@@ -157,6 +157,130 @@ __host__ __device__ inline FaceWords zface_words(uint32_t r0, int dir, const Geo
     return out;
 }
 
+/* Leading face with its masks in closed form (no table lookups).  The sites
+ * of a 4x4x4 brick whose coordinate along axis k lies in a value set V
+ * (bit v of V = value v) form a "cylinder" mask; coordinate bits of axis k
+ * are bits k and k + 3 of the brick index, so each axis has a closed form:
+ *   x: period 16, value v at byte (v >> 1), pattern 0x55 << (v & 1)
+ *   y: period 32, value v at half (v >> 1), pattern 0x3333 << 2 (v & 1)
+ *   z: value v at word half (v >> 1), pattern 0x0F0F0F0F << 4 (v & 1)
+ * written as one multiplication of the spread value set. */
+__host__ __device__ __forceinline__ uint32_t cyl_x(uint32_t V)
+{
+    return ((V & 3u) | ((V & 12u) << 6)) * 0x00550055u;
+}
+__host__ __device__ __forceinline__ uint32_t cyl_y(uint32_t V)
+{
+    return ((V & 1u) | ((V & 2u) << 1) | ((V & 4u) << 14) | ((V & 8u) << 15)) * 0x3333u;
+}
+__host__ __device__ __forceinline__ void cyl_z(uint32_t V, uint32_t &lo, uint32_t &hi)
+{
+    lo = ((V & 1u) | ((V & 2u) << 3)) * 0x0F0F0F0Fu;
+    hi = (((V >> 2) & 1u) | (((V >> 3) & 1u) << 4)) * 0x0F0F0F0Fu;
+}
+
+struct FaceM {
+    uint32_t w[4];             /* brick words: (b-half, c-half) = (0,0), (1,0), (0,1), (1,1) */
+    uint32_t lo[4], hi[4];     /* site masks inside each word (zero: word not touched) */
+    uint32_t ma, ua;           /* payload mask and unit of the move axis */
+};
+
+/* The face of a move of the monomer at r0 in direction dir: the 3x3 sites
+ * two steps ahead along the move axis a, -1..+1 along the transverse axes
+ * b, c (b = y for a = x, else x; c = y for a = z, else z). */
+__host__ __device__ __forceinline__ FaceM face_alu(uint32_t r0, int dir, const Geometry &g)
+{
+    const uint32_t ax = (uint32_t)dir >> 1;
+    const uint32_t bx = ax == 0u ? 1u : 0u, cx = ax == 2u ? 1u : 2u;
+    const uint32_t ma = axis_mask(g, (int)ax), mb = axis_mask(g, (int)bx), mc = axis_mask(g, (int)cx);
+    const uint32_t ua = 1u << ax, ub = 1u << bx, uc = 1u << cx;
+    const uint32_t two = ua << 3; /* dilated 2 along the move axis */
+    const uint32_t pa = (dir & 1) ? (((r0 | ~ma) + two) & ma) : (((r0 & ma) - two) & ma);
+    const uint32_t b0 = ((r0 & mb) - ub) & mb;
+    const uint32_t b2 = ((r0 | ~mb) + ub) & mb;
+    const uint32_t c0 = ((r0 & mc) - uc) & mc;
+    const uint32_t c2 = ((r0 | ~mc) + uc) & mc;
+    const uint32_t la = ((pa >> ax) & 1u) | ((pa >> (ax + 2u)) & 2u);
+    const uint32_t lb = ((b0 >> bx) & 1u) | ((b0 >> (bx + 2u)) & 2u);
+    const uint32_t lc = ((c0 >> cx) & 1u) | ((c0 >> (cx + 2u)) & 2u);
+    const uint32_t ha = pa >> 6, hb0 = b0 >> 6, hb2 = b2 >> 6, hc0 = c0 >> 6, hc2 = c2 >> 6;
+    FaceM f;
+    f.w[0] = ha | hb0 | hc0;
+    f.w[1] = ha | hb2 | hc0;
+    f.w[2] = ha | hb0 | hc2;
+    f.w[3] = ha | hb2 | hc2;
+    /* value sets: the plane value along a, the transverse ranges split at
+     * the brick edge into the near (0) and far (1) brick */
+    const uint32_t P = 1u << la;
+    const uint32_t tb = 7u << lb, tc = 7u << lc;
+    const uint32_t B0 = tb & 15u, B1 = tb >> 4, C0 = tc & 15u, C1 = tc >> 4;
+    const uint32_t X0 = cyl_x(ax == 0u ? P : B0), X1 = cyl_x(ax == 0u ? P : B1);
+    const uint32_t Y0 = cyl_y(ax == 1u ? P : (ax == 0u ? B0 : C0));
+    const uint32_t Y1 = cyl_y(ax == 1u ? P : (ax == 0u ? B1 : C1));
+    uint32_t Z0l, Z0h, Z1l, Z1h;
+    cyl_z(ax == 2u ? P : C0, Z0l, Z0h);
+    cyl_z(ax == 2u ? P : C1, Z1l, Z1h);
+    /* word (gb, gc): x takes half gb, z half gc, y half gb when it is the b
+     * axis (a = x) and gc otherwise; the plane axis has equal halves */
+    const uint32_t t0 = X0 & Y0;
+    const uint32_t t1 = X1 & (ax == 0u ? Y1 : Y0);
+    const uint32_t t2 = X0 & (ax == 0u ? Y0 : Y1);
+    const uint32_t t3 = X1 & Y1;
+    f.lo[0] = t0 & Z0l;
+    f.hi[0] = t0 & Z0h;
+    f.lo[1] = t1 & Z0l;
+    f.hi[1] = t1 & Z0h;
+    f.lo[2] = t2 & Z1l;
+    f.hi[2] = t2 & Z1h;
+    f.lo[3] = t3 & Z1l;
+    f.hi[3] = t3 & Z1h;
+    f.ma = ma;
+    f.ua = ua;
+    return f;
+}
+
+/* The four brick words of the face and the index of its masks in the face
+ * table ((ax * 4 + la) * 4 + lb) * 4 + lc (la, lb, lc: the low coordinate
+ * bits of the plane and of the first transverse values), with the
+ * direction constants computed in registers. */
+struct FaceW {
+    uint32_t w[4];
+    uint32_t t;
+    uint32_t ma, ua;
+};
+
+__host__ __device__ __forceinline__ FaceW face_words(uint32_t r0, int dir, const Geometry &g)
+{
+    const uint32_t ax = (uint32_t)dir >> 1;
+    const uint32_t bx = ax == 0u ? 1u : 0u, cx = ax == 2u ? 1u : 2u;
+    const uint32_t ma = axis_mask(g, (int)ax), mb = axis_mask(g, (int)bx), mc = axis_mask(g, (int)cx);
+    const uint32_t ua = 1u << ax, ub = 1u << bx, uc = 1u << cx;
+    const uint32_t two = ua << 3;
+    const uint32_t pa = (dir & 1) ? (((r0 | ~ma) + two) & ma) : (((r0 & ma) - two) & ma);
+    const uint32_t b0 = ((r0 & mb) - ub) & mb;
+    const uint32_t b2 = ((r0 | ~mb) + ub) & mb;
+    const uint32_t c0 = ((r0 & mc) - uc) & mc;
+    const uint32_t c2 = ((r0 | ~mc) + uc) & mc;
+    const uint32_t la = ((pa >> ax) & 1u) | ((pa >> (ax + 2u)) & 2u);
+    const uint32_t lb = ((b0 >> bx) & 1u) | ((b0 >> (bx + 2u)) & 2u);
+    const uint32_t lc = ((c0 >> cx) & 1u) | ((c0 >> (cx + 2u)) & 2u);
+    const uint32_t ha = pa >> 6, hb0 = b0 >> 6, hb2 = b2 >> 6, hc0 = c0 >> 6, hc2 = c2 >> 6;
+    FaceW f;
+    f.w[0] = ha | hb0 | hc0;
+    f.w[1] = ha | hb2 | hc0;
+    f.w[2] = ha | hb0 | hc2;
+    f.w[3] = ha | hb2 | hc2;
+    f.t = ((ax * 4u + la) * 4u + lb) * 4u + lc;
+    f.ma = ma;
+    f.ua = ua;
+    return f;
+}
+
+__host__ __device__ __forceinline__ unsigned long long face_mask(const FaceM &f, int g)
+{
+    return ((unsigned long long)f.hi[g] << 32) | f.lo[g];
+}
+
 /* ------------------------------------------------------------------ RNGs */
 
 enum RngKind { RNG_INTHASH = 1, RNG_SARU = 2, RNG_PHILOX = 3 };

@@ -230,7 +230,8 @@ __global__ void k_bondcodes(const uint32_t *__restrict__ pos, const uint32_t *__
 enum SweepMode {
     SWEEP_GATHER = 0, /* bonds tested from the partners' positions */
     SWEEP_STORED = 1, /* bonds tested from stored codes (bond vector mod 8) */
-    SWEEP_STAGED = 2  /* stored codes; a CTA's slab segments staged in shared memory by bulk copies */
+    SWEEP_STAGED = 2, /* stored codes; a CTA's slab segments staged in shared memory by bulk copies */
+    SWEEP_WINDOWED = 6 /* stored codes; independent work done inside the barrier waits (k_sweep_w), 6..8 */
 };
 
 /* Shared-memory layout of the staged mode for a window of W items (W a
@@ -537,6 +538,380 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
         if (nCand) atomicAdd(s.counters + 0, (unsigned long long)nCand);
         if (nAcc) atomicAdd(s.counters + 1, (unsigned long long)nAcc);
     }
+}
+
+/* ------------------------------------------------ windowed persistent kernel
+ *
+ * The same substep as k_sweep (check, grid barrier, perform, grid barrier)
+ * with each grid barrier split into arrival and wait, and the wait used for
+ * the work that does not depend on the other CTAs:
+ *   after arriving at the check->perform barrier: zero the previous
+ *     substep's targets, and fetch the bond data of this CTA's candidates
+ *     into registers (a candidate's own bond codes are written only by its
+ *     own CTA, and the partners' CTAs do not move during this colour);
+ *   after arriving at the perform->next barrier: draw the next substep's
+ *     directions into shared memory.
+ * A CTA owns the same range of every colour slab for the whole launch, so
+ * the positions (and bond counts) of its monomers stay in shared memory
+ * from the start of the launch to its end; a move writes its new position
+ * there and only the lattice and the bond codes go to global memory.  Warp 0
+ * stays out of the window work so that thread 0 sees the barrier complete
+ * as soon as it does.  Each warp keeps its own candidate list (ballot
+ * prefix sums, no atomics); the perform phase takes the candidates of all
+ * warps in one index space.  The colour ranges of the CTA live in shared
+ * memory and the next schedule entry is fetched a substep ahead, so no
+ * global load chain starts a substep.
+ */
+constexpr uint32_t kWinMaxSpecies = 32;
+
+/* Shared memory of the windowed kernel, for at most W items of one colour
+ * and P items of all colours per CTA and T threads: positions of all the
+ * CTA's monomers (4 B), direction | bonds << 3 of this substep's items
+ * (1 B), bond counts of all the CTA's monomers (1 B), then two sets (this
+ * substep's and the previous one's) of per-warp candidate lists of
+ * seg = 32 * ceil(W / T) entries. */
+struct WinLayout {
+    uint32_t W, T, P;
+    __host__ __device__ uint32_t seg() const { return 32u * ((W + T - 1u) / T); }
+    __host__ __device__ size_t pos() const { return 0; }
+    __host__ __device__ size_t x() const { return (size_t)P * 4; }
+    __host__ __device__ size_t deg() const { return x() + W; }
+    __host__ __device__ size_t lists() const { return (deg() + P + 15) & ~(size_t)15; }
+    __host__ __device__ size_t bytes() const { return lists() + (size_t)2 * (T / 32u) * seg() * 8u; }
+};
+
+/* apply an accepted move: lattice bits, position (shared memory), image
+ * counter, own bond codes and the partners' codes of the bonds back
+ * (per-axis negation) */
+__device__ __forceinline__ void apply_move(const Sys &s, unsigned long long *lat, uint32_t *spos, uint32_t slot, uint32_t r0,
+                                           int dir, const Geometry &geo, uint32_t dgm, uint32_t q0, uint32_t v0, uint32_t c0,
+                                           uint32_t q1, uint32_t v1, uint32_t c1)
+{
+    const uint32_t npad = s.npad;
+    const uint32_t ax = (uint32_t)(dir >> 1);
+    const uint32_t ma = axis_mask(geo, (int)ax), ua = 1u << ax;
+    const uint32_t r1 = (dir & 1) ? zinc(r0, ma, ua) : zdec(r0, ma, ua);
+    const uint32_t w0 = r0 >> 6, w1 = r1 >> 6;
+    const unsigned long long b0 = 1ull << (r0 & 63u), b1 = 1ull << (r1 & 63u);
+    if (w0 == w1) {
+        atomicXor(lat + w0, b0 | b1);
+    } else {
+        atomicXor(lat + w0, b0);
+        atomicXor(lat + w1, b1);
+    }
+    *spos = r1;
+    const bool wrapped = (dir & 1) ? ((r1 & ma) == 0) : ((r0 & ma) == 0);
+    if (wrapped) s.img[(size_t)ax * npad + slot] += (dir & 1) ? 1 : -1;
+    uint16_t *bcode = s.bcode;
+    if (dgm > 0) {
+        const uint32_t nc = (dir & 1) ? bcode_dec(c0, ax) : bcode_inc(c0, ax);
+        bcode[slot] = (uint16_t)nc;
+        bcode[(size_t)v0 * npad + q0] = (uint16_t)bcode_neg(nc);
+    }
+    if (dgm > 1) {
+        const uint32_t nc = (dir & 1) ? bcode_dec(c1, ax) : bcode_inc(c1, ax);
+        bcode[(size_t)npad + slot] = (uint16_t)nc;
+        bcode[(size_t)v1 * npad + q1] = (uint16_t)bcode_neg(nc);
+    }
+    for (uint32_t b = 2; b < dgm; ++b) {
+        const size_t own = (size_t)b * npad + slot;
+        const uint32_t nc = (dir & 1) ? bcode_dec(bcode[own], ax) : bcode_inc(bcode[own], ax);
+        bcode[own] = (uint16_t)nc;
+        bcode[(size_t)s.rev[own] * npad + s.nbr[own]] = (uint16_t)bcode_neg(nc);
+    }
+}
+
+/* one shape of the windowed kernel: U items per thread in flight in the
+ * check phase; blockDim.x threads (a multiple of 32, 64 to 1024) */
+template <int RNG, int U>
+__global__ void __launch_bounds__(1024, 1)
+    k_sweep_w(Sys s, const Substep *__restrict__ sched, uint32_t k0, uint32_t k1, GridBarrier *bar,
+              unsigned long long timeoutNs, uint32_t maxdeg, uint32_t window, uint32_t nspec, uint32_t ptotal)
+{
+    const uint32_t T = blockDim.x, NW = T >> 5;
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    __shared__ __align__(16) unsigned long long s_table[kFaceTableA];
+    __shared__ uint32_t s_after[6 * 16];
+    __shared__ uint32_t s_lo[kWinMaxSpecies], s_n[kWinMaxSpecies], s_off[kWinMaxSpecies], s_base[kWinMaxSpecies];
+    __shared__ unsigned int s_wcnt[2][32];
+
+    const WinLayout lay{window, T, ptotal};
+    const uint32_t seg = lay.seg();
+    uint32_t *spos = reinterpret_cast<uint32_t *>(s_dyn + lay.pos());
+    uint8_t *px = s_dyn + lay.x();
+    uint8_t *sdeg = s_dyn + lay.deg();
+    uint2 *lists = reinterpret_cast<uint2 *>(s_dyn + lay.lists());
+
+    build_face_table_a(s_table);
+    for (uint32_t e = threadIdx.x; e < 96; e += T) { /* the CTA may have fewer than 96 threads */
+        const uint32_t dir = e >> 4, w = e & 15u, ax = dir >> 1;
+        uint32_t bits = 0;
+        for (uint32_t b = 0; b < 32; ++b) {
+            const uint32_t c = w * 32u + b;
+            const uint32_t nc = (dir & 1u) ? bcode_dec(c, ax) : bcode_inc(c, ax); /* (q - r0) - D */
+            bits |= ((s.bonds.forbidden[nc >> 5] >> (nc & 31u)) & 1u) << b;
+        }
+        s_after[e] = bits;
+    }
+    if (threadIdx.x < nspec) {
+        /* this CTA's contiguous range of every colour slab */
+        const Species sp = s.spec[threadIdx.x];
+        const uint32_t lo = (uint32_t)(((uint64_t)sp.n * blockIdx.x) / gridDim.x);
+        const uint32_t hi = (uint32_t)(((uint64_t)sp.n * (blockIdx.x + 1)) / gridDim.x);
+        s_lo[threadIdx.x] = lo;
+        s_n[threadIdx.x] = hi - lo;
+        s_off[threadIdx.x] = sp.off + lo;
+    }
+    if (threadIdx.x < 64) s_wcnt[threadIdx.x >> 5][threadIdx.x & 31u] = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t b = 0;
+        for (uint32_t c = 0; c < nspec; ++c) {
+            s_base[c] = b;
+            b += s_n[c];
+        }
+    }
+    __syncthreads();
+    /* the CTA's positions and bond counts, resident for the launch */
+    for (uint32_t c = 0; c < nspec; ++c)
+        for (uint32_t w = threadIdx.x; w < s_n[c]; w += T) {
+            spos[s_base[c] + w] = s.pos[s_off[c] + w];
+            sdeg[s_base[c] + w] = s.deg[s_off[c] + w];
+        }
+    __syncthreads();
+
+    unsigned long long *lat = reinterpret_cast<unsigned long long *>(s.lat);
+    unsigned long long *tmp = reinterpret_cast<unsigned long long *>(s.tmp);
+    const Geometry geo = s.g;
+    const uint32_t words = s.latWords >> 1;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t lanemask = (1u << lane) - 1u;
+    const uint32_t npad = s.npad;
+    const uint32_t *__restrict__ nbr = s.nbr;
+    const uint16_t *bcode = s.bcode;
+    unsigned int nCand = 0, nAcc = 0;
+    unsigned int target = 0;
+    bool alive = true;
+
+    /* directions of the items of substep dn, by warps 1.. */
+    auto prep = [&](const Substep &dn) {
+        const uint32_t plo = s_lo[dn.species], n = s_n[dn.species], base = s_base[dn.species];
+#pragma unroll 2
+        for (uint32_t w = threadIdx.x - 32u; w < n; w += T - 32u)
+            px[w] = (uint8_t)((uint32_t)direction(draw<RNG>(dn.seed, dn.iter, plo + w, dn.iterHi)) | ((uint32_t)sdeg[base + w] << 3));
+    };
+    /* zero the target words of warp wi's candidates of the substep using buffer buf, list set p */
+    auto clear_targets = [&](uint32_t buf, uint32_t p, uint32_t wi) {
+        unsigned long long *tp = tmp + (size_t)buf * words;
+        const uint2 *pl = lists + ((size_t)p * NW + wi) * seg;
+        const unsigned int pc = s_wcnt[p][wi];
+        for (uint32_t j = lane; j < pc; j += 32u) {
+            const uint2 e = pl[j];
+            tp[zstep(e.y, (int)(e.x >> 28), geo) >> 6] = 0ull;
+        }
+    };
+    /* occupied sites of a face */
+    auto occupied = [&](const unsigned long long *L, const FaceW &fw) -> unsigned long long {
+        const ulonglong2 *tp = reinterpret_cast<const ulonglong2 *>(s_table + (fw.t << 2));
+        const ulonglong2 m01 = tp[0], m23 = tp[1];
+        unsigned long long o = L[fw.w[0]] & m01.x;
+        if (m01.y) o |= L[fw.w[1]] & m01.y;
+        if (m23.x) o |= L[fw.w[2]] & m23.x;
+        if (m23.y) o |= L[fw.w[3]] & m23.y;
+        return o;
+    };
+
+    Substep d = sched[k0];
+    if (threadIdx.x >= 32) prep(d);
+    __syncthreads();
+    uint32_t prevBuf = 0;
+
+    for (uint32_t k = k0; k < k1; ++k) {
+        const Substep dnext = k + 1u < k1 ? sched[k + 1u] : d; /* arrives long before it is used */
+        const uint32_t n = s_n[d.species], off = s_off[d.species], base = s_base[d.species];
+        const uint32_t p = k & 1u;
+        uint2 *wlist = lists + ((size_t)p * NW + warp) * seg;
+        unsigned long long *tb = tmp + (size_t)d.buf * words;
+        unsigned int wc = 0; /* this warp's candidates (warp-uniform) */
+
+        /* phase A: U items per thread at a time */
+        for (uint32_t b0 = 0; b0 < n; b0 += (uint32_t)U * T) {
+            FaceW f[U];
+            uint32_t r0[U], x[U], ca[U], cb[U];
+            unsigned long long occ[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint32_t w = b0 + (uint32_t)u * T + threadIdx.x;
+                const uint32_t ws = w < n ? w : 0u;
+                r0[u] = spos[base + ws];
+                x[u] = px[ws];
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint32_t w = b0 + (uint32_t)u * T + threadIdx.x;
+                f[u] = face_words(r0[u], (int)(x[u] & 7u), geo);
+                occ[u] = 1ull;
+                ca[u] = cb[u] = 0u;
+                if (w < n) {
+                    occ[u] = occupied(lat, f[u]);
+                    if (maxdeg > 0) ca[u] = bcode[off + w];
+                    if (maxdeg > 1) cb[u] = bcode[(size_t)npad + off + w];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint32_t w = b0 + (uint32_t)u * T + threadIdx.x;
+                const int dir = (int)(x[u] & 7u);
+                const uint32_t dg = x[u] >> 3;
+                bool ok = occ[u] == 0ull;
+                if (ok) {
+                    const uint32_t *after = s_after + dir * 16;
+                    if (dg > 0) ok = !((after[ca[u] >> 5] >> (ca[u] & 31u)) & 1u);
+                    if (dg > 1) ok = ok && !((after[cb[u] >> 5] >> (cb[u] & 31u)) & 1u);
+                    for (uint32_t j = 2; ok && j < dg; ++j) {
+                        const uint32_t c = bcode[(size_t)j * npad + off + w];
+                        if ((after[c >> 5] >> (c & 31u)) & 1u) ok = false;
+                    }
+                }
+                if (ok) {
+                    const uint32_t r1 = (dir & 1) ? zinc(r0[u], f[u].ma, f[u].ua) : zdec(r0[u], f[u].ma, f[u].ua);
+                    atomicOr(tb + (r1 >> 6), 1ull << (r1 & 63u));
+                }
+                const unsigned int m = __ballot_sync(0xFFFFFFFFu, ok);
+                if (ok) wlist[wc + __popc(m & lanemask)] = make_uint2(w | ((uint32_t)dir << 28), r0[u]);
+                wc += __popc(m);
+            }
+        }
+        if (lane == 0) s_wcnt[p][warp] = wc;
+        nCand += lane == 0 ? wc : 0u;
+
+        /* check -> perform barrier */
+        __syncthreads();
+        grid_arrive(bar, target, gridDim.x);
+        /* the previous substep's targets (nobody reads or writes that buffer
+         * until every CTA has passed the next barrier); warp 1 also takes
+         * warp 0's */
+        if (k > k0 && warp > 0) {
+            clear_targets(prevBuf, p ^ 1u, warp);
+            if (warp == 1) clear_targets(prevBuf, p ^ 1u, 0);
+        }
+        /* The CTA's candidates in one index space: lane l of every warp
+         * holds the exclusive offset of warp l's list.  Candidate j goes to
+         * thread 32 + j (warp 0 stays free to watch the barrier); its bond
+         * data are fetched now. */
+        const unsigned int cntl = lane < NW ? s_wcnt[p][lane] : 0u;
+        unsigned int incl = cntl;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned int t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if ((int)lane >= o) incl += t;
+        }
+        const unsigned int excl = incl - cntl;
+        const unsigned int total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        /* list entry of candidate j: the last warp whose offset is <= j */
+        auto entry = [&](uint32_t j) -> uint2 {
+            uint32_t lo = 0;
+#pragma unroll
+            for (uint32_t step = 16; step > 0; step >>= 1) {
+                const uint32_t mid = lo + step;
+                const unsigned int om = __shfl_sync(0xFFFFFFFFu, excl, mid & 31u);
+                if (mid < NW && om <= j) lo = mid;
+            }
+            return lists[((size_t)p * NW + lo) * seg + (j - __shfl_sync(0xFFFFFFFFu, excl, lo))];
+        };
+        const uint32_t jb = threadIdx.x - 32u;
+        const bool bval = threadIdx.x >= 32 && jb < total;
+        uint2 e0 = make_uint2(0u, 0u);
+        uint32_t bdg = 0, bq0 = 0, bv0 = 0, bc0 = 0, bq1 = 0, bv1 = 0, bc1 = 0;
+        if (warp > 0 && 32u * (warp - 1u) < total) { /* warp-uniform */
+            e0 = entry(bval ? jb : 0u);
+            if (bval) {
+                const uint32_t w = e0.x & 0x0FFFFFFFu, slot = off + w;
+                bdg = sdeg[base + w];
+                if (maxdeg > 0) {
+                    bq0 = nbr[slot];
+                    bv0 = s.rev[slot];
+                    bc0 = bcode[slot];
+                }
+                if (maxdeg > 1) {
+                    bq1 = nbr[(size_t)npad + slot];
+                    bv1 = s.rev[(size_t)npad + slot];
+                    bc1 = bcode[(size_t)npad + slot];
+                }
+            }
+        }
+        if (!grid_wait(bar, target, timeoutNs)) {
+            alive = false;
+            break;
+        }
+
+        /* phase B: perform the candidates */
+        {
+            const unsigned long long *tr = tmp + (size_t)d.buf * words;
+            if (bval) {
+                const uint32_t w = e0.x & 0x0FFFFFFFu;
+                if (!occupied(tr, face_words(e0.y, (int)(e0.x >> 28), geo))) {
+                    apply_move(s, lat, spos + base + w, off + w, e0.y, (int)(e0.x >> 28), geo, bdg, bq0, bv0, bc0, bq1, bv1, bc1);
+                    ++nAcc;
+                }
+            }
+            for (uint32_t j0 = T - 32u; j0 < total; j0 += T) {
+                /* beyond the first T - 32 candidates: all threads, fetched now */
+                const uint32_t j = j0 + threadIdx.x;
+                const uint2 e = entry(j < total ? j : 0u);
+                if (j >= total) continue;
+                const uint32_t w = e.x & 0x0FFFFFFFu, slot = off + w;
+                const uint32_t dgm = sdeg[base + w];
+                uint32_t q0 = 0, v0 = 0, c0 = 0, q1 = 0, v1 = 0, c1 = 0;
+                if (maxdeg > 0) {
+                    q0 = nbr[slot];
+                    v0 = s.rev[slot];
+                    c0 = bcode[slot];
+                }
+                if (maxdeg > 1) {
+                    q1 = nbr[(size_t)npad + slot];
+                    v1 = s.rev[(size_t)npad + slot];
+                    c1 = bcode[(size_t)npad + slot];
+                }
+                if (occupied(tr, face_words(e.y, (int)(e.x >> 28), geo))) continue;
+                apply_move(s, lat, spos + base + w, slot, e.y, (int)(e.x >> 28), geo, dgm, q0, v0, c0, q1, v1, c1);
+                ++nAcc;
+            }
+        }
+
+        /* perform -> next check barrier */
+        __syncthreads();
+        grid_arrive(bar, target, gridDim.x);
+        if (k + 1u < k1 && threadIdx.x >= 32) prep(dnext);
+        if (!grid_wait(bar, target, timeoutNs)) {
+            alive = false;
+            break;
+        }
+        prevBuf = d.buf;
+        d = dnext;
+    }
+    /* every CTA has passed the last barrier: zero the last targets so the
+     * next launch starts from clean target lattices */
+    if (alive && k1 > k0) clear_targets(prevBuf, (k1 - 1u) & 1u, warp);
+    /* positions back to global memory */
+    __syncthreads();
+    for (uint32_t c = 0; c < nspec; ++c)
+        for (uint32_t w = threadIdx.x; w < s_n[c]; w += T) s.pos[s_off[c] + w] = spos[s_base[c] + w];
+    for (int o = 16; o > 0; o >>= 1) nAcc += __shfl_down_sync(0xFFFFFFFFu, nAcc, o);
+    if (lane == 0 && s.counters) {
+        if (nCand) atomicAdd(s.counters + 0, (unsigned long long)nCand);
+        if (nAcc) atomicAdd(s.counters + 1, (unsigned long long)nAcc);
+    }
+}
+
+/* the windowed shapes: items in flight per thread in the check phase; the
+ * CTA size is chosen at configuration to pack the CTA's items tightly */
+constexpr int kWinU[3] = {1, 2, 4};
+
+template <int RNG>
+const void *win_kernel(int i)
+{
+    return i == 0 ? (const void *)k_sweep_w<RNG, 1> : i == 1 ? (const void *)k_sweep_w<RNG, 2> : (const void *)k_sweep_w<RNG, 4>;
 }
 
 /* rounds grid barriers expecting `expected` CTAs; with expected > gridDim.x
@@ -1006,7 +1381,9 @@ struct Engine {
      * in shared memory when that fits. */
     int sweepMode = 0;
     uint32_t sweepWindow = 0;
-    int forcedShape = -1; /* -1 automatic; 0..2 bond mode; +3: candidate lists in global memory */
+    int forcedShape = -1; /* -1 automatic; 0..2 bond mode; +3: candidate lists in global memory; 6 windowed */
+    int sweepThreads = kSweepThreads;
+    uint32_t sweepTotal = 0; /* windowed kernel: most items of all colours one CTA owns */
 
     /* Persistent-kernel launch shape: one CTA per SM (cooperative launch,
      * all CTAs resident); each CTA owns 1/grid of every colour slab.  The
@@ -1040,12 +1417,53 @@ struct Engine {
         sweepSmem = smem;
         sweepWindow = W;
         sweepMode = MODE;
+        sweepThreads = kSweepThreads;
+        return true;
+    }
+
+    /* the windowed kernel (shape 6 + variant): one CTA per SM; positions,
+     * directions and both candidate lists in shared memory */
+    template <int RNG>
+    bool configureWindowed(int smCount, size_t smemLimit, int variant)
+    {
+        if (nSpecies > kWinMaxSpecies) return false;
+        const uint32_t grid = (uint32_t)smCount;
+        const uint32_t per = (nmax + grid - 1) / grid + 1u;
+        const uint32_t W = (per + 15u) & ~15u;
+        /* fewest rounds of U items per thread at <= 1024 threads, then the
+         * fewest warps for that many rounds (at least 2: warp 0 watches the
+         * barriers) */
+        const uint32_t U = (uint32_t)kWinU[variant];
+        const uint32_t rounds = (per + U * 1024u - 1u) / (U * 1024u);
+        const uint32_t threads = std::max<uint32_t>(64u, 32u * ((per + 32u * U * rounds - 1u) / (32u * U * rounds)));
+        uint32_t P = 0; /* most items of all colours one CTA owns */
+        for (uint32_t c = 0; c < nSpecies; ++c) P += (spec[c].n + grid - 1) / grid;
+        P = (P + 15u) & ~15u;
+        const size_t smem = WinLayout{W, threads, P}.bytes();
+        if (smem > smemLimit) return false;
+        const void *fn = win_kernel<RNG>(variant);
+        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int fit = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, fn, (int)threads, smem));
+        if (fit < 1) return false;
+        sweepGrid = (int)grid;
+        sweepCap = W;
+        sweepSmem = smem;
+        sweepWindow = W;
+        sweepMode = SWEEP_WINDOWED + variant;
+        sweepThreads = (int)threads;
+        sweepTotal = P;
         return true;
     }
 
     template <int RNG>
     void configureRng(int smCount, size_t smemLimit)
     {
+        if (forcedShape >= SWEEP_WINDOWED) {
+            if (!storedBonds || !configureWindowed<RNG>(smCount, smemLimit, forcedShape - SWEEP_WINDOWED))
+                throw std::runtime_error("the requested persistent-kernel shape is not available for this system");
+            return;
+        }
         if (forcedShape >= 0) {
             const int m = forcedShape % 3;
             bool ok = false;
@@ -1056,6 +1474,9 @@ struct Engine {
             return;
         }
         if (storedBonds) {
+            /* 4 items in flight when a CTA has more than a thousand per colour */
+            const int v = (nmax + (uint32_t)smCount - 1u) / (uint32_t)smCount > 1024u ? 2 : 1;
+            if (configureWindowed<RNG>(smCount, smemLimit, v)) return;
             if (configureFor<RNG, SWEEP_STAGED>(smCount, smemLimit)) return;
             if (configureFor<RNG, SWEEP_STORED>(smCount, smemLimit)) return;
         }
@@ -1078,7 +1499,7 @@ struct Engine {
         else
             configureRng<RNG_INTHASH>(sms, limit);
         dfree(d_glist);
-        if (sweepSmem == 0) dalloc(d_glist, (size_t)sweepGrid * sweepCap);
+        if (sweepSmem == 0 && sweepMode < SWEEP_WINDOWED) dalloc(d_glist, (size_t)sweepGrid * sweepCap);
     }
 
     void launchSweep(const Substep *sched, uint32_t k0, uint32_t k1)
@@ -1092,6 +1513,16 @@ struct Engine {
         uint32_t win = sweepWindow;
         void *args[] = {&s, (void *)&sched, &k0, &k1, &bar, &gl, &cap, &to, &md, &win};
         CK(cudaMemsetAsync(d_bar, 0, sizeof(GridBarrier), stream)); /* the counting barrier starts at 0 */
+        if (sweepMode >= SWEEP_WINDOWED) {
+            uint32_t ns = nSpecies, pt = sweepTotal;
+            void *wargs[] = {&s, (void *)&sched, &k0, &k1, &bar, &to, &md, &win, &ns, &pt};
+            const int v = sweepMode - SWEEP_WINDOWED;
+            const void *wf = rng == BFM_RNG_SARU     ? win_kernel<RNG_SARU>(v)
+                             : rng == BFM_RNG_PHILOX ? win_kernel<RNG_PHILOX>(v)
+                                                     : win_kernel<RNG_INTHASH>(v);
+            CK(cudaLaunchCooperativeKernel(wf, dim3(sweepGrid), dim3(sweepThreads), wargs, sweepSmem, stream));
+            return;
+        }
         const void *fn = nullptr;
         if (rng == BFM_RNG_SARU)
             fn = sweepMode == SWEEP_STAGED ? (const void *)k_sweep<RNG_SARU, SWEEP_STAGED>
@@ -1752,7 +2183,7 @@ int bfm_time_kernels(bfm_handle *h, uint32_t nmcs, double *ms, uint64_t *launche
 int bfm_set_sweep_shape(bfm_handle *h, int shape)
 {
     GUARD(h, {
-        if (shape < -1 || shape > 5) throw InvalidArgument("sweep shape must be -1 (automatic) or 0..5");
+        if (shape < -1 || shape > 8) throw InvalidArgument("sweep shape must be -1 (automatic) or 0..8");
         h->e.forcedShape = shape;
         if (h->e.initialized) h->e.configureSweep();
     });
@@ -1764,7 +2195,7 @@ int bfm_get_launch_info(const bfm_handle *h, int *mode, int *grid, int *threads,
     if (!h->e.initialized) return BFM_ENOTINIT;
     if (mode) *mode = h->e.launchMode == 0 ? h->e.sweepMode : -h->e.launchMode;
     if (grid) *grid = h->e.sweepGrid;
-    if (threads) *threads = kSweepThreads;
+    if (threads) *threads = h->e.sweepThreads;
     if (smem_bytes) *smem_bytes = h->e.sweepSmem;
     return BFM_OK;
 }

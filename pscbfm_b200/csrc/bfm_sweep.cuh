@@ -136,6 +136,49 @@ __device__ __forceinline__ bool grid_barrier_count(GridBarrier *bar, unsigned in
     return s_ok2 != 0;
 }
 
+/* Split form of the counting barrier, so that a CTA can do work that does
+ * not depend on the other CTAs between its arrival and its wait.
+ * grid_arrive: after a __syncthreads that ends the CTA's part, thread 0 adds
+ * its arrival with release semantics.  grid_wait: thread 0 polls the counter
+ * (acquire) until `target` arrivals; the error word and the clock are read
+ * only every 32 polls so that a poll is a single load.  Both return the
+ * CTA-wide verdict through shared memory after a __syncthreads. */
+__device__ __forceinline__ void grid_arrive(GridBarrier *bar, unsigned int &target, unsigned int nblocks)
+{
+    if (threadIdx.x == 0) {
+        target += nblocks;
+        red_release_add(&bar->count, 1u);
+    }
+}
+
+__device__ __forceinline__ bool grid_wait(GridBarrier *bar, unsigned int target, unsigned long long timeoutNs)
+{
+    __shared__ unsigned int s_ok3;
+    if (threadIdx.x == 0) {
+        unsigned int ok = 1;
+        if ((int)(ld_acquire_gpu(&bar->count) - target) < 0) {
+            const unsigned long long t0 = global_ns();
+            for (unsigned int polls = 1;; ++polls) {
+                if ((int)(ld_acquire_gpu(&bar->count) - target) >= 0) break;
+                if ((polls & 31u) == 0) {
+                    if (ld_acquire_gpu(&bar->err)) {
+                        ok = 0;
+                        break;
+                    }
+                    if (polls > kBarrierMaxPolls || global_ns() - t0 > timeoutNs) {
+                        atomicExch(&bar->err, 1u);
+                        ok = 0;
+                        break;
+                    }
+                }
+            }
+        }
+        s_ok3 = ok;
+    }
+    __syncthreads();
+    return s_ok3 != 0;
+}
+
 /* ---- bulk (TMA) copies global -> shared on an mbarrier ------------------ */
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
@@ -310,6 +353,48 @@ __device__ __forceinline__ Face4 face4d(uint32_t r0, int dir, const DirConst &d,
     f.m[2] = t23.x;
     f.m[3] = t23.y;
     return f;
+}
+
+/* The leading face as four word indices plus the index of its mask entry
+ * in the table of build_face_table_a (masks fetched where they are used). */
+struct FaceT {
+    uint32_t w[4];
+    uint32_t t;
+};
+
+__device__ __forceinline__ FaceT face4t(uint32_t r0, int dir, const DirConst &d)
+{
+    const uint32_t two = d.ua << 3;
+    const uint32_t pa = (dir & 1) ? (((r0 | ~d.ma) + two) & d.ma) : (((r0 & d.ma) - two) & d.ma);
+    const uint32_t b0 = ((r0 & d.mb) - d.ub) & d.mb;
+    const uint32_t b2 = ((r0 | ~d.mb) + d.ub) & d.mb;
+    const uint32_t c0 = ((r0 & d.mc) - d.uc) & d.mc;
+    const uint32_t c2 = ((r0 | ~d.mc) + d.uc) & d.mc;
+    const uint32_t ax = (uint32_t)(dir >> 1);
+    const uint32_t la = ((pa >> ax) & 1u) | ((pa >> (ax + 2)) & 2u);
+    const uint32_t lb = ((b0 >> d.bx) & 1u) | ((b0 >> (d.bx + 2)) & 2u);
+    const uint32_t lc = ((c0 >> d.cx) & 1u) | ((c0 >> (d.cx + 2)) & 2u);
+    const uint32_t ha = pa >> 6, hb0 = b0 >> 6, hb2 = b2 >> 6, hc0 = c0 >> 6, hc2 = c2 >> 6;
+    FaceT f;
+    f.w[0] = ha | hb0 | hc0;
+    f.w[1] = ha | hb2 | hc0;
+    f.w[2] = ha | hb0 | hc2;
+    f.w[3] = ha | hb2 | hc2;
+    f.t = ((ax * 4u + la) * 4u + lb) * 4u + lc;
+    return f;
+}
+
+/* occupied sites of a face given its words and table entry */
+__device__ __forceinline__ unsigned long long face_bits(const unsigned long long *lat, const uint32_t *w,
+                                                        const unsigned long long *tableA, uint32_t t)
+{
+    const ulonglong2 *tp = reinterpret_cast<const ulonglong2 *>(tableA + (t << 2));
+    const ulonglong2 m01 = tp[0], m23 = tp[1];
+    unsigned long long o = lat[w[0]] & m01.x;
+    if (m01.y) o |= lat[w[1]] & m01.y;
+    if (m23.x) o |= lat[w[2]] & m23.x;
+    if (m23.y) o |= lat[w[3]] & m23.y;
+    return o;
 }
 
 /* The leading face of a monomer at r0 moving in dir as <= 4 (word, mask). */

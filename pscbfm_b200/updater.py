@@ -238,7 +238,8 @@ class UpdaterGPUScBFM_AB_Type:
         return {"mode": m.value, "ctas": g.value, "threads": t.value, "smem_bytes": b.value}
 
     def setSweepShape(self, shape: int):
-        """-1 automatic; 0 gather, 1 stored bond codes, 2 staged; +3 global candidate lists."""
+        """-1 automatic; 0 gather, 1 stored bond codes, 2 staged; +3 global candidate lists;
+        6..8 windowed (1024 threads x 1 item, 1024 x 2, 512 x 4)."""
         self._check(self._lib.bfm_set_sweep_shape(self._h, int(shape)))
 
     def setBarrierTimeoutMs(self, ms: int):
