@@ -73,7 +73,7 @@ struct Sys {
     int32_t *img;
     const uint32_t *nbr;
     const uint8_t *deg;
-    uint16_t *bcode;      /* bond codes zbond(partner, self), row per bond (stored-bond path) */
+    uint16_t *bcode;      /* bond codes zbond(partner, self), stored-bond path; layout bc_index */
     const uint8_t *rev;   /* for bond row j of a monomer: the row of the partner that points back */
     uint8_t *flags;
     uint32_t *lat;
@@ -85,6 +85,16 @@ struct Sys {
     Geometry g;
     Bondset bonds;
 };
+
+/* Bond codes of a slot: rows 0 and 1 interleaved in one 32-bit word (row 0
+ * in the low half), so that the check reads both with one load and a move
+ * writes both with one store; rows j >= 2 follow as rows of npad entries. */
+__host__ __device__ __forceinline__ size_t bc_index(uint32_t j, uint32_t slot, uint32_t npad)
+{
+    return j < 2u ? 2u * (size_t)slot + j : (size_t)j * npad + slot;
+}
+__device__ __forceinline__ uint32_t *bc_pair(uint16_t *bcode) { return reinterpret_cast<uint32_t *>(bcode); }
+__device__ __forceinline__ const uint32_t *bc_pair(const uint16_t *bcode) { return reinterpret_cast<const uint32_t *>(bcode); }
 
 /* ------------------------------------------------------------- kernels */
 
@@ -222,7 +232,7 @@ __global__ void k_bondcodes(const uint32_t *__restrict__ pos, const uint32_t *__
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npad; i += gridDim.x * blockDim.x) {
         const uint32_t r = pos[i];
         for (uint32_t j = 0; j < deg[i]; ++j)
-            bcode[(size_t)j * npad + i] = (uint16_t)zbond(pos[nbr[(size_t)j * npad + i]], r);
+            bcode[bc_index(j, i, npad)] = (uint16_t)zbond(pos[nbr[(size_t)j * npad + i]], r);
     }
 }
 
@@ -235,13 +245,12 @@ enum SweepMode {
 };
 
 /* Shared-memory layout of the staged mode for a window of W items (W a
- * multiple of 16): positions (4 B), bond codes rows 0 and 1 (2 B each), bond
- * count and direction (1 B each), then the candidate list. */
+ * multiple of 16): positions (4 B), bond codes rows 0 and 1 (one 32-bit
+ * word), bond count and direction (1 B each), then the candidate list. */
 struct StageLayout {
     uint32_t W;
     __host__ __device__ size_t pos() const { return 0; }
-    __host__ __device__ size_t bc0() const { return (size_t)W * 4; }
-    __host__ __device__ size_t bc1() const { return (size_t)W * 6; }
+    __host__ __device__ size_t bc() const { return (size_t)W * 4; }
     __host__ __device__ size_t dg() const { return (size_t)W * 8; }
     __host__ __device__ size_t dirs() const { return (size_t)W * 9; }
     __host__ __device__ size_t list() const { return (size_t)W * 10; }
@@ -269,8 +278,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
 
     const StageLayout lay{window};
     uint32_t *st_pos = reinterpret_cast<uint32_t *>(s_dyn + lay.pos());
-    uint16_t *st_bc0 = reinterpret_cast<uint16_t *>(s_dyn + lay.bc0());
-    uint16_t *st_bc1 = reinterpret_cast<uint16_t *>(s_dyn + lay.bc1());
+    uint32_t *st_bc = reinterpret_cast<uint32_t *>(s_dyn + lay.bc());
     uint8_t *st_dg = s_dyn + lay.dg();
     uint8_t *st_dir = s_dyn + lay.dirs();
     uint2 *list = glist ? glist + (size_t)blockIdx.x * cap : reinterpret_cast<uint2 *>(s_dyn + (STAGE ? lay.list() : 0));
@@ -324,13 +332,12 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
         if (STAGE && threadIdx.x == 0) {
             /* stage this CTA's segments of the slab: all copies in flight at once */
             const uint32_t wn = ((hi + 15u) & ~15u) - wlo;
-            const uint32_t rows = maxdeg < 2 ? maxdeg : 2u;
+            const uint32_t codes = maxdeg > 0 ? 4u : 0u;
             fence_proxy_async();
-            mbar_arrive_expect_tx(&s_mbar, wn * (4u + 1u + 2u * rows));
+            mbar_arrive_expect_tx(&s_mbar, wn * (4u + 1u + codes));
             bulk_g2s(st_pos, pos + sp.off + wlo, wn * 4u, &s_mbar);
             bulk_g2s(st_dg, deg + sp.off + wlo, wn, &s_mbar);
-            if (rows > 0) bulk_g2s(st_bc0, bcode + sp.off + wlo, wn * 2u, &s_mbar);
-            if (rows > 1) bulk_g2s(st_bc1, bcode + (size_t)npad + sp.off + wlo, wn * 2u, &s_mbar);
+            if (codes) bulk_g2s(st_bc, bc_pair(bcode) + sp.off + wlo, wn * 4u, &s_mbar);
         }
         /* zero the target words this CTA's candidates set in the previous substep */
         if (havePrev) {
@@ -363,8 +370,9 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
             nr0 = pos[slot];
             ndg = deg[slot];
             if (STORED) {
-                na = maxdeg > 0 ? bcode[slot] : 0u;
-                nb = maxdeg > 1 ? bcode[(size_t)npad + slot] : 0u;
+                const uint32_t pr = maxdeg > 0 ? bc_pair(bcode)[slot] : 0u;
+                na = pr & 0xFFFFu;
+                nb = pr >> 16;
             } else {
                 na = maxdeg > 0 ? nbr[slot] : 0u;
                 nb = maxdeg > 1 ? nbr[(size_t)npad + slot] : 0u;
@@ -378,8 +386,9 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
                 const uint32_t w = valid ? i - wlo : 0u;
                 r0 = st_pos[w];
                 dg = st_dg[w];
-                ea = maxdeg > 0 ? st_bc0[w] : 0u;
-                eb = maxdeg > 1 ? st_bc1[w] : 0u;
+                const uint32_t pr = maxdeg > 0 ? st_bc[w] : 0u;
+                ea = pr & 0xFFFFu;
+                eb = pr >> 16;
                 dir = st_dir[w];
             } else {
                 r0 = nr0;
@@ -392,8 +401,9 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
                     nr0 = pos[slot];
                     ndg = deg[slot];
                     if (STORED) {
-                        na = maxdeg > 0 ? bcode[slot] : 0u;
-                        nb = maxdeg > 1 ? bcode[(size_t)npad + slot] : 0u;
+                        const uint32_t pr = maxdeg > 0 ? bc_pair(bcode)[slot] : 0u;
+                        na = pr & 0xFFFFu;
+                        nb = pr >> 16;
                     } else {
                         na = maxdeg > 0 ? nbr[slot] : 0u;
                         nb = maxdeg > 1 ? nbr[(size_t)npad + slot] : 0u;
@@ -467,12 +477,13 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
                     if (maxdeg > 0) {
                         q0 = nbr[slot];
                         v0 = s.rev[slot];
-                        c0 = bcode[slot];
+                        const uint32_t pr = bc_pair(bcode)[slot];
+                        c0 = pr & 0xFFFFu;
+                        c1 = pr >> 16;
                     }
                     if (maxdeg > 1) {
                         q1 = nbr[(size_t)npad + slot];
                         v1 = s.rev[(size_t)npad + slot];
-                        c1 = bcode[(size_t)npad + slot];
                     }
                 }
                 if (face4_occupied(tr, f)) continue;
@@ -493,20 +504,17 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
                     /* own bonds: (q - r0) -> (q - r1); the partner's bond back is
                      * always the per-axis negation, so it is written, not read */
                     if (dgm > 0) {
-                        const uint32_t nc = (dir & 1) ? bcode_dec(c0, ax) : bcode_inc(c0, ax);
-                        bcode[slot] = (uint16_t)nc;
-                        bcode[(size_t)v0 * npad + q0] = (uint16_t)bcode_neg(nc);
-                    }
-                    if (dgm > 1) {
-                        const uint32_t nc = (dir & 1) ? bcode_dec(c1, ax) : bcode_inc(c1, ax);
-                        bcode[(size_t)npad + slot] = (uint16_t)nc;
-                        bcode[(size_t)v1 * npad + q1] = (uint16_t)bcode_neg(nc);
+                        const uint32_t n0 = (dir & 1) ? bcode_dec(c0, ax) : bcode_inc(c0, ax);
+                        const uint32_t n1 = dgm > 1 ? ((dir & 1) ? bcode_dec(c1, ax) : bcode_inc(c1, ax)) : c1;
+                        bc_pair(bcode)[slot] = n0 | (n1 << 16);
+                        bcode[bc_index(v0, q0, npad)] = (uint16_t)bcode_neg(n0);
+                        if (dgm > 1) bcode[bc_index(v1, q1, npad)] = (uint16_t)bcode_neg(n1);
                     }
                     for (uint32_t b = 2; b < dgm; ++b) {
                         const size_t own = (size_t)b * npad + slot;
                         const uint32_t nc = (dir & 1) ? bcode_dec(bcode[own], ax) : bcode_inc(bcode[own], ax);
                         bcode[own] = (uint16_t)nc;
-                        bcode[(size_t)s.rev[own] * npad + nbr[own]] = (uint16_t)bcode_neg(nc);
+                        bcode[bc_index(s.rev[own], nbr[own], npad)] = (uint16_t)bcode_neg(nc);
                     }
                 }
                 ++nAcc;
@@ -604,20 +612,17 @@ __device__ __forceinline__ void apply_move(const Sys &s, unsigned long long *lat
     if (wrapped) s.img[(size_t)ax * npad + slot] += (dir & 1) ? 1 : -1;
     uint16_t *bcode = s.bcode;
     if (dgm > 0) {
-        const uint32_t nc = (dir & 1) ? bcode_dec(c0, ax) : bcode_inc(c0, ax);
-        bcode[slot] = (uint16_t)nc;
-        bcode[(size_t)v0 * npad + q0] = (uint16_t)bcode_neg(nc);
-    }
-    if (dgm > 1) {
-        const uint32_t nc = (dir & 1) ? bcode_dec(c1, ax) : bcode_inc(c1, ax);
-        bcode[(size_t)npad + slot] = (uint16_t)nc;
-        bcode[(size_t)v1 * npad + q1] = (uint16_t)bcode_neg(nc);
+        const uint32_t n0 = (dir & 1) ? bcode_dec(c0, ax) : bcode_inc(c0, ax);
+        const uint32_t n1 = dgm > 1 ? ((dir & 1) ? bcode_dec(c1, ax) : bcode_inc(c1, ax)) : c1;
+        bc_pair(bcode)[slot] = n0 | (n1 << 16);
+        bcode[bc_index(v0, q0, npad)] = (uint16_t)bcode_neg(n0);
+        if (dgm > 1) bcode[bc_index(v1, q1, npad)] = (uint16_t)bcode_neg(n1);
     }
     for (uint32_t b = 2; b < dgm; ++b) {
         const size_t own = (size_t)b * npad + slot;
         const uint32_t nc = (dir & 1) ? bcode_dec(bcode[own], ax) : bcode_inc(bcode[own], ax);
         bcode[own] = (uint16_t)nc;
-        bcode[(size_t)s.rev[own] * npad + s.nbr[own]] = (uint16_t)bcode_neg(nc);
+        bcode[bc_index(s.rev[own], s.nbr[own], npad)] = (uint16_t)bcode_neg(nc);
     }
 }
 
@@ -737,7 +742,7 @@ __global__ void __launch_bounds__(1024, 1)
         /* phase A: U items per thread at a time */
         for (uint32_t b0 = 0; b0 < n; b0 += (uint32_t)U * T) {
             FaceW f[U];
-            uint32_t r0[U], x[U], ca[U], cb[U];
+            uint32_t r0[U], x[U], ca[U];
             unsigned long long occ[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
@@ -751,11 +756,10 @@ __global__ void __launch_bounds__(1024, 1)
                 const uint32_t w = b0 + (uint32_t)u * T + threadIdx.x;
                 f[u] = face_words(r0[u], (int)(x[u] & 7u), geo);
                 occ[u] = 1ull;
-                ca[u] = cb[u] = 0u;
+                ca[u] = 0u;
                 if (w < n) {
                     occ[u] = occupied(lat, f[u]);
-                    if (maxdeg > 0) ca[u] = bcode[off + w];
-                    if (maxdeg > 1) cb[u] = bcode[(size_t)npad + off + w];
+                    if (maxdeg > 0) ca[u] = bc_pair(bcode)[off + w];
                 }
             }
 #pragma unroll
@@ -766,8 +770,9 @@ __global__ void __launch_bounds__(1024, 1)
                 bool ok = occ[u] == 0ull;
                 if (ok) {
                     const uint32_t *after = s_after + dir * 16;
-                    if (dg > 0) ok = !((after[ca[u] >> 5] >> (ca[u] & 31u)) & 1u);
-                    if (dg > 1) ok = ok && !((after[cb[u] >> 5] >> (cb[u] & 31u)) & 1u);
+                    const uint32_t a0 = ca[u] & 0x1FFu, a1 = (ca[u] >> 16) & 0x1FFu;
+                    if (dg > 0) ok = !((after[a0 >> 5] >> (a0 & 31u)) & 1u);
+                    if (dg > 1) ok = ok && !((after[a1 >> 5] >> (a1 & 31u)) & 1u);
                     for (uint32_t j = 2; ok && j < dg; ++j) {
                         const uint32_t c = bcode[(size_t)j * npad + off + w];
                         if ((after[c >> 5] >> (c & 31u)) & 1u) ok = false;
@@ -831,12 +836,13 @@ __global__ void __launch_bounds__(1024, 1)
                 if (maxdeg > 0) {
                     bq0 = nbr[slot];
                     bv0 = s.rev[slot];
-                    bc0 = bcode[slot];
+                    const uint32_t pr = bc_pair(bcode)[slot];
+                    bc0 = pr & 0xFFFFu;
+                    bc1 = pr >> 16;
                 }
                 if (maxdeg > 1) {
                     bq1 = nbr[(size_t)npad + slot];
                     bv1 = s.rev[(size_t)npad + slot];
-                    bc1 = bcode[(size_t)npad + slot];
                 }
             }
         }
@@ -866,12 +872,13 @@ __global__ void __launch_bounds__(1024, 1)
                 if (maxdeg > 0) {
                     q0 = nbr[slot];
                     v0 = s.rev[slot];
-                    c0 = bcode[slot];
+                    const uint32_t pr = bc_pair(bcode)[slot];
+                    c0 = pr & 0xFFFFu;
+                    c1 = pr >> 16;
                 }
                 if (maxdeg > 1) {
                     q1 = nbr[(size_t)npad + slot];
                     v1 = s.rev[(size_t)npad + slot];
-                    c1 = bcode[(size_t)npad + slot];
                 }
                 if (occupied(tr, face_words(e.y, (int)(e.x >> 28), geo))) continue;
                 apply_move(s, lat, spos + base + w, slot, e.y, (int)(e.x >> 28), geo, dgm, q0, v0, c0, q1, v1, c1);
@@ -1311,7 +1318,7 @@ struct Engine {
         dalloc(d_nbr, nbrRows * npad); dalloc(d_nbr2, nbrRows * npad);
         dalloc(d_deg, npad); dalloc(d_deg2, npad);
         dalloc(d_rev, nbrRows * npad); dalloc(d_rev2, nbrRows * npad);
-        dalloc(d_bcode, nbrRows * npad);
+        dalloc(d_bcode, std::max<size_t>(nbrRows, 2) * npad); /* rows 0 and 1 interleaved: bc_index */
         dalloc(d_s2o, npad); dalloc(d_s2o2, npad); dalloc(d_o2s, n);
         dalloc(d_flags, npad);
         dalloc(d_lat, latWords);
@@ -1339,7 +1346,7 @@ struct Engine {
         CK(cudaMemcpyAsync(d_nbr, hnbr.data(), hnbr.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
         CK(cudaMemcpyAsync(d_deg, hdeg.data(), npad, cudaMemcpyHostToDevice, stream));
         CK(cudaMemcpyAsync(d_rev, hrev.data(), hrev.size(), cudaMemcpyHostToDevice, stream));
-        CK(cudaMemsetAsync(d_bcode, 0, nbrRows * npad * sizeof(uint16_t), stream));
+        CK(cudaMemsetAsync(d_bcode, 0, std::max<size_t>(nbrRows, 2) * npad * sizeof(uint16_t), stream));
         CK(cudaMemcpyAsync(d_s2o, s2o.data(), npad * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
         CK(cudaMemcpyAsync(d_o2s, o2s.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
         CK(cudaMemcpyAsync(d_lat, hlat.data(), latWords * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
