@@ -294,7 +294,8 @@ def run_b200(args, ranks):
     bytes_launch = (b_check + b_perf) * k_attempts / max(k_launches, 1)
     achieved = bytes_launch / t_launch / 1e9
     traffic = None
-    prof = os.path.join(HERE, "profiles", "k_sweep_melt256_traffic.json")
+    kname = "k_sweep_w" if launch_info.get("mode", 0) >= 6 else "k_sweep"
+    prof = os.path.join(HERE, "profiles", f"{kname}_melt256_traffic.json")
     if os.path.exists(prof):
         try:
             # DRAM bytes per attempted move from one ncu capture of a shorter
@@ -326,7 +327,7 @@ def run_b200(args, ranks):
                 "d2h_bytes_per_step": system.n * 12},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": traffic, "kernel": "k_sweep", "peak_source": f"{hbm_kind} hbm_gbs",
+                     "traffic": traffic, "kernel": kname, "peak_source": f"{hbm_kind} hbm_gbs",
                      "bytes_per_attempt": {"check": b_check, "perform": b_perf},
                      "attempts_per_launch": k_attempts / max(k_launches, 1),
                      "launch_ms": t_launch * 1e3, "launches_timed": k_launches,
