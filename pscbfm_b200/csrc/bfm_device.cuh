@@ -239,6 +239,36 @@ __host__ __device__ __forceinline__ FaceM face_alu(uint32_t r0, int dir, const G
     return f;
 }
 
+/* Entry e = ((ax * 4 + la) * 4 + lb) * 4 + lc of the face-mask table: for a
+ * move along axis ax whose leading face lies in the plane with low
+ * coordinate bits la, and whose transverse ranges start at low bits lb, lc,
+ * the masks of the nine face sites in the (up to) four bricks it touches,
+ * m[gb | gc << 1] (gb, gc: the range spills into the next brick along b, c). */
+__host__ __device__ inline void face_table_entry(int e, unsigned long long *m)
+{
+    const int a = e >> 6, la = (e >> 4) & 3, lb = (e >> 2) & 3, lc = e & 3;
+    const int bx = (a == 0) ? 1 : 0;
+    const int cx = (a == 2) ? 1 : 2;
+    const uint32_t abit = (((uint32_t)la & 1u) | (((uint32_t)la & 2u) << 2)) << a;
+    unsigned long long m0 = 0, m1 = 0, m2 = 0, m3 = 0;
+    for (int ib = 0; ib < 3; ++ib)
+        for (int ic = 0; ic < 3; ++ic) {
+            const int vb = lb + ib, vc = lc + ic;
+            const int g = (vb >= 4 ? 1 : 0) | (vc >= 4 ? 2 : 0);
+            const uint32_t ub = (uint32_t)(vb & 3), uc = (uint32_t)(vc & 3);
+            const uint32_t bit = abit | (((ub & 1u) | ((ub & 2u) << 2)) << bx) | (((uc & 1u) | ((uc & 2u) << 2)) << cx);
+            const unsigned long long v = 1ull << bit;
+            if (g == 0) m0 |= v;
+            else if (g == 1) m1 |= v;
+            else if (g == 2) m2 |= v;
+            else m3 |= v;
+        }
+    m[0] = m0;
+    m[1] = m1;
+    m[2] = m2;
+    m[3] = m3;
+}
+
 /* The four brick words of the face and the index of its masks in the face
  * table ((ax * 4 + la) * 4 + lb) * 4 + lc (la, lb, lc: the low coordinate
  * bits of the plane and of the first transverse values), with the

@@ -268,29 +268,7 @@ constexpr int kFaceTableA = 3 * 4 * 4 * 4 * 4;
 
 __device__ __forceinline__ void build_face_table_a(unsigned long long *t)
 {
-    for (int e = threadIdx.x; e < 192; e += blockDim.x) {
-        const int a = e >> 6, la = (e >> 4) & 3, lb = (e >> 2) & 3, lc = e & 3;
-        const int bx = (a == 0) ? 1 : 0;
-        const int cx = (a == 2) ? 1 : 2;
-        const uint32_t abit = (((uint32_t)la & 1u) | (((uint32_t)la & 2u) << 2)) << a;
-        unsigned long long m0 = 0, m1 = 0, m2 = 0, m3 = 0;
-        for (int ib = 0; ib < 3; ++ib)
-            for (int ic = 0; ic < 3; ++ic) {
-                const int vb = lb + ib, vc = lc + ic;
-                const int g = (vb >= 4 ? 1 : 0) | (vc >= 4 ? 2 : 0);
-                const uint32_t ub = (uint32_t)(vb & 3), uc = (uint32_t)(vc & 3);
-                const uint32_t bit = abit | (((ub & 1u) | ((ub & 2u) << 2)) << bx) | (((uc & 1u) | ((uc & 2u) << 2)) << cx);
-                const unsigned long long v = 1ull << bit;
-                if (g == 0) m0 |= v;
-                else if (g == 1) m1 |= v;
-                else if (g == 2) m2 |= v;
-                else m3 |= v;
-            }
-        t[e * 4 + 0] = m0;
-        t[e * 4 + 1] = m1;
-        t[e * 4 + 2] = m2;
-        t[e * 4 + 3] = m3;
-    }
+    for (int e = threadIdx.x; e < 192; e += blockDim.x) face_table_entry(e, t + e * 4);
 }
 
 /* Per-direction constants: payload masks of the move axis and of the two
