@@ -88,6 +88,26 @@ int bfm_run(bfm_handle *h, uint32_t nmcs);
 int bfm_get_monomer_position(bfm_handle *h, uint32_t i, int32_t *x, int32_t *y, int32_t *z);
 /* all positions (unfolded, as doCopyBack .cu:3402-3484 returns them), 3*n int32 */
 int bfm_get_positions(bfm_handle *h, int32_t *xyz, size_t n);
+
+/* ---- chain analysis on the device (the reference's AnalyzerMsd,
+ * src/AnalyzerMsd.tpp, for systems of linear chains) ----
+ * Chains, their end monomers and middle monomer are found once by the
+ * reference analyzer's rule (AnalyzerMsd.tpp:193-280); BFM_EINVAL when the
+ * bond graph is not a set of linear chains. */
+int bfm_analyzer_init(bfm_handle *h, uint32_t *n_chains);
+/* Observables of the current state, computed on the device:
+ * out[0] chains, out[1] <R_e^2>, out[2] <R_g^2>, out[3..7] g1..g5 against the
+ * time origin (first, middle, last monomer, chain centre of mass -- each
+ * minus the box centre-of-mass drift when there is more than one chain --
+ * and middle monomer minus chain centre of mass; AnalyzerMsd.tpp:392-421;
+ * zero before an origin is set), out[8..10] the box centre of mass.
+ * set_origin != 0 makes the current state the time origin afterwards. */
+int bfm_analyze(bfm_handle *h, int set_origin, double *out, size_t n_out);
+/* original monomer ids of every chain's first end, middle and last end */
+int bfm_analyzer_chain_ids(bfm_handle *h, uint32_t *first, uint32_t *middle, uint32_t *last, uint32_t n_chains);
+/* per-chain R_e^2, R_g^2 and centre of mass (x, y, z per chain) of the last bfm_analyze */
+int bfm_analyze_per_chain(bfm_handle *h, double *re2, double *rg2, double *com, uint32_t n_chains);
+
 /* cleanup (.h:487, .cu:3486-3502): frees the set-up; setters may be used again */
 int bfm_cleanup(bfm_handle *h);
 

@@ -261,3 +261,63 @@ class RefUpdater:
         if getattr(self, "_h", None):
             ref_gpu().ref_destroy(self._h)
             self._h = None
+
+
+# ---------------------------------------------------------------- chain analysis
+def linear_chains(deg, nbr):
+    """Restatement of AnalyzerMsd::getLinearPolymerSystemInfo
+    (src/AnalyzerMsd.tpp:193-280) for test use: chains in order of their
+    lowest id, walked with a stack; end monomers in the order met; the middle
+    monomer floor(n/2) bonds from the first end.  Returns (first, middle,
+    last, members) with members a list of id arrays."""
+    n = len(deg)
+    visited = np.zeros(n, dtype=bool)
+    first, middle, last, members = [], [], [], []
+    for i0 in range(n):
+        if visited[i0]:
+            continue
+        ends, todo, mem = [], [i0], [i0]
+        visited[i0] = True
+        while todo:
+            m = todo.pop()
+            nn = int(deg[m])
+            if nn > 2:
+                raise ValueError("not linear chains")
+            if nn <= 1:
+                ends.append(m)
+            for b in range(nn):
+                q = int(nbr[m][b])
+                if not visited[q]:
+                    visited[q] = True
+                    todo.append(q)
+                    mem.append(q)
+        if len(mem) == 1 and len(ends) == 1:
+            ends.append(ends[0])
+        if len(ends) != 2:
+            raise ValueError("not exactly two chain ends")
+        mid = prev = ends[0]
+        for _ in range(len(mem) // 2):
+            nxt = int(nbr[mid][0]) if int(nbr[mid][0]) != prev else int(nbr[mid][1])
+            prev, mid = mid, nxt
+        first.append(ends[0]); middle.append(mid); last.append(ends[1]); members.append(np.array(mem))
+    return np.array(first), np.array(middle), np.array(last), members
+
+
+def chain_observables(pos, first, middle, last, members, origin=None):
+    """<R_e^2>, <R_g^2>, per-chain centres and g1..g5 against `origin` (the
+    dict this function returns for the origin state), as AnalyzerMsd
+    computes them (src/AnalyzerMsd.tpp:304-421), in float64."""
+    p = np.asarray(pos, dtype=np.float64)
+    com = np.stack([p[m].mean(axis=0) for m in members])
+    re2 = ((p[last] - p[first]) ** 2).sum(axis=1)
+    rg2 = np.array([((p[m] - p[m].mean(axis=0)) ** 2).sum(axis=1).mean() for m in members])
+    box = com.mean(axis=0)
+    vals = [p[first], p[middle], p[last], com, p[middle] - com]
+    g = [0.0] * 5
+    if origin is not None:
+        drift = box - origin["box"] if len(members) > 1 else np.zeros(3)
+        for k in range(5):
+            d = vals[k] - origin["vals"][k] - (drift if k < 4 else 0.0)
+            g[k] = float((d * d).sum(axis=1).mean())
+    return {"re2": float(re2.mean()), "rg2": float(rg2.mean()), "re2_chain": re2, "rg2_chain": rg2,
+            "com": com, "box": box, "vals": vals, "g": g}

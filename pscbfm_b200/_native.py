@@ -19,7 +19,7 @@ LIBPATH = os.path.join(HERE, LIBNAME)
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 SOURCES = ["bfm_engine.cu", "bfm_diag.cu"]
-HEADERS = ["bfm_device.cuh", "bfm_host.hpp", "bfm_sweep.cuh", "../../include/pscbfm_b200.h"]
+HEADERS = ["bfm_device.cuh", "bfm_host.hpp", "bfm_sweep.cuh", "bfm_analyze.cuh", "../../include/pscbfm_b200.h"]
 
 NVCC_FLAGS = [
     "-std=c++17",
@@ -97,6 +97,10 @@ _SIGS = {
     "bfm_run": (_c.c_int, [_P, _c.c_uint32]),
     "bfm_get_monomer_position": (_c.c_int, [_P, _c.c_uint32, _c.POINTER(_c.c_int32), _c.POINTER(_c.c_int32), _c.POINTER(_c.c_int32)]),
     "bfm_get_positions": (_c.c_int, [_P, _P, _c.c_size_t]),
+    "bfm_analyzer_init": (_c.c_int, [_P, _c.POINTER(_c.c_uint32)]),
+    "bfm_analyze": (_c.c_int, [_P, _c.c_int, _P, _c.c_size_t]),
+    "bfm_analyzer_chain_ids": (_c.c_int, [_P, _P, _P, _P, _c.c_uint32]),
+    "bfm_analyze_per_chain": (_c.c_int, [_P, _P, _P, _P, _c.c_uint32]),
     "bfm_cleanup": (_c.c_int, [_P]),
     "bfm_get_lattice": (_c.c_int, [_P, _P, _c.c_size_t]),
     "bfm_get_lattice_words": (_c.c_int, [_P, _c.POINTER(_c.c_size_t)]),

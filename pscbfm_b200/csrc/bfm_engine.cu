@@ -37,6 +37,7 @@
 #include "bfm_device.cuh"
 #include "bfm_host.hpp"
 #include "bfm_sweep.cuh"
+#include "bfm_analyze.cuh"
 #include "../../include/pscbfm_b200.h"
 
 using namespace bfm;
@@ -1126,6 +1127,7 @@ struct Engine {
         dfree(d_deg); dfree(d_deg2); dfree(d_rev); dfree(d_rev2); dfree(d_bcode); dfree(d_s2o); dfree(d_s2o2); dfree(d_o2s); dfree(d_flags);
         dfree(d_lat); dfree(d_tmp); dfree(d_spec); dfree(d_counters); dfree(d_perm); dfree(d_inv);
         dfree(d_iota); dfree(d_keys); dfree(d_out); dfree(d_bar); dfree(d_glist);
+        releaseAnalyzer();
         if (d_cub) cudaFree(d_cub);
         d_cub = nullptr;
         for (int b = 0; b < 2; ++b) {
@@ -1747,6 +1749,62 @@ struct Engine {
         }
     }
 
+    /* ------------------------------------------------ chain analysis */
+    LinearChains chains;
+    bool chainsReady = false, haveOrigin = false;
+    uint32_t *d_coff = nullptr, *d_cmem = nullptr, *d_cfirst = nullptr, *d_cmid = nullptr, *d_clast = nullptr;
+    ChainSums *d_csum = nullptr;
+    ChainOrigin *d_corg = nullptr;
+    double *d_cbox = nullptr, *d_cre2 = nullptr, *d_crg2 = nullptr, *d_ccom = nullptr, *d_cout = nullptr;
+
+    void releaseAnalyzer()
+    {
+        dfree(d_coff); dfree(d_cmem); dfree(d_cfirst); dfree(d_cmid); dfree(d_clast); dfree(d_csum); dfree(d_corg);
+        dfree(d_cbox); dfree(d_cre2); dfree(d_crg2); dfree(d_ccom); dfree(d_cout);
+        chainsReady = haveOrigin = false;
+    }
+
+    uint32_t nChains() const { return (uint32_t)chains.first.size(); }
+
+    /* linear chains of the system by the reference analyzer's rule */
+    void analyzerInit()
+    {
+        if (!initialized) throw std::runtime_error("initialize must be called first");
+        LinearChains lc = linear_chains(n, deg.data(), nbr.data());
+        releaseAnalyzer();
+        chains = std::move(lc);
+        const uint32_t nc = nChains();
+        dalloc(d_coff, nc + 1); dalloc(d_cmem, (size_t)n); dalloc(d_cfirst, nc); dalloc(d_cmid, nc); dalloc(d_clast, nc);
+        dalloc(d_csum, nc); dalloc(d_corg, nc); dalloc(d_cbox, 3); dalloc(d_cre2, nc); dalloc(d_crg2, nc);
+        dalloc(d_ccom, 3 * (size_t)nc); dalloc(d_cout, 16);
+        CK(cudaMemcpyAsync(d_coff, chains.off.data(), (nc + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_cmem, chains.members.data(), (size_t)n * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_cfirst, chains.first.data(), nc * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_cmid, chains.middle.data(), nc * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_clast, chains.last.data(), nc * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        CK(cudaStreamSynchronize(stream));
+        chainsReady = true;
+        haveOrigin = false;
+    }
+
+    /* observables of the current state (out: 11 doubles); setOrigin makes
+     * the current state the time origin of the mean-square displacements */
+    void analyze(double *out, bool setOrigin)
+    {
+        if (!chainsReady) throw std::runtime_error("bfm_analyzer_init must be called first");
+        const uint32_t nc = nChains();
+        const int blocks = (int)std::min<uint32_t>((npad + kThreads - 1) / kThreads, 148 * 16);
+        k_unpack<<<blocks, kThreads, 0, stream>>>(d_pos, d_img, d_s2o, npad, (int32_t)L[0], (int32_t)L[1], (int32_t)L[2], d_out);
+        const int cblocks = (int)std::min<uint32_t>((nc + 7) / 8, 148 * 8);
+        k_chain_sums<<<std::max(cblocks, 1), 256, 0, stream>>>(d_out, d_coff, d_cmem, nc, d_csum);
+        k_chain_observables<<<1, kAnalyzeThreads, 0, stream>>>(d_out, d_csum, d_coff, d_cfirst, d_cmid, d_clast, nc, d_corg, d_cbox,
+                                                               haveOrigin ? 1 : 0, setOrigin ? 1 : 0, d_cre2, d_crg2, d_ccom, d_cout);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(out, d_cout, 11 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        if (setOrigin) haveOrigin = true;
+    }
+
     void readback()
     {
         if (!initialized) throw std::runtime_error("initialize must be called first");
@@ -2089,6 +2147,56 @@ int bfm_get_positions(bfm_handle *h, int32_t *xyz, size_t n)
         if (!xyz || n != h->e.n) throw InvalidArgument("position buffer does not match the number of monomers");
         h->e.readback();
         std::memcpy(xyz, h->e.h_out, 3 * n * sizeof(int32_t));
+    });
+}
+
+int bfm_analyzer_init(bfm_handle *h, uint32_t *n_chains)
+{
+    if (h && !h->e.initialized) {
+        h->e.err = "initialize must be called first";
+        return BFM_ENOTINIT;
+    }
+    GUARD(h, {
+        h->e.analyzerInit();
+        if (n_chains) *n_chains = h->e.nChains();
+    });
+}
+
+int bfm_analyze(bfm_handle *h, int set_origin, double *out, size_t n_out)
+{
+    if (h && !h->e.initialized) {
+        h->e.err = "initialize must be called first";
+        return BFM_ENOTINIT;
+    }
+    GUARD(h, {
+        if (!out || n_out < 11) throw InvalidArgument("bfm_analyze needs an output array of 11 doubles");
+        double tmp[11];
+        h->e.analyze(tmp, set_origin != 0);
+        std::memcpy(out, tmp, sizeof(tmp));
+    });
+}
+
+int bfm_analyzer_chain_ids(bfm_handle *h, uint32_t *first, uint32_t *middle, uint32_t *last, uint32_t n_chains)
+{
+    GUARD(h, {
+        if (!h->e.chainsReady) throw std::runtime_error("bfm_analyzer_init must be called first");
+        if (n_chains != h->e.nChains()) throw InvalidArgument("n_chains does not match the number of chains");
+        if (first) std::memcpy(first, h->e.chains.first.data(), n_chains * sizeof(uint32_t));
+        if (middle) std::memcpy(middle, h->e.chains.middle.data(), n_chains * sizeof(uint32_t));
+        if (last) std::memcpy(last, h->e.chains.last.data(), n_chains * sizeof(uint32_t));
+    });
+}
+
+int bfm_analyze_per_chain(bfm_handle *h, double *re2, double *rg2, double *com, uint32_t n_chains)
+{
+    GUARD(h, {
+        if (!h->e.chainsReady) throw std::runtime_error("bfm_analyzer_init must be called first");
+        if (n_chains != h->e.nChains()) throw InvalidArgument("n_chains does not match the number of chains");
+        auto &e = h->e;
+        if (re2) CK(cudaMemcpyAsync(re2, e.d_cre2, n_chains * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+        if (rg2) CK(cudaMemcpyAsync(rg2, e.d_crg2, n_chains * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+        if (com) CK(cudaMemcpyAsync(com, e.d_ccom, 3 * (size_t)n_chains * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+        CK(cudaStreamSynchronize(e.stream));
     });
 }
 

@@ -63,6 +63,7 @@ class UpdaterGPUScBFM_AB_Type:
         _raise(self._lib.bfm_create(ctypes.byref(h)), "bfm_create failed")
         self._h = h
         self._n = 0
+        self._nchains = 0
         self._steps_between_sortings = 5000
 
     # ------------------------------------------------------------ plumbing
@@ -182,6 +183,40 @@ class UpdaterGPUScBFM_AB_Type:
         out = np.empty((self._n, 3), dtype=np.int32)
         self._check(self._lib.bfm_get_positions(self._h, out.ctypes.data, self._n))
         return out
+
+    # ---- chain analysis on the device (the reference's AnalyzerMsd)
+    def analyzerInit(self) -> int:
+        """Find the linear chains (first end, middle, last end) by the
+        reference analyzer's rule; ValueError if the system is not made of
+        linear chains.  Returns the number of chains."""
+        nc = ctypes.c_uint32()
+        self._check(self._lib.bfm_analyzer_init(self._h, ctypes.byref(nc)))
+        self._nchains = nc.value
+        return nc.value
+
+    def analyze(self, set_origin: bool = False) -> dict:
+        """Chain observables of the current state, computed on the GPU:
+        <R_e^2>, <R_g^2>, g1..g5 against the time origin (zero before one is
+        set) and the box centre of mass.  set_origin makes the current state
+        the origin of later calls."""
+        out = np.zeros(11, dtype=np.float64)
+        self._check(self._lib.bfm_analyze(self._h, int(bool(set_origin)), out.ctypes.data, out.size))
+        return {"chains": int(out[0]), "re2": float(out[1]), "rg2": float(out[2]),
+                "g": [float(v) for v in out[3:8]], "box_com": out[8:11].copy()}
+
+    def analyzerChainIds(self):
+        nc = self._nchains
+        f, m, l = (np.empty(nc, dtype=np.uint32) for _ in range(3))
+        self._check(self._lib.bfm_analyzer_chain_ids(self._h, f.ctypes.data, m.ctypes.data, l.ctypes.data, nc))
+        return f, m, l
+
+    def analyzePerChain(self):
+        """per-chain R_e^2, R_g^2 and centre of mass of the last analyze()"""
+        nc = self._nchains
+        re2, rg2 = np.empty(nc), np.empty(nc)
+        com = np.empty((nc, 3))
+        self._check(self._lib.bfm_analyze_per_chain(self._h, re2.ctypes.data, rg2.ctypes.data, com.ctypes.data, nc))
+        return re2, rg2, com
 
     def getLattice(self) -> np.ndarray:
         nw = ctypes.c_size_t()
