@@ -63,7 +63,10 @@ int bfm_set_monomer_coordinates(bfm_handle *h, uint32_t i, int32_t x, int32_t y,
 int bfm_set_connectivity(bfm_handle *h, uint32_t i, uint32_t j);
 /* setLatticeSize (.h:496): powers of two, 8 <= L <= 1024 per axis */
 int bfm_set_lattice_size(bfm_handle *h, uint64_t bx, uint64_t by, uint64_t bz);
-/* setPeriodicity (.h:505); only fully periodic boxes are simulated */
+/* setPeriodicity (.h:505).  Along a non-periodic axis the box has walls: a
+ * cube corner takes the coordinates 0 .. L-2 and a move that would leave
+ * them is refused (the check of .cu:988-996 for unsigned coordinates, with
+ * each axis' own size); initialize refuses a monomer outside the walls. */
 int bfm_set_periodicity(bfm_handle *h, int px, int py, int pz);
 /* setAge / getAge (.h:506-507) */
 int bfm_set_age(bfm_handle *h, int64_t age);

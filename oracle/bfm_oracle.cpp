@@ -255,6 +255,16 @@ struct Sweep {
     std::vector<uint32_t> target;
     uint64_t nAttempt = 0, nCandidate = 0, nAccept = 0;
     int nThreads = 1;
+    bool periodic[3] = {true, true, true};
+
+    /* the box test of the check kernel for non-periodic axes (.cu:988-996),
+     * on the reference's unsigned device coordinates (a step below 0 wraps
+     * to the type's maximum), with the axis' own box size */
+    bool inside(int64_t c0, int64_t c1, int64_t L) const
+    {
+        if (c1 < 0) return false;
+        return (0 < c0 && c1 < L - 1) || (c0 == 0 && c1 <= 1) || (c0 == L - 1 && c1 > 1);
+    }
 
     uint32_t z(int64_t x, int64_t y, int64_t zz) const { return zindex(x, y, zz, mx, my, mz); }
 
@@ -312,6 +322,9 @@ struct Sweep {
             const uint32_t rn = draw(seed, iteration, (uint32_t)i);
             const int dir = (int)(rn % 6u);
             const int64_t x1 = px[id] + DX[dir], y1 = py[id] + DY[dir], z1 = pz[id] + DZ[dir];
+            if ((!periodic[0] && !inside(px[id], x1, Lx)) || (!periodic[1] && !inside(py[id], y1, Ly)) ||
+                (!periodic[2] && !inside(pz[id], z1, Lz)))
+                continue;
             bool bad = false;
             for (uint32_t j = 0; j < nnbr[id] && !bad; ++j) {
                 const uint32_t nb = nbr[(size_t)id * 8 + j];
@@ -346,7 +359,7 @@ struct Sweep {
         nAccept += na;
     }
 
-    /* runSimulationOnGPU (.cu:2902-3400), periodic boxes */
+    /* runSimulationOnGPU (.cu:2902-3400) */
     void run(uint32_t nMCS, R250State &r250)
     {
         for (uint32_t iStep = 0; iStep < nMCS; ++iStep, ++age) {
@@ -370,6 +383,15 @@ using namespace orc;
 extern "C" {
 
 uint32_t orc_saru(uint32_t seed, uint32_t iteration, uint32_t subseq) { return saru_u32(seed, iteration, subseq); }
+
+/* setPeriodicity of the emulated updater (before the first run) */
+void orc_sweep_set_periodicity(void *h, int px, int py, int pz)
+{
+    auto *s = static_cast<Sweep *>(h);
+    s->periodic[0] = px != 0;
+    s->periodic[1] = py != 0;
+    s->periodic[2] = pz != 0;
+}
 uint32_t orc_hash_rng(uint32_t seed, uint32_t subseq) { return hash_rng(seed, subseq); }
 uint32_t orc_philox(uint64_t seed, uint64_t subseq, uint64_t offset) { return philox4x32_10(seed, subseq, offset); }
 uint32_t orc_zindex(int64_t x, int64_t y, int64_t z, uint32_t mx, uint32_t my, uint32_t mz) { return zindex(x, y, z, mx, my, mz); }

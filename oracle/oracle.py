@@ -57,6 +57,7 @@ def orc() -> ctypes.CDLL:
         L.orc_sweep_create.restype = _P
         L.orc_sweep_create.argtypes = [_c.c_uint32] * 4 + [_P, _P, _P, _P, _c.c_int, _c.c_int64, _c.c_int64, _c.c_int]
         L.orc_sweep_destroy.argtypes = [_P]
+        L.orc_sweep_set_periodicity.argtypes = [_P, _c.c_int, _c.c_int, _c.c_int]
         L.orc_sweep_run.argtypes = [_P, _c.c_uint32, _P]
         L.orc_sweep_get.argtypes = [_P, _P]
         L.orc_sweep_age.restype = _c.c_int64
@@ -103,7 +104,7 @@ def graph_coloring(deg, nbr8, uniform=True):
 class Sweep:
     """Stateful CPU emulation of the reference's colored sweep."""
 
-    def __init__(self, system, rng=2, age=0, sort_every=5000, threads=None):
+    def __init__(self, system, rng=2, age=0, sort_every=5000, threads=None, periodic=(True, True, True)):
         L = orc()
         self.n = system.n
         self._pos = np.ascontiguousarray(system.pos, dtype=np.int32)
@@ -118,6 +119,7 @@ class Sweep:
                                      int(sort_every), int(threads))
         if not self._h:
             raise RuntimeError("oracle sweep set-up failed")
+        L.orc_sweep_set_periodicity(self._h, *(int(bool(p)) for p in periodic))
 
     def run(self, nmcs: int, r250: np.ndarray):
         orc().orc_sweep_run(self._h, int(nmcs), r250.ctypes.data)
@@ -215,6 +217,7 @@ def ref_gpu():
         L.ref_last_error.restype = _c.c_char_p
         L.ref_create.restype = _P
         L.ref_create.argtypes = [_c.c_int, _c.c_int] + [_c.c_uint32] * 4 + [_P, _P, _P, _P, _c.c_int, _c.c_int64, _c.c_int64]
+        L.ref_set_periodicity.argtypes = [_c.c_int]
         L.ref_run.restype = _c.c_int
         L.ref_run.argtypes = [_P, _c.c_uint32]
         L.ref_get.argtypes = [_P, _P, _c.c_uint32]
@@ -230,10 +233,11 @@ def ref_gpu():
 class RefUpdater:
     """The reference's own UpdaterGPUScBFM_AB_Type<T> on the GPU (oracle/_ref)."""
 
-    def __init__(self, system, rng=2, age=0, sort_every=5000, ctype=0, gpu=0):
+    def __init__(self, system, rng=2, age=0, sort_every=5000, ctype=0, gpu=0, periodic=(True, True, True)):
         L = ref_gpu()
         if L is None:
             raise RuntimeError("oracle/_ref/libref_pscbfm.so is not built")
+        L.ref_set_periodicity(sum(1 << a for a in range(3) if periodic[a]))
         self.n = system.n
         self._pos = np.ascontiguousarray(system.pos, dtype=np.int32)
         self._deg = np.ascontiguousarray(system.deg, dtype=np.uint32)

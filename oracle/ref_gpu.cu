@@ -41,6 +41,9 @@ struct Ref : RefBase {
     int64_t age() override { return u.getAge(); }
 };
 
+/* periodicity (bit a: axis a periodic) of the next ref_create */
+int g_periodic = 7;
+
 template <typename T>
 RefBase *make(int gpu, uint32_t Lx, uint32_t Ly, uint32_t Lz, uint32_t n, const int32_t *pos3,
               const uint32_t *nnbr, const uint32_t *nbr8, const uint8_t *allowed512, int rng, int64_t age,
@@ -57,7 +60,7 @@ RefBase *make(int gpu, uint32_t Lx, uint32_t Ly, uint32_t Lz, uint32_t n, const 
     u.setRng((typename UpdaterGPUScBFM_AB_Type<T>::Rng)rng);
     u.setAge(age);
     u.setStepsBetweenSortings(sortEvery);
-    u.setPeriodicity(true, true, true);
+    u.setPeriodicity((g_periodic & 1) != 0, (g_periodic & 2) != 0, (g_periodic & 4) != 0);
     u.setLatticeSize(Lx, Ly, Lz);
     u.setNrOfAllMonomers(n);
     for (uint32_t i = 0; i < n; ++i) u.setMonomerCoordinates(i, pos3[3 * i], pos3[3 * i + 1], pos3[3 * i + 2]);
@@ -81,6 +84,9 @@ thread_local std::string g_err;
 extern "C" {
 
 const char *ref_last_error() { return g_err.c_str(); }
+
+/* setPeriodicity of the next ref_create (bit a: axis a periodic; default 7) */
+void ref_set_periodicity(int mask) { g_periodic = mask; }
 
 /* ctype: 0 = int32_t (the adapter's default instantiation), 1 = uint8_t,
  * 2 = uint16_t (GPUScBFM_AB_Type.h:253-285) */

@@ -117,7 +117,8 @@ def write_bfm(path, system, frames, ids=None):
     out += b"#!version=2.0\n"
     out += f"!number_of_monomers={n}\n".encode()
     out += "".join(f"!box_{a}={b}\n" for a, b in zip("xyz", system.box)).encode()
-    out += "".join(f"!periodic_{a}=1\n" for a in "xyz").encode()
+    per = getattr(system, "periodic", (True, True, True))
+    out += "".join(f"!periodic_{a}={int(bool(p))}\n" for a, p in zip("xyz", per)).encode()
     out += b"!set_of_bondvectors\n"
     for i, v in ids.items():
         out += f"{v[0]} {v[1]} {v[2]}:{i}\n".encode()

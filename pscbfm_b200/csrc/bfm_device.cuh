@@ -22,6 +22,8 @@ namespace bfm {
  * (power-of-two edge lengths, so masking is the periodic wrap). */
 struct Geometry {
     uint32_t m[3];      /* m[0] = dilated(Lx-1), m[1] = dilated(Ly-1) << 1, m[2] = dilated(Lz-1) << 2 */
+    uint32_t open = 0;  /* bit a set: axis a is not periodic */
+    uint32_t top[3] = {0, 0, 0}; /* open axis a: dilated(L_a - 2) << a, the highest corner coordinate */
 };
 
 __host__ __device__ inline uint32_t dilate3(uint32_t x)
@@ -54,6 +56,22 @@ __host__ __device__ inline uint32_t zcode(uint32_t x, uint32_t y, uint32_t z)
 __host__ __device__ inline uint32_t axis_mask(const Geometry &g, int ax)
 {
     return ax == 0 ? g.m[0] : (ax == 1 ? g.m[1] : g.m[2]);
+}
+
+/* A move that would take the corner out of the box along a non-periodic
+ * axis.  The reference's check (UpdaterGPUScBFM_AB_Type.cu:988-996) lets the
+ * corner of a 2x2x2 cube take the coordinates 0 .. L-2 along such an axis
+ * (for its unsigned coordinate types; it compares y and z with the x size,
+ * which is the same test for cubic boxes).  Positions are kept inside that
+ * range from set-up on, so a step is refused exactly when it starts on the
+ * edge it is heading for. */
+__host__ __device__ inline bool leaves_box(uint32_t r0, int dir, const Geometry &g)
+{
+    const int ax = dir >> 1;
+    if (!((g.open >> ax) & 1u)) return false;
+    const uint32_t c = r0 & axis_mask(g, ax);
+    const uint32_t top = ax == 0 ? g.top[0] : (ax == 1 ? g.top[1] : g.top[2]);
+    return (dir & 1) ? c == top : c == 0u;
 }
 
 /* +1 / -1 along one axis with periodic wrap (mask = that axis' payload) */

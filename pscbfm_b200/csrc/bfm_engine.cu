@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(kThreads) k_check(Sys s, const Substep *__rest
             const int dir = direction(draw<RNG>(d.seed, d.iter, i, d.iterHi));
             const uint32_t r1 = zstep(r0, dir, s.g);
             const uint32_t nb = s.deg[slot];
-            bool ok = true;
+            bool ok = !leaves_box(r0, dir, s.g);
             for (uint32_t j = 0; j < nb; ++j) {
                 const uint32_t q = s.pos[s.nbr[(size_t)j * s.npad + slot]];
                 const uint32_t code = zbond(q, r1);
@@ -419,7 +419,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
                 const uint32_t r1 = dstep(r0, dir, dc);
                 if (STORED) {
                     const uint32_t *after = s_after + dir * 16;
-                    ok = !face4_occupied(lat, f);
+                    ok = !face4_occupied(lat, f) && !leaves_box(r0, dir, s.g);
                     if (dg > 0) ok = ok && !((after[ea >> 5] >> (ea & 31u)) & 1u);
                     if (dg > 1) ok = ok && !((after[eb >> 5] >> (eb & 31u)) & 1u);
                     for (uint32_t j = 2; j < dg; ++j) {
@@ -429,7 +429,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
                 } else {
                     const uint32_t p0 = pos[ea];
                     const uint32_t p1 = pos[eb];
-                    ok = !face4_occupied(lat, f);
+                    ok = !face4_occupied(lat, f) && !leaves_box(r0, dir, s.g);
                     if (dg > 0) {
                         const uint32_t c = zbond(p0, r1);
                         ok = ok && !((s_forbid[c >> 5] >> (c & 31u)) & 1u);
@@ -768,7 +768,7 @@ __global__ void __launch_bounds__(1024, 1)
                 const uint32_t w = b0 + (uint32_t)u * T + threadIdx.x;
                 const int dir = (int)(x[u] & 7u);
                 const uint32_t dg = x[u] >> 3;
-                bool ok = occ[u] == 0ull;
+                bool ok = occ[u] == 0ull && !leaves_box(r0[u], dir, geo);
                 if (ok) {
                     const uint32_t *after = s_after + dir * 16;
                     const uint32_t a0 = ca[u] & 0x1FFu, a1 = (ca[u] >> 16) & 0x1FFu;
@@ -1179,10 +1179,8 @@ struct Engine {
         if (initialized)
             throw std::runtime_error("Initialize was already called and may not be called again until cleanup was called!");
         if (!nSet || n == 0) throw std::runtime_error("setNrOfAllMonomers must be called with n > 0 before initialize");
-        for (int a = 0; a < 3; ++a) {
+        for (int a = 0; a < 3; ++a)
             if (L[a] == 0) throw std::runtime_error("setLatticeSize must be called before initialize");
-            if (!periodic[a]) throw std::runtime_error("only fully periodic boxes are supported by this build");
-        }
         if (rng != BFM_RNG_INTHASH && rng != BFM_RNG_SARU && rng != BFM_RNG_PHILOX)
             throw std::runtime_error("random number generator " + std::to_string(rng) +
                                      " is not provided by this build (IntHash = 1, Saru = 2, Philox = 3)");
@@ -1203,7 +1201,18 @@ struct Engine {
         Lm = (uint32_t)std::max(L[0], std::max(L[1], L[2]));
         keyBits = 3 * ilog2(Lm);
         latWords = ((size_t)Lm * Lm * Lm) / 32;
-        for (int a = 0; a < 3; ++a) g.m[a] = dilate3((uint32_t)L[a] - 1) << a;
+        g.open = 0;
+        for (int a = 0; a < 3; ++a) {
+            g.m[a] = dilate3((uint32_t)L[a] - 1) << a;
+            g.top[a] = periodic[a] ? 0u : dilate3((uint32_t)L[a] - 2) << a;
+            if (!periodic[a]) g.open |= 1u << a;
+        }
+        /* along a non-periodic axis every cube lies inside the box: corner in 0 .. L-2 */
+        for (uint32_t i = 0; i < n; ++i)
+            for (int a = 0; a < 3; ++a)
+                if (!periodic[a] && (xyz[3 * (size_t)i + a] < 0 || xyz[3 * (size_t)i + a] > (int64_t)L[a] - 2))
+                    throw InvalidArgument("monomer " + std::to_string(i) + " lies outside the box along the non-periodic axis " +
+                                          std::string(1, "xyz"[a]));
 
         /* graph colouring (initializeSpeciesSorting, .cu:1561-1686) */
         for (uint32_t i = 0; i < n; ++i)

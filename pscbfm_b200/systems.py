@@ -60,6 +60,7 @@ class System:
     chains: list = field(default_factory=list)   # (first id, length) of linear chains
     attributes: np.ndarray | None = None
     name: str = ""
+    periodic: tuple = (True, True, True)
 
     @property
     def n(self) -> int:
@@ -159,6 +160,58 @@ def saw_chains(n_chains: int, chain_len: int, box=(128, 128, 128), seed: int = 1
     return System(tuple(int(b) for b in box), pos.astype(np.int32), deg, nbr,
                   chains=[(c * chain_len, chain_len) for c in range(n_chains)], attributes=attrs,
                   name=f"saw_{n_chains}x{chain_len}_L{box[0]}")
+
+
+def open_box_chains(n_chains: int, chain_len: int, box=(32, 32, 32), seed: int = 12345,
+                    periodic=(False, False, False), max_tries: int = 200) -> System:
+    """Linear self-avoiding chains in a box whose axes marked False are
+    walls: along those axes every cube corner lies in 0 .. L-2.  Grown like
+    saw_chains, with positions outside the walls refused."""
+    rng = np.random.default_rng(seed)
+    occ = _Occupancy(box)
+    lo = np.array([0 if not p else -(1 << 30) for p in periodic], dtype=np.int64)
+    hi = np.array([box[a] - 2 if not periodic[a] else (1 << 30) for a in range(3)], dtype=np.int64)
+
+    def fits(q):
+        return bool((q >= lo).all() and (q <= hi).all()) and occ.free(q)
+
+    n = n_chains * chain_len
+    pos = np.zeros((n, 3), np.int64)
+    deg, nbr = _empty_topology(n)
+    bvec = BONDS_108.astype(np.int64)
+    for c in range(n_chains):
+        first = c * chain_len
+        for _ in range(max_tries):
+            start = np.array([rng.integers(0, box[a] - 1 if not periodic[a] else box[a]) for a in range(3)])
+            if not fits(start):
+                continue
+            occ.set(start)
+            pos[first] = start
+            ok = True
+            for k in range(1, chain_len):
+                prev = pos[first + k - 1]
+                placed = False
+                for bi in rng.permutation(108):
+                    cand = prev + bvec[bi]
+                    if fits(cand):
+                        occ.set(cand)
+                        pos[first + k] = cand
+                        placed = True
+                        break
+                if not placed:
+                    for q in range(k):
+                        occ.set(pos[first + q], False)
+                    ok = False
+                    break
+            if ok:
+                break
+        else:
+            raise RuntimeError("could not place chain %d" % c)
+        for k in range(1, chain_len):
+            _connect(deg, nbr, first + k - 1, first + k)
+    return System(tuple(int(b) for b in box), pos.astype(np.int32), deg, nbr,
+                  chains=[(c * chain_len, chain_len) for c in range(n_chains)],
+                  name=f"open_{n_chains}x{chain_len}_L{box[0]}", periodic=tuple(bool(p) for p in periodic))
 
 
 def ordered_melt(L: int = 256, chain_len: int | None = None) -> System:

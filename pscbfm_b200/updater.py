@@ -291,7 +291,7 @@ class UpdaterGPUScBFM_AB_Type:
         self.setRng(rng)
         self.setAge(age)
         self.setStepsBetweenSortings(steps_between_sortings)
-        self.setPeriodicity(True, True, True)
+        self.setPeriodicity(*getattr(system, "periodic", (True, True, True)))
         self.setLatticeSize(*system.box)
         self.setNrOfAllMonomers(system.n)
         self.setAllMonomerCoordinates(system.pos)
