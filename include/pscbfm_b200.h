@@ -171,6 +171,19 @@ int bfm_barrier_selftest_variant(int gpu, uint32_t timeout_ms, uint32_t extra_ar
  * colors[n] receives the colours, *ncolors their number. */
 int bfm_color_graph(uint32_t n, const uint8_t *deg, const uint32_t *nbr8, int uniform, uint32_t *colors,
                     uint32_t *ncolors);
+/* The same colours for a forest (linear chains, stars, combs), with the
+ * reference's depth-first walk (graphColoring.tpp:176-351) replaced by a
+ * parity union-find on GPU `gpu`: on a forest the walk gives every node the
+ * parity of its distance to the lowest id of its component; the uniform
+ * rebalancing pass then runs on the host as in bfm_color_graph.  A graph
+ * that is not a forest is coloured on the host; *on_device tells which. */
+int bfm_color_graph_device(int gpu, uint32_t n, const uint8_t *deg, const uint32_t *nbr8, int uniform, uint32_t *colors,
+                           uint32_t *ncolors, int *on_device);
+/* colouring at initialize: 0 the host walk (default), 1 the device for
+ * forests (same colours, see bfm_color_graph_device); bfm_get_coloring
+ * reports the mode and whether the last initialize coloured on the device */
+int bfm_set_coloring(bfm_handle *h, int mode);
+int bfm_get_coloring(const bfm_handle *h, int *mode, int *on_device);
 
 /* One colour substep (check + perform) on device arrays the caller owns,
  * without allocating any device memory.  No counterpart in the reference:

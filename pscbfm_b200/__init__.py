@@ -13,6 +13,7 @@ from .updater import (  # noqa: F401
     DeviceTimeout,
     Rng,
     UpdaterGPUScBFM_AB_Type,
+    color_graph,
     r250_get_state,
     r250_rand32,
     r250_seed,

@@ -18,8 +18,8 @@ LIBNAME = "libpscbfm_b200.so"
 LIBPATH = os.path.join(HERE, LIBNAME)
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["bfm_engine.cu", "bfm_diag.cu"]
-HEADERS = ["bfm_device.cuh", "bfm_host.hpp", "bfm_sweep.cuh", "bfm_analyze.cuh", "../../include/pscbfm_b200.h"]
+SOURCES = ["bfm_engine.cu", "bfm_diag.cu", "bfm_color.cu"]
+HEADERS = ["bfm_device.cuh", "bfm_host.hpp", "bfm_sweep.cuh", "bfm_analyze.cuh", "bfm_color.hpp", "../../include/pscbfm_b200.h"]
 
 NVCC_FLAGS = [
     "-std=c++17",
@@ -120,6 +120,9 @@ _SIGS = {
     "bfm_barrier_selftest_variant": (_c.c_int, [_c.c_int, _c.c_uint32, _c.c_uint32, _c.c_uint32, _c.c_int, _c.c_uint32,
                                                 _c.POINTER(_c.c_double)]),
     "bfm_color_graph": (_c.c_int, [_c.c_uint32, _P, _P, _c.c_int, _P, _P]),
+    "bfm_color_graph_device": (_c.c_int, [_c.c_int, _c.c_uint32, _P, _P, _c.c_int, _P, _P, _P]),
+    "bfm_set_coloring": (_c.c_int, [_P, _c.c_int]),
+    "bfm_get_coloring": (_c.c_int, [_P, _P, _P]),
     "bfm_substep_noalloc": (_c.c_int, [_P, _P, _P, _P, _c.c_uint32, _P, _c.c_uint32, _c.c_uint32, _c.c_uint32, _P,
                                        _c.c_uint32, _c.c_uint32, _c.c_uint32, _c.c_uint32, _c.c_int, _P]),
     "bfm_debug_philox_vs_curand": (_c.c_int, [_c.c_int, _c.c_uint64, _c.c_uint64, _c.c_uint64, _c.c_uint32, _P]),

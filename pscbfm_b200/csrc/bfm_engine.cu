@@ -38,6 +38,7 @@
 #include "bfm_host.hpp"
 #include "bfm_sweep.cuh"
 #include "bfm_analyze.cuh"
+#include "bfm_color.hpp"
 #include "../../include/pscbfm_b200.h"
 
 using namespace bfm;
@@ -1049,8 +1050,10 @@ struct Engine {
     int rng = BFM_RNG_INTHASH; /* the reference's default (.cu:1407) */
     int64_t sortEvery = 5000;
     int launchMode = 0;
+    int coloringMode = 0; /* 0 host walk (the reference's); 1 device for forests, host otherwise */
 
     /* ---- derived at initialize */
+    bool colorOnDevice = false;
     bool initialized = false;
     Geometry g{};
     Bondset bonds{};
@@ -1219,7 +1222,12 @@ struct Engine {
             for (uint32_t j = 0; j < deg[i]; ++j)
                 if (nbr[(size_t)i * 8 + j] >= n)
                     throw InvalidArgument("bond partner id out of range for monomer " + std::to_string(i));
-        color = color_graph(n, deg.data(), nbr.data(), true);
+        colorOnDevice = false;
+        if (coloringMode == 1) {
+            CK(cudaSetDevice(gpu));
+            colorOnDevice = color_forest_device(n, deg.data(), nbr.data(), true, color);
+        }
+        if (!colorOnDevice) color = color_graph(n, deg.data(), nbr.data(), true);
         nSpecies = 0;
         for (uint32_t i = 0; i < n; ++i) nSpecies = std::max(nSpecies, color[i] + 1);
         std::vector<uint32_t> count(nSpecies, 0);
@@ -2387,6 +2395,49 @@ int bfm_set_launch_mode(bfm_handle *h, int mode)
         if (mode < 0 || mode > 2) throw InvalidArgument("launch mode must be 0 (persistent), 1 (graphs) or 2 (direct)");
         h->e.launchMode = mode;
     });
+}
+
+int bfm_set_coloring(bfm_handle *h, int mode)
+{
+    GUARD(h, {
+        if (mode != 0 && mode != 1) throw InvalidArgument("colouring mode must be 0 (host) or 1 (device for forests)");
+        h->e.coloringMode = mode;
+    });
+}
+
+int bfm_get_coloring(const bfm_handle *h, int *mode, int *on_device)
+{
+    if (!h) return BFM_EINVAL;
+    if (mode) *mode = h->e.coloringMode;
+    if (on_device) *on_device = h->e.colorOnDevice ? 1 : 0;
+    return BFM_OK;
+}
+
+int bfm_color_graph_device(int gpu, uint32_t n, const uint8_t *deg, const uint32_t *nbr8, int uniform, uint32_t *colors,
+                           uint32_t *ncolors, int *on_device)
+{
+    if ((n && (!deg || !nbr8 || !colors)) || !ncolors) return BFM_EINVAL;
+    try {
+        for (uint32_t i = 0; i < n; ++i) {
+            if (deg[i] > 8) return BFM_EINVAL;
+            for (uint32_t j = 0; j < deg[i]; ++j)
+                if (nbr8[(size_t)i * 8 + j] >= n) return BFM_EINVAL;
+        }
+        if (cudaSetDevice(gpu) != cudaSuccess) return BFM_ECUDA;
+        std::vector<uint32_t> c;
+        const bool dev = color_forest_device(n, deg, nbr8, uniform != 0, c);
+        if (!dev) c = color_graph(n, deg, nbr8, uniform != 0);
+        uint32_t k = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            colors[i] = c[i];
+            k = std::max(k, c[i] + 1);
+        }
+        *ncolors = k;
+        if (on_device) *on_device = dev ? 1 : 0;
+        return BFM_OK;
+    } catch (std::exception const &) {
+        return BFM_ECUDA;
+    }
 }
 
 int bfm_color_graph(uint32_t n, const uint8_t *deg, const uint32_t *nbr8, int uniform, uint32_t *colors, uint32_t *ncolors)

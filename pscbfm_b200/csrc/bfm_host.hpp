@@ -66,12 +66,12 @@ struct R250 {
  *     do not use, scanning the colours rarest-first (the scan goes on after a
  *     move, as in the reference).
  * nbr holds 8 slots per node.  Throws std::runtime_error past 255 colours. */
-inline std::vector<uint32_t> color_graph(uint32_t n, const uint8_t *deg, const uint32_t *nbr, bool uniform)
+inline std::vector<uint32_t> dfs_colors(uint32_t n, const uint8_t *deg, const uint32_t *nbr, std::vector<size_t> &count)
 {
     const uint32_t kNone = 0xFFFFFFFFu;
     const int64_t kNoNode = -1;
     std::vector<uint32_t> color(n, kNone);
-    std::vector<size_t> count;
+    count.clear();
     std::vector<uint8_t> taken(256);
     for (uint32_t root = 0; root < n; ++root) {
         if (color[root] != kNone) continue;
@@ -116,7 +116,14 @@ inline std::vector<uint32_t> color_graph(uint32_t n, const uint8_t *deg, const u
             }
         }
     }
-    if (uniform && !count.empty()) {
+    return color;
+}
+
+/* step 2 of color_graph on a colouring and its colour counts */
+inline void rebalance_colors(uint32_t n, const uint8_t *deg, const uint32_t *nbr, std::vector<uint32_t> &color,
+                             std::vector<size_t> &count)
+{
+    if (!count.empty()) {
         using Entry = std::pair<uint32_t, size_t>;
         const size_t k = count.size();
         std::vector<Entry> rarest(k);
@@ -144,6 +151,13 @@ inline std::vector<uint32_t> color_graph(uint32_t n, const uint8_t *deg, const u
             }
         }
     }
+}
+
+inline std::vector<uint32_t> color_graph(uint32_t n, const uint8_t *deg, const uint32_t *nbr, bool uniform)
+{
+    std::vector<size_t> count;
+    std::vector<uint32_t> color = dfs_colors(n, deg, nbr, count);
+    if (uniform) rebalance_colors(n, deg, nbr, color, count);
     return color;
 }
 

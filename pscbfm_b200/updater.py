@@ -184,6 +184,16 @@ class UpdaterGPUScBFM_AB_Type:
         self._check(self._lib.bfm_get_positions(self._h, out.ctypes.data, self._n))
         return out
 
+    def setColoring(self, mode: int):
+        """colouring at initialize: 0 host walk (default), 1 device for forests"""
+        self._check(self._lib.bfm_set_coloring(self._h, int(mode)))
+
+    def getColoring(self):
+        """(mode, whether the last initialize coloured on the device)"""
+        m, d = ctypes.c_int(), ctypes.c_int()
+        self._check(self._lib.bfm_get_coloring(self._h, ctypes.byref(m), ctypes.byref(d)))
+        return m.value, bool(d.value)
+
     # ---- chain analysis on the device (the reference's AnalyzerMsd)
     def analyzerInit(self) -> int:
         """Find the linear chains (first end, middle, last end) by the
@@ -299,6 +309,30 @@ class UpdaterGPUScBFM_AB_Type:
         self.setBondSet(system.allowed)
         self.initialize()
         return self
+
+
+def color_graph(deg, nbr, uniform: bool = True, device: bool = False, gpu: int = 0):
+    """The species colouring initialize() uses (the reference's
+    graphColoring with uniform rebalancing).  device=True computes the same
+    colours of a forest on the GPU (see bfm_color_graph_device).  Returns
+    (colours, number of colours, coloured on the device)."""
+    d = np.ascontiguousarray(deg, dtype=np.uint8)
+    b = np.ascontiguousarray(nbr, dtype=np.uint32)
+    n = d.size
+    col = np.zeros(n, dtype=np.uint32)
+    nc = ctypes.c_uint32()
+    lib = _native.lib()
+    if device:
+        dev = ctypes.c_int()
+        st = lib.bfm_color_graph_device(int(gpu), n, d.ctypes.data, b.ctypes.data, int(uniform), col.ctypes.data,
+                                        ctypes.byref(nc), ctypes.byref(dev))
+        on_dev = bool(dev.value)
+    else:
+        st = lib.bfm_color_graph(n, d.ctypes.data, b.ctypes.data, int(uniform), col.ctypes.data, ctypes.byref(nc))
+        on_dev = False
+    if st != _native.BFM_OK:
+        _raise(st, f"colouring failed (status {st})")
+    return col, nc.value, on_dev
 
 
 # process-global R250 colour/seed generator (LeMonADE's RandomNumberGenerators)
