@@ -574,8 +574,14 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
  */
 constexpr uint32_t kWinMaxSpecies = 32;
 
+constexpr uint32_t kTabReplicas = 8; /* copies of every face-mask entry, read by lane % 8 */
+constexpr size_t kWinTableBytes = (size_t)4 * 192 * kTabReplicas * 8;
+
 /* Shared memory of the windowed kernel, for at most W items of one colour
- * and P items of all colours per CTA and T threads: positions of all the
+ * and P items of all colours per CTA and T threads: the face-mask table
+ * split by mask (word g of the face) and replicated kTabReplicas times so
+ * that lanes reading different entries rarely share a bank (48 KB),
+ * positions of all the
  * CTA's monomers (4 B), direction | bonds << 3 of this substep's items
  * (1 B), bond counts of all the CTA's monomers (1 B), then two sets (this
  * substep's and the previous one's) of per-warp candidate lists of
@@ -583,8 +589,9 @@ constexpr uint32_t kWinMaxSpecies = 32;
 struct WinLayout {
     uint32_t W, T, P;
     __host__ __device__ uint32_t seg() const { return 32u * ((W + T - 1u) / T); }
-    __host__ __device__ size_t pos() const { return 0; }
-    __host__ __device__ size_t x() const { return (size_t)P * 4; }
+    __host__ __device__ size_t table() const { return 0; }
+    __host__ __device__ size_t pos() const { return kWinTableBytes; }
+    __host__ __device__ size_t x() const { return pos() + (size_t)P * 4; }
     __host__ __device__ size_t deg() const { return x() + W; }
     __host__ __device__ size_t lists() const { return (deg() + P + 15) & ~(size_t)15; }
     __host__ __device__ size_t bytes() const { return lists() + (size_t)2 * (T / 32u) * seg() * 8u; }
@@ -637,19 +644,24 @@ __global__ void __launch_bounds__(1024, 1)
 {
     const uint32_t T = blockDim.x, NW = T >> 5;
     extern __shared__ __align__(16) unsigned char s_dyn[];
-    __shared__ __align__(16) unsigned long long s_table[kFaceTableA];
     __shared__ uint32_t s_after[6 * 16];
     __shared__ uint32_t s_lo[kWinMaxSpecies], s_n[kWinMaxSpecies], s_off[kWinMaxSpecies], s_base[kWinMaxSpecies];
     __shared__ unsigned int s_wcnt[2][32];
 
     const WinLayout lay{window, T, ptotal};
     const uint32_t seg = lay.seg();
+    unsigned long long *s_tab = reinterpret_cast<unsigned long long *>(s_dyn + lay.table());
     uint32_t *spos = reinterpret_cast<uint32_t *>(s_dyn + lay.pos());
     uint8_t *px = s_dyn + lay.x();
     uint8_t *sdeg = s_dyn + lay.deg();
     uint2 *lists = reinterpret_cast<uint2 *>(s_dyn + lay.lists());
 
-    build_face_table_a(s_table);
+    for (uint32_t e = threadIdx.x; e < 192; e += T) {
+        unsigned long long m[4];
+        face_table_entry((int)e, m);
+        for (uint32_t g = 0; g < 4; ++g)
+            for (uint32_t r = 0; r < kTabReplicas; ++r) s_tab[((size_t)g * 192 + e) * kTabReplicas + r] = m[g];
+    }
     for (uint32_t e = threadIdx.x; e < 96; e += T) { /* the CTA may have fewer than 96 threads */
         const uint32_t dir = e >> 4, w = e & 15u, ax = dir >> 1;
         uint32_t bits = 0;
@@ -717,14 +729,16 @@ __global__ void __launch_bounds__(1024, 1)
             tp[zstep(e.y, (int)(e.x >> 28), geo) >> 6] = 0ull;
         }
     };
-    /* occupied sites of a face */
+    /* occupied sites of a face: which of words 1..3 it touches follows from
+     * the table entry (the transverse ranges spill over when lb, lc >= 2) */
     auto occupied = [&](const unsigned long long *L, const FaceW &fw) -> unsigned long long {
-        const ulonglong2 *tp = reinterpret_cast<const ulonglong2 *>(s_table + (fw.t << 2));
-        const ulonglong2 m01 = tp[0], m23 = tp[1];
-        unsigned long long o = L[fw.w[0]] & m01.x;
-        if (m01.y) o |= L[fw.w[1]] & m01.y;
-        if (m23.x) o |= L[fw.w[2]] & m23.x;
-        if (m23.y) o |= L[fw.w[3]] & m23.y;
+        const bool sb = ((fw.t >> 2) & 3u) >= 2u, sc = (fw.t & 3u) >= 2u;
+        const unsigned long long *tp = s_tab + (size_t)fw.t * kTabReplicas + (lane & (kTabReplicas - 1u));
+        constexpr size_t G = (size_t)192 * kTabReplicas;
+        unsigned long long o = L[fw.w[0]] & tp[0];
+        if (sb) o |= L[fw.w[1]] & tp[G];
+        if (sc) o |= L[fw.w[2]] & tp[2 * G];
+        if (sb && sc) o |= L[fw.w[3]] & tp[3 * G];
         return o;
     };
 
@@ -1500,9 +1514,7 @@ struct Engine {
             return;
         }
         if (storedBonds) {
-            /* 4 items in flight when a CTA has more than a thousand per colour */
-            const int v = (nmax + (uint32_t)smCount - 1u) / (uint32_t)smCount > 1024u ? 2 : 1;
-            if (configureWindowed<RNG>(smCount, smemLimit, v)) return;
+            if (configureWindowed<RNG>(smCount, smemLimit, 1)) return; /* 2 items in flight per thread */
             if (configureFor<RNG, SWEEP_STAGED>(smCount, smemLimit)) return;
             if (configureFor<RNG, SWEEP_STORED>(smCount, smemLimit)) return;
         }
