@@ -246,16 +246,50 @@ enum SweepMode {
     SWEEP_WINDOWED = 6 /* stored codes; independent work done inside the barrier waits (k_sweep_w), 6..8 */
 };
 
+/* The face-mask table in shared memory, split by word g of the face and
+ * replicated kTabReplicas times (entry e, word g, copy r at
+ * (g * 192 + e) * kTabReplicas + r), read by lane % kTabReplicas: lanes
+ * reading different entries rarely share a bank.  48 KB. */
+constexpr uint32_t kTabReplicas = 8;
+constexpr size_t kWinTableBytes = (size_t)4 * 192 * kTabReplicas * 8;
+
+__device__ __forceinline__ void build_split_table(unsigned long long *tab)
+{
+    for (uint32_t e = threadIdx.x; e < 192; e += blockDim.x) {
+        unsigned long long m[4];
+        face_table_entry((int)e, m);
+        for (uint32_t g = 0; g < 4; ++g)
+            for (uint32_t r = 0; r < kTabReplicas; ++r) tab[((size_t)g * 192 + e) * kTabReplicas + r] = m[g];
+    }
+}
+
+/* occupied sites of a face in lattice L; which of words 1..3 it touches
+ * follows from the table entry (the transverse ranges spill over into the
+ * next brick when lb, lc >= 2), so the loads do not wait for the masks */
+__device__ __forceinline__ unsigned long long split_occupied(const unsigned long long *L, const FaceW &fw,
+                                                             const unsigned long long *tab, uint32_t lane)
+{
+    const bool sb = ((fw.t >> 2) & 3u) >= 2u, sc = (fw.t & 3u) >= 2u;
+    const unsigned long long *tp = tab + (size_t)fw.t * kTabReplicas + (lane & (kTabReplicas - 1u));
+    constexpr size_t G = (size_t)192 * kTabReplicas;
+    unsigned long long o = L[fw.w[0]] & tp[0];
+    if (sb) o |= L[fw.w[1]] & tp[G];
+    if (sc) o |= L[fw.w[2]] & tp[2 * G];
+    if (sb && sc) o |= L[fw.w[3]] & tp[3 * G];
+    return o;
+}
+
 /* Shared-memory layout of the staged mode for a window of W items (W a
- * multiple of 16): positions (4 B), bond codes rows 0 and 1 (one 32-bit
- * word), bond count and direction (1 B each), then the candidate list. */
+ * multiple of 16), after the face-mask table: positions (4 B), bond codes
+ * rows 0 and 1 (one 32-bit word), bond count and direction (1 B each), then
+ * the candidate list (all modes keep the table first). */
 struct StageLayout {
     uint32_t W;
-    __host__ __device__ size_t pos() const { return 0; }
-    __host__ __device__ size_t bc() const { return (size_t)W * 4; }
-    __host__ __device__ size_t dg() const { return (size_t)W * 8; }
-    __host__ __device__ size_t dirs() const { return (size_t)W * 9; }
-    __host__ __device__ size_t list() const { return (size_t)W * 10; }
+    __host__ __device__ size_t pos() const { return kWinTableBytes; }
+    __host__ __device__ size_t bc() const { return kWinTableBytes + (size_t)W * 4; }
+    __host__ __device__ size_t dg() const { return kWinTableBytes + (size_t)W * 8; }
+    __host__ __device__ size_t dirs() const { return kWinTableBytes + (size_t)W * 9; }
+    __host__ __device__ size_t list() const { return kWinTableBytes + (size_t)W * 10; }
     __host__ __device__ size_t bytes(uint32_t cap) const { return list() + (size_t)cap * 8; }
 };
 
@@ -271,7 +305,6 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
     constexpr bool STORED = MODE != SWEEP_GATHER;
     constexpr bool STAGE = MODE == SWEEP_STAGED;
     extern __shared__ __align__(16) unsigned char s_dyn[];
-    __shared__ __align__(16) unsigned long long s_table[kFaceTableA];
     __shared__ __align__(16) DirConst s_dir[6];
     __shared__ uint32_t s_forbid[16];
     __shared__ uint32_t s_after[6 * 16]; /* forbidden after a move in dir: bit (code) of row dir */
@@ -283,9 +316,10 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
     uint32_t *st_bc = reinterpret_cast<uint32_t *>(s_dyn + lay.bc());
     uint8_t *st_dg = s_dyn + lay.dg();
     uint8_t *st_dir = s_dyn + lay.dirs();
-    uint2 *list = glist ? glist + (size_t)blockIdx.x * cap : reinterpret_cast<uint2 *>(s_dyn + (STAGE ? lay.list() : 0));
+    uint2 *list = glist ? glist + (size_t)blockIdx.x * cap : reinterpret_cast<uint2 *>(s_dyn + (STAGE ? lay.list() : kWinTableBytes));
+    unsigned long long *s_tab = reinterpret_cast<unsigned long long *>(s_dyn);
 
-    build_face_table_a(s_table);
+    build_split_table(s_tab);
     build_dir_table(s_dir, s.g);
     if (threadIdx.x < 16) s_forbid[threadIdx.x] = s.bonds.forbidden[threadIdx.x];
     if (threadIdx.x < 96) {
@@ -416,11 +450,11 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
             if (valid) {
                 if (!STAGE) dir = direction(draw<RNG>(d.seed, d.iter, i, d.iterHi));
                 const DirConst dc = s_dir[dir];
-                const Face4 f = face4d(r0, dir, dc, s_table);
+                const FaceW fw = face_words(r0, dir, s.g);
                 const uint32_t r1 = dstep(r0, dir, dc);
                 if (STORED) {
                     const uint32_t *after = s_after + dir * 16;
-                    ok = !face4_occupied(lat, f) && !leaves_box(r0, dir, s.g);
+                    ok = !split_occupied(lat, fw, s_tab, lane) && !leaves_box(r0, dir, s.g);
                     if (dg > 0) ok = ok && !((after[ea >> 5] >> (ea & 31u)) & 1u);
                     if (dg > 1) ok = ok && !((after[eb >> 5] >> (eb & 31u)) & 1u);
                     for (uint32_t j = 2; j < dg; ++j) {
@@ -430,7 +464,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
                 } else {
                     const uint32_t p0 = pos[ea];
                     const uint32_t p1 = pos[eb];
-                    ok = !face4_occupied(lat, f) && !leaves_box(r0, dir, s.g);
+                    ok = !split_occupied(lat, fw, s_tab, lane) && !leaves_box(r0, dir, s.g);
                     if (dg > 0) {
                         const uint32_t c = zbond(p0, r1);
                         ok = ok && !((s_forbid[c >> 5] >> (c & 31u)) & 1u);
@@ -471,7 +505,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
                 const uint32_t slot = e.x & 0x0FFFFFFFu;
                 const uint32_t r0 = e.y;
                 const DirConst dc = s_dir[dir];
-                const Face4 f = face4d(r0, dir, dc, s_table);
+                const FaceW fw = face_words(r0, dir, s.g);
                 /* bond data of a possible move, loaded together with the probe */
                 uint32_t dgm = 0, q0 = 0, q1 = 0, v0 = 0, v1 = 0, c0 = 0, c1 = 0;
                 if (STORED) {
@@ -488,7 +522,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
                         v1 = s.rev[(size_t)npad + slot];
                     }
                 }
-                if (face4_occupied(tr, f)) continue;
+                if (split_occupied(tr, fw, s_tab, lane)) continue;
                 const uint32_t r1 = dstep(r0, dir, dc);
                 const uint32_t w0 = r0 >> 6, w1 = r1 >> 6;
                 const unsigned long long b0 = 1ull << (r0 & 63u), b1 = 1ull << (r1 & 63u);
@@ -574,9 +608,6 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
  */
 constexpr uint32_t kWinMaxSpecies = 32;
 
-constexpr uint32_t kTabReplicas = 8; /* copies of every face-mask entry, read by lane % 8 */
-constexpr size_t kWinTableBytes = (size_t)4 * 192 * kTabReplicas * 8;
-
 /* Shared memory of the windowed kernel, for at most W items of one colour
  * and P items of all colours per CTA and T threads: the face-mask table
  * split by mask (word g of the face) and replicated kTabReplicas times so
@@ -656,12 +687,7 @@ __global__ void __launch_bounds__(1024, 1)
     uint8_t *sdeg = s_dyn + lay.deg();
     uint2 *lists = reinterpret_cast<uint2 *>(s_dyn + lay.lists());
 
-    for (uint32_t e = threadIdx.x; e < 192; e += T) {
-        unsigned long long m[4];
-        face_table_entry((int)e, m);
-        for (uint32_t g = 0; g < 4; ++g)
-            for (uint32_t r = 0; r < kTabReplicas; ++r) s_tab[((size_t)g * 192 + e) * kTabReplicas + r] = m[g];
-    }
+    build_split_table(s_tab);
     for (uint32_t e = threadIdx.x; e < 96; e += T) { /* the CTA may have fewer than 96 threads */
         const uint32_t dir = e >> 4, w = e & 15u, ax = dir >> 1;
         uint32_t bits = 0;
@@ -729,17 +755,8 @@ __global__ void __launch_bounds__(1024, 1)
             tp[zstep(e.y, (int)(e.x >> 28), geo) >> 6] = 0ull;
         }
     };
-    /* occupied sites of a face: which of words 1..3 it touches follows from
-     * the table entry (the transverse ranges spill over when lb, lc >= 2) */
     auto occupied = [&](const unsigned long long *L, const FaceW &fw) -> unsigned long long {
-        const bool sb = ((fw.t >> 2) & 3u) >= 2u, sc = (fw.t & 3u) >= 2u;
-        const unsigned long long *tp = s_tab + (size_t)fw.t * kTabReplicas + (lane & (kTabReplicas - 1u));
-        constexpr size_t G = (size_t)192 * kTabReplicas;
-        unsigned long long o = L[fw.w[0]] & tp[0];
-        if (sb) o |= L[fw.w[1]] & tp[G];
-        if (sc) o |= L[fw.w[2]] & tp[2 * G];
-        if (sb && sc) o |= L[fw.w[3]] & tp[3 * G];
-        return o;
+        return split_occupied(L, fw, s_tab, lane);
     };
 
     Substep d = sched[k0];
@@ -1424,6 +1441,7 @@ struct Engine {
     int forcedShape = -1; /* -1 automatic; 0..2 bond mode; +3: candidate lists in global memory; 6 windowed */
     int sweepThreads = kSweepThreads;
     uint32_t sweepTotal = 0; /* windowed kernel: most items of all colours one CTA owns */
+    bool sweepGlobalList = false; /* k_sweep: candidate lists in global memory */
 
     /* Persistent-kernel launch shape: one CTA per SM (cooperative launch,
      * all CTAs resident); each CTA owns 1/grid of every colour slab.  The
@@ -1439,22 +1457,24 @@ struct Engine {
         const uint32_t per = (nmax + grid - 1) / grid + 1u;
         const uint32_t cap = std::max<uint32_t>(32u, per);
         const uint32_t W = ((per + 15u) & ~15u) + 32u;
-        size_t smem = 0;
-        const bool globalList = forcedShape >= 3;
+        size_t smem = kWinTableBytes;
+        bool globalList = forcedShape >= 3;
         if (MODE == SWEEP_STAGED) {
             if (globalList) return false;
             smem = StageLayout{W}.bytes(cap);
             if (smem > smemLimit) return false;
         } else {
-            smem = !globalList && (size_t)cap * sizeof(uint2) <= kSweepSmemListMax ? (size_t)cap * sizeof(uint2) : 0;
+            if ((size_t)cap * sizeof(uint2) > kSweepSmemListMax) globalList = true;
+            if (!globalList) smem += (size_t)cap * sizeof(uint2);
         }
-        if (smem > 0) CK(cudaFuncSetAttribute(k_sweep<RNG, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CK(cudaFuncSetAttribute(k_sweep<RNG, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int fit = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k_sweep<RNG, MODE>, kSweepThreads, smem));
         if (fit < 1) return false;
         sweepGrid = (int)grid;
         sweepCap = cap;
         sweepSmem = smem;
+        sweepGlobalList = globalList;
         sweepWindow = W;
         sweepMode = MODE;
         sweepThreads = kSweepThreads;
@@ -1491,6 +1511,7 @@ struct Engine {
         sweepSmem = smem;
         sweepWindow = W;
         sweepMode = SWEEP_WINDOWED + variant;
+        sweepGlobalList = false;
         sweepThreads = (int)threads;
         sweepTotal = P;
         return true;
@@ -1537,13 +1558,13 @@ struct Engine {
         else
             configureRng<RNG_INTHASH>(sms, limit);
         dfree(d_glist);
-        if (sweepSmem == 0 && sweepMode < SWEEP_WINDOWED) dalloc(d_glist, (size_t)sweepGrid * sweepCap);
+        if (sweepGlobalList) dalloc(d_glist, (size_t)sweepGrid * sweepCap);
     }
 
     void launchSweep(const Substep *sched, uint32_t k0, uint32_t k1)
     {
         Sys s = sys();
-        uint2 *gl = sweepSmem ? nullptr : d_glist;
+        uint2 *gl = sweepGlobalList ? d_glist : nullptr;
         uint32_t cap = sweepCap;
         GridBarrier *bar = d_bar;
         unsigned long long to = timeoutNs;
