@@ -52,6 +52,9 @@ def parse():
     p.add_argument("--melt-mcs", type=int, default=2000)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--box", type=int, default=256,
+                   help="edge of the cubic melt (256: the 4096 x 256 benchmark melt; 512, 1024: the same density "
+                        "with chains of L monomers, states beyond L2)")
     p.add_argument("--sweep-shape", type=int, default=-1,
                    help="persistent-kernel shape (-1 automatic; see bfm_set_sweep_shape)")
     return p.parse_args()
@@ -181,9 +184,17 @@ def peaks():
 
 
 # --------------------------------------------------------------- workload
-def make_workload():
+def make_workload(box: int = 256):
     from pscbfm_b200 import systems
-    return systems.ordered_melt(256)
+    return systems.ordered_melt(box)
+
+
+def workload_name(box: int, system) -> str:
+    if box == 256:
+        return WORKLOAD
+    chains = len(system.chains)
+    return (f"dense linear melt: {chains} chains x N={system.n // chains} ({system.n:,} monomers), {box}^3 periodic "
+            f"lattice, volume fraction 0.5, 108-vector bond set, 2 colours, Saru RNG")
 
 
 def algorithmic_bytes(c: float, a: float, kbar: float, C: int = 4):
@@ -235,7 +246,7 @@ def run_b200(args, ranks):
     import pscbfm_b200 as pb
     gpu = ranks.local
     torch.cuda.set_device(gpu)
-    system = make_workload()
+    system = make_workload(args.box)
     pb.r250_seed(1000 + ranks.rank)
     u = pb.UpdaterGPUScBFM_AB_Type().setup(system, gpu=gpu, rng=pb.Rng.Saru)
     if args.sweep_shape != -1:
@@ -295,7 +306,7 @@ def run_b200(args, ranks):
     achieved = bytes_launch / t_launch / 1e9
     traffic = None
     kname = "k_sweep_w" if launch_info.get("mode", 0) >= 6 else "k_sweep"
-    prof = os.path.join(HERE, "profiles", f"{kname}_melt256_traffic.json")
+    prof = os.path.join(HERE, "profiles", f"{kname}_melt{args.box}_traffic.json")
     if os.path.exists(prof):
         try:
             # DRAM bytes per attempted move from one ncu capture of a shorter
@@ -317,7 +328,7 @@ def run_b200(args, ranks):
         "vs_baseline": None,
         "dtype": "u32",
         "data": "synthetic (seeded serpentine melt of the stated shape, melted in place before warm-up)",
-        "config": {"workload": WORKLOAD, "mcs_per_step": S, "monomers": system.n, "box": list(system.box),
+        "config": {"workload": workload_name(args.box, system), "mcs_per_step": S, "monomers": system.n, "box": list(system.box),
                    "colours": nspec, "replicas": ranks.world,
                    "l2": "flushed before every step (256 MiB write); the 19 MiB state is L2-resident within a step",
                    "launch": "one persistent cooperative kernel per chunk of up to 4096 colour substeps",
@@ -344,6 +355,10 @@ def run_b200(args, ranks):
 
 def run_reference(args, ranks):
     if ranks.rank != 0:
+        return
+    if args.box != 256:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's 8-bit device coordinates take boxes of "
+                                                               "at most 256 per axis"}), flush=True)
         return
     from oracle import oracle
     system = make_workload()
