@@ -135,45 +135,6 @@ __host__ __device__ inline Face zface(uint32_t r0, int dir, const Geometry &g)
     return f;
 }
 
-/* The leading face in 64-bit lattice words.  A word holds the 4x4x4 brick
- * of sites sharing all code bits above bit 5, so three consecutive values of
- * a transverse axis fall into at most two bricks and the nine face sites into
- * at most four words (2.25 on average).  w[k] / m[k]: word index and the mask
- * of face sites inside it; m[k] == 0 means word k is not needed. */
-struct FaceWords {
-    uint32_t w[4];
-    unsigned long long m[4];
-};
-
-__host__ __device__ inline FaceWords zface_words(uint32_t r0, int dir, const Geometry &g)
-{
-    const Face f = zface(r0, dir, g);
-    const uint32_t bh = f.base >> 6, bl = f.base & 63u;
-    const uint32_t hb0 = f.b[0] >> 6, hb2 = f.b[2] >> 6;
-    const uint32_t hc0 = f.c[0] >> 6, hc2 = f.c[2] >> 6;
-    FaceWords out;
-    out.m[0] = out.m[1] = out.m[2] = out.m[3] = 0ull;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        const uint32_t gb = (f.b[i] >> 6) != hb0 ? 1u : 0u;
-        const uint32_t lb = bl | (f.b[i] & 63u);
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            const uint32_t gc = (f.c[j] >> 6) != hc0 ? 2u : 0u;
-            const unsigned long long bit = 1ull << (lb | (f.c[j] & 63u));
-            const uint32_t k = gb | gc;
-            out.m[0] |= k == 0 ? bit : 0ull;
-            out.m[1] |= k == 1 ? bit : 0ull;
-            out.m[2] |= k == 2 ? bit : 0ull;
-            out.m[3] |= k == 3 ? bit : 0ull;
-        }
-    }
-    out.w[0] = bh | hb0 | hc0;
-    out.w[1] = bh | hb2 | hc0;
-    out.w[2] = bh | hb0 | hc2;
-    out.w[3] = bh | hb2 | hc2;
-    return out;
-}
 
 /* Leading face with its masks in closed form (no table lookups).  The sites
  * of a 4x4x4 brick whose coordinate along axis k lies in a value set V

@@ -19,8 +19,8 @@
  * its previous candidates (the target lattice is double buffered, so this
  * never races with the marks of the running substep).  Lattices are read as
  * 64-bit words: a word is a 4x4x4 brick of sites in Z-order, so the nine
- * sites of a leading face lie in at most four words, whose masks come from a
- * per-CTA table.
+ * sites of a leading face lie in at most four words (face_words), whose
+ * masks come from a table in shared memory (face_table_entry).
  *
  * Grid barriers wait with a bound: after `timeoutNs` of %globaltimer (or a
  * fixed number of polls) a waiting CTA raises the error word and every CTA
@@ -232,45 +232,6 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, uint3
     return false;
 }
 
-/* Face-mask table: for a move along axis a and the low two bits lb, lc of the
- * first transverse values (b-1, c-1), the masks of the nine face sites in the
- * (up to) four bricks, with the move axis' own bits still zero.  Entry
- * ((a*4 + lb)*4 + lc)*4 + (gb | gc<<1). */
-constexpr int kFaceTable = 3 * 4 * 4 * 4;
-
-__device__ __forceinline__ void build_face_table(unsigned long long *t)
-{
-    for (int e = threadIdx.x; e < 48; e += blockDim.x) {
-        const int a = e >> 4, lb = (e >> 2) & 3, lc = e & 3;
-        const int bx = (a == 0) ? 1 : 0;
-        const int cx = (a == 2) ? 1 : 2;
-        unsigned long long m[4] = {0, 0, 0, 0};
-        for (int ib = 0; ib < 3; ++ib)
-            for (int ic = 0; ic < 3; ++ic) {
-                const int vb = lb + ib, vc = lc + ic;
-                const int g = (vb >= 4 ? 1 : 0) | (vc >= 4 ? 2 : 0);
-                const uint32_t ub = (uint32_t)(vb & 3), uc = (uint32_t)(vc & 3);
-                const uint32_t bit = (((ub & 1u) | ((ub & 2u) << 2)) << bx) | (((uc & 1u) | ((uc & 2u) << 2)) << cx);
-                m[g] |= 1ull << bit;
-            }
-        for (int g = 0; g < 4; ++g) t[e * 4 + g] = m[g];
-    }
-}
-
-struct Face4 {
-    uint32_t w[4];
-    unsigned long long m[4];
-};
-
-/* Face-mask table including the move axis' own two low bits la:
- * entry (((ax*4 + la)*4 + lb)*4 + lc)*4 + (gb | gc<<1). 6 KiB. */
-constexpr int kFaceTableA = 3 * 4 * 4 * 4 * 4;
-
-__device__ __forceinline__ void build_face_table_a(unsigned long long *t)
-{
-    for (int e = threadIdx.x; e < 192; e += blockDim.x) face_table_entry(e, t + e * 4);
-}
-
 /* Per-direction constants: payload masks of the move axis and of the two
  * transverse axes, their unit bits, and the bit position of the transverse
  * axes (for extracting their two low coordinate bits). */
@@ -302,118 +263,6 @@ __device__ __forceinline__ void build_dir_table(DirConst *t, const Geometry &g)
 __device__ __forceinline__ uint32_t dstep(uint32_t a, int dir, const DirConst &d)
 {
     return (dir & 1) ? ((a & ~d.ma) | (((a | ~d.ma) + d.ua) & d.ma)) : ((a & ~d.ma) | (((a & d.ma) - d.ua) & d.ma));
-}
-
-/* The leading face as <= 4 (word, mask), from the direction constants and
- * the table with the move axis' bits included. */
-__device__ __forceinline__ Face4 face4d(uint32_t r0, int dir, const DirConst &d, const unsigned long long *tableA)
-{
-    const uint32_t two = d.ua << 3; /* dilated 2 along the move axis */
-    const uint32_t pa = (dir & 1) ? (((r0 | ~d.ma) + two) & d.ma) : (((r0 & d.ma) - two) & d.ma);
-    const uint32_t b0 = ((r0 & d.mb) - d.ub) & d.mb;
-    const uint32_t b2 = ((r0 | ~d.mb) + d.ub) & d.mb;
-    const uint32_t c0 = ((r0 & d.mc) - d.uc) & d.mc;
-    const uint32_t c2 = ((r0 | ~d.mc) + d.uc) & d.mc;
-    const uint32_t ax = (uint32_t)(dir >> 1);
-    const uint32_t la = ((pa >> ax) & 1u) | ((pa >> (ax + 2)) & 2u);
-    const uint32_t lb = ((b0 >> d.bx) & 1u) | ((b0 >> (d.bx + 2)) & 2u);
-    const uint32_t lc = ((c0 >> d.cx) & 1u) | ((c0 >> (d.cx + 2)) & 2u);
-    const ulonglong2 *t = reinterpret_cast<const ulonglong2 *>(tableA + ((((ax * 4u + la) * 4u + lb) * 4u + lc) << 2));
-    const ulonglong2 t01 = t[0], t23 = t[1];
-    const uint32_t ha = pa >> 6, hb0 = b0 >> 6, hb2 = b2 >> 6, hc0 = c0 >> 6, hc2 = c2 >> 6;
-    Face4 f;
-    f.w[0] = ha | hb0 | hc0;
-    f.w[1] = ha | hb2 | hc0;
-    f.w[2] = ha | hb0 | hc2;
-    f.w[3] = ha | hb2 | hc2;
-    f.m[0] = t01.x;
-    f.m[1] = t01.y;
-    f.m[2] = t23.x;
-    f.m[3] = t23.y;
-    return f;
-}
-
-/* The leading face as four word indices plus the index of its mask entry
- * in the table of build_face_table_a (masks fetched where they are used). */
-struct FaceT {
-    uint32_t w[4];
-    uint32_t t;
-};
-
-__device__ __forceinline__ FaceT face4t(uint32_t r0, int dir, const DirConst &d)
-{
-    const uint32_t two = d.ua << 3;
-    const uint32_t pa = (dir & 1) ? (((r0 | ~d.ma) + two) & d.ma) : (((r0 & d.ma) - two) & d.ma);
-    const uint32_t b0 = ((r0 & d.mb) - d.ub) & d.mb;
-    const uint32_t b2 = ((r0 | ~d.mb) + d.ub) & d.mb;
-    const uint32_t c0 = ((r0 & d.mc) - d.uc) & d.mc;
-    const uint32_t c2 = ((r0 | ~d.mc) + d.uc) & d.mc;
-    const uint32_t ax = (uint32_t)(dir >> 1);
-    const uint32_t la = ((pa >> ax) & 1u) | ((pa >> (ax + 2)) & 2u);
-    const uint32_t lb = ((b0 >> d.bx) & 1u) | ((b0 >> (d.bx + 2)) & 2u);
-    const uint32_t lc = ((c0 >> d.cx) & 1u) | ((c0 >> (d.cx + 2)) & 2u);
-    const uint32_t ha = pa >> 6, hb0 = b0 >> 6, hb2 = b2 >> 6, hc0 = c0 >> 6, hc2 = c2 >> 6;
-    FaceT f;
-    f.w[0] = ha | hb0 | hc0;
-    f.w[1] = ha | hb2 | hc0;
-    f.w[2] = ha | hb0 | hc2;
-    f.w[3] = ha | hb2 | hc2;
-    f.t = ((ax * 4u + la) * 4u + lb) * 4u + lc;
-    return f;
-}
-
-/* occupied sites of a face given its words and table entry */
-__device__ __forceinline__ unsigned long long face_bits(const unsigned long long *lat, const uint32_t *w,
-                                                        const unsigned long long *tableA, uint32_t t)
-{
-    const ulonglong2 *tp = reinterpret_cast<const ulonglong2 *>(tableA + (t << 2));
-    const ulonglong2 m01 = tp[0], m23 = tp[1];
-    unsigned long long o = lat[w[0]] & m01.x;
-    if (m01.y) o |= lat[w[1]] & m01.y;
-    if (m23.x) o |= lat[w[2]] & m23.x;
-    if (m23.y) o |= lat[w[3]] & m23.y;
-    return o;
-}
-
-/* The leading face of a monomer at r0 moving in dir as <= 4 (word, mask). */
-__device__ __forceinline__ Face4 face4(uint32_t r0, int dir, const Geometry &g, const unsigned long long *table)
-{
-    const int ax = dir >> 1;
-    const int bx = (ax == 0) ? 1 : 0;
-    const int cx = (ax == 2) ? 1 : 2;
-    const uint32_t ua = 1u << ax;
-    const uint32_t ma = axis_mask(g, ax), mb = axis_mask(g, bx), mc = axis_mask(g, cx);
-    const uint32_t p = (dir & 1) ? zinc(zinc(r0, ma, ua), ma, ua) : zdec(zdec(r0, ma, ua), ma, ua);
-    const uint32_t pa = p & ma;
-    const uint32_t ub = 1u << bx, uc = 1u << cx;
-    const uint32_t b0 = ((p & mb) - ub) & mb;           /* dilated b-1 */
-    const uint32_t b2 = (((p & mb) | ~mb) + ub) & mb;   /* dilated b+1 */
-    const uint32_t c0 = ((p & mc) - uc) & mc;
-    const uint32_t c2 = (((p & mc) | ~mc) + uc) & mc;
-    const uint32_t lb = ((b0 >> bx) & 1u) | ((b0 >> (bx + 2)) & 2u);
-    const uint32_t lc = ((c0 >> cx) & 1u) | ((c0 >> (cx + 2)) & 2u);
-    const unsigned long long *t = table + (((ax * 4 + (int)lb) * 4 + (int)lc) << 2);
-    const uint32_t sh = pa & 63u; /* the move axis' low bits inside the word */
-    const uint32_t ha = pa >> 6, hb0 = b0 >> 6, hb2 = b2 >> 6, hc0 = c0 >> 6, hc2 = c2 >> 6;
-    Face4 f;
-    f.w[0] = ha | hb0 | hc0;
-    f.w[1] = ha | hb2 | hc0;
-    f.w[2] = ha | hb0 | hc2;
-    f.w[3] = ha | hb2 | hc2;
-    f.m[0] = t[0] << sh;
-    f.m[1] = t[1] << sh;
-    f.m[2] = t[2] << sh;
-    f.m[3] = t[3] << sh;
-    return f;
-}
-
-__device__ __forceinline__ bool face4_occupied(const unsigned long long *lat, const Face4 &f)
-{
-    unsigned long long o = lat[f.w[0]] & f.m[0];
-    if (f.m[1]) o |= lat[f.w[1]] & f.m[1];
-    if (f.m[2]) o |= lat[f.w[2]] & f.m[2];
-    if (f.m[3]) o |= lat[f.w[3]] & f.m[3];
-    return o != 0ull;
 }
 
 } // namespace bfm
