@@ -14,7 +14,10 @@
  */
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
+#include <iostream>
+#include <ostream>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -29,6 +32,23 @@ public:
     using T_Id = uint32_t;
 
     enum class Rng { IntHash = 1, Saru = 2, Philox = 3, Pcg = 4, Xorwow = 5 };
+
+    /* The reference's per-updater log switch (its SelectedLogger mLog,
+     * .h:225; the adapter's activateLogging calls mLog.activate(level),
+     * GPUScBFM_AB_Type.h:97-106).  Only "Stats" changes anything here: while
+     * it is active every runSimulationOnGPU counts the filters as the
+     * reference does and prints the analysis to std::cerr after the run, as
+     * the reference does (.cu:3348-3387). */
+    struct LogLevels {
+        std::vector<std::string> active;
+        void activate(std::string const &level)
+        {
+            if (!isActive(level)) active.push_back(level);
+        }
+        void deactivate(std::string const &level) { active.erase(std::remove(active.begin(), active.end(), level), active.end()); }
+        bool isActive(std::string const &level) const { return std::find(active.begin(), active.end(), level) != active.end(); }
+    };
+    LogLevels mLog;
 
     UpdaterGPUScBFM_AB_Type() { check(bfm_create(&mHandle)); }
     virtual ~UpdaterGPUScBFM_AB_Type() { destruct(); }
@@ -92,8 +112,46 @@ public:
     /* synchronous like the reference: positions are valid on return */
     void runSimulationOnGPU(uint32_t nrMCS_per_Call)
     {
+        const bool stats = mLog.isActive("Stats");
+        check(bfm_set_filter_stats(mHandle, stats ? 1 : mFilterMode));
         check(bfm_run(mHandle, nrMCS_per_Call));
         check(bfm_get_positions(mHandle, mPositions.data(), mPositions.size() / 3));
+        if (stats) printFilterAnalysis(std::cerr);
+    }
+
+    /* The reference prints its filter analysis when its "Stats" log level
+     * is active (.cu:2917-2936, :3348-3387).  Here: setFilterStats(1) for
+     * the reference's numbers (2: the moves made, 0: off), then
+     * printFilterAnalysis after a run writes them in the reference's format. */
+    void setFilterStats(int mode)
+    {
+        check(bfm_set_filter_stats(mHandle, mode));
+        mFilterMode = mode;
+    }
+    void printFilterAnalysis(std::ostream &os) const
+    {
+        static const char *const names[5] = {"Box Boundaries", "Invalid Bonds", "Volume Exclusion",
+                                             "! Invalid Bonds && Volume Exclusion",
+                                             "! Invalid Bonds && ! Volume Exclusion && Parallel Volume Exclusion"};
+        uint32_t k = 0;
+        check(bfm_get_nspecies(mHandle, &k));
+        std::vector<double> st(25 * (size_t)k);
+        check(bfm_get_filter_stats(mHandle, st.data(), st.size()));
+        os << "Filter analysis. Format:\n" << "Filter Reason: min | mean +- stddev | max\n";
+        for (uint32_t g = 0; g < k; ++g) {
+            size_t n = 0;
+            check(bfm_get_species_order(mHandle, g, nullptr, 0, &n));
+            const double pct = 100. / (double)n;
+            os << "\n=== Group " << char('A' + g) << " (" << n << ") ===\n";
+            for (int f = 0; f < 5; ++f) {
+                const double *v = &st[((size_t)g * 5 + f) * 5];
+                os << names[f] << ": " << v[0] << "(" << pct * v[0] << "%) | " << v[1] << "(" << pct * v[1]
+                   << "%) +- " << v[2] << " | " << v[3] << "(" << pct * v[3] << "%)\n";
+            }
+            const double *v1 = &st[((size_t)g * 5 + 1) * 5], *v3 = &st[((size_t)g * 5 + 3) * 5];
+            const double left = (double)n - (v1[1] * v1[4] + v3[1] * v3[4]) / v3[4];
+            os << "Remaining after 1st kernel: " << left << "(" << pct * left << "%)\n";
+        }
     }
 
     int32_t getMonomerPositionInX(T_Id i) { return mPositions.at(3 * (size_t)i); }
@@ -112,4 +170,5 @@ private:
     bfm_handle *mHandle = nullptr;
     std::vector<int32_t> mPositions;
     int64_t mSteps = 5000;
+    int mFilterMode = 0;
 };

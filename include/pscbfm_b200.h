@@ -111,6 +111,30 @@ int bfm_analyzer_chain_ids(bfm_handle *h, uint32_t *first, uint32_t *middle, uin
 /* per-chain R_e^2, R_g^2 and centre of mass (x, y, z per chain) of the last bfm_analyze */
 int bfm_analyze_per_chain(bfm_handle *h, double *re2, double *rg2, double *com, uint32_t n_chains);
 
+/* The reference's "Stats" filter analysis (runSimulationOnGPU with the
+ * "Stats" log active: .cu:2917-2936, :3141-3152, :3186-3197, :3316-3330,
+ * printed at :3348-3387).  While on, bfm_run runs the per-substep kernels
+ * (same trajectory) and counts, per colour substep,
+ *   [0] moves out of the box (non-periodic axes; the reference never fills it),
+ *   [1] invalid bonds, [2] occupied leading faces, [3] occupied leading
+ *   faces with valid bonds (kernelCountFilteredCheck, .cu:1033-1097),
+ *   [4] parallel refusals (kernelCountFilteredPerform, .cu:1192-1216).
+ * mode 1 reproduces the reference's printed numbers: filters 0-3 for
+ * IntHash directions whatever the RNG (.cu:1030-1032); filter 4 after the
+ * move (an accepted monomer is tested from its new corner), and with
+ * checkFront's byte fetch on the reference's bit-packed target lattice
+ * (UpdaterGPUScBFM_AB_Type.h:30, .cu:420-428, :1213): a face site s counts
+ * when any target bit of sites 8s .. 8s+7 is set and s < Lx*Ly*Lz/8.
+ * mode 2 counts the moves made: this RNG's directions, filter 4 = the
+ * candidates refused.  Mode 0 (default) is off.
+ * bfm_get_filter_stats: for the last run, per species s and filter f,
+ * out[(s * 5 + f) * 5 + 0..4] = min, mean, standard deviation (the
+ * reference's n/(n-1) form, .cu:3363-3366, NaN for one substep), max over
+ * the substeps of that species, and the number of those substeps (the
+ * reference's ns); n_out >= 25 * species; zeros where the species did not run. */
+int bfm_set_filter_stats(bfm_handle *h, int mode);
+int bfm_get_filter_stats(const bfm_handle *h, double *out, size_t n_out);
+
 /* cleanup (.h:487, .cu:3486-3502): frees the set-up; setters may be used again */
 int bfm_cleanup(bfm_handle *h);
 

@@ -19,6 +19,7 @@
  * Every function below cites the reference lines it restates.
  */
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -256,6 +257,10 @@ struct Sweep {
     uint64_t nAttempt = 0, nCandidate = 0, nAccept = 0;
     int nThreads = 1;
     bool periodic[3] = {true, true, true};
+    /* filter statistics of the reference's "Stats" mode (.cu:2917-2936):
+     * per species and filter, over the substeps of the latest run */
+    int filterStats = 0; /* 0 off, 1 counted as the reference's count kernels, 2 the moves made */
+    std::vector<double> fsum, fsum2, fmin, fmax, fcnt;
 
     /* the box test of the check kernel for non-periodic axes (.cu:988-996),
      * on the reference's unsigned device coordinates (a step below 0 wraps
@@ -299,11 +304,52 @@ struct Sweep {
         return false;
     }
 
+    /* checkFront of the reference's perform count (.cu:1213): the nine
+     * face sites' Z-order indices used as byte indices into the bit-packed
+     * temporary lattice of L^3/8 bytes -- byte b holds the target bits of
+     * sites 8b .. 8b+7 -- with fetches past its end reading zero (a linear
+     * texture of that size, .cu:2226-2240). */
+    bool front_bytes(int64_t x0, int64_t y0, int64_t z0, int dir) const
+    {
+        const int axis = dir >> 1;
+        const int s2 = (dir & 1) ? 2 : -2;
+        const uint64_t nbytes = (uint64_t)Lx * Ly * Lz / 8;
+        for (int a = -1; a <= 1; ++a)
+            for (int b = -1; b <= 1; ++b) {
+                int64_t x = x0, y = y0, zz = z0;
+                if (axis == 0) { x += s2; y += a; zz += b; }
+                else if (axis == 1) { y += s2; x += a; zz += b; }
+                else { zz += s2; x += a; y += b; }
+                const uint64_t byte = z(x, y, zz);
+                if (byte >= nbytes) continue;
+                for (int k = 0; k < 8; ++k)
+                    if (tmp[8 * byte + k]) return true;
+            }
+        return false;
+    }
+
     uint32_t draw(uint32_t seed, uint64_t iteration, uint32_t local) const
     {
         if (rng == RNG_INTHASH) return hash_rng(seed, local);
         if (rng == RNG_PHILOX) return philox4x32_10(seed, local, iteration);
         return saru_u32(seed, (uint32_t)iteration, local);
+    }
+
+    /* kernelCountFilteredCheck (.cu:1033-1097) for one monomer and
+     * direction: the move leaves the box ([0], which the reference never
+     * counts); inside the box, a bond becomes invalid ([1]) and,
+     * independently, the leading face is occupied ([2]). */
+    void filter_tests(uint32_t id, int dir, bool &out, bool &bad, bool &occ) const
+    {
+        const int64_t x1 = px[id] + DX[dir], y1 = py[id] + DY[dir], z1 = pz[id] + DZ[dir];
+        out = (!periodic[0] && !inside(px[id], x1, Lx)) || (!periodic[1] && !inside(py[id], y1, Ly)) ||
+              (!periodic[2] && !inside(pz[id], z1, Lz));
+        if (out) return;
+        for (uint32_t j = 0; j < nnbr[id] && !bad; ++j) {
+            const uint32_t nb = nbr[(size_t)id * 8 + j];
+            bad = forbidden[bond_index(px[nb] - x1, py[nb] - y1, pz[nb] - z1)] != 0;
+        }
+        occ = front(lattice, px[id], py[id], pz[id], dir);
     }
 
     /* one colour substep: kernelSimulationScBFMCheckSpecies (.cu:930-1028)
@@ -316,11 +362,26 @@ struct Sweep {
         flags.assign(m, 0);
         target.assign(m, 0);
         uint64_t nc = 0, na = 0;
-#pragma omp parallel for num_threads(nThreads) reduction(+ : nc) schedule(static)
+        /* filter counts, kernelCountFilteredCheck (.cu:1033-1097) and
+         * kernelCountFilteredPerform (.cu:1192-1216): [0] walls (counted
+         * here, never by the reference), [1] invalid bond, [2] occupied
+         * front, [3] occupied front with valid bonds, [4] parallel refusal */
+        uint64_t f0 = 0, f1 = 0, f2 = 0, f3 = 0, f4 = 0;
+#pragma omp parallel for num_threads(nThreads) reduction(+ : nc, f0, f1, f2, f3) schedule(static)
         for (long long i = 0; i < m; ++i) {
             const uint32_t id = ids[i];
             const uint32_t rn = draw(seed, iteration, (uint32_t)i);
             const int dir = (int)(rn % 6u);
+            if (filterStats) {
+                /* the reference's count kernel draws IntHash directions whatever the RNG */
+                const int dc = filterStats == 1 ? (int)(hash_rng(seed, (uint32_t)i) % 6u) : dir;
+                bool out = false, bad = false, occ = false;
+                filter_tests(id, dc, out, bad, occ);
+                f0 += out;
+                f1 += bad;
+                f2 += occ;
+                f3 += occ && !bad;
+            }
             const int64_t x1 = px[id] + DX[dir], y1 = py[id] + DY[dir], z1 = pz[id] + DZ[dir];
             if ((!periodic[0] && !inside(px[id], x1, Lx)) || (!periodic[1] && !inside(py[id], y1, Ly)) ||
                 (!periodic[2] && !inside(pz[id], z1, Lz)))
@@ -337,12 +398,23 @@ struct Sweep {
             __atomic_store_n(&tmp[target[i]], (uint8_t)1, __ATOMIC_RELAXED);
             ++nc;
         }
-#pragma omp parallel for num_threads(nThreads) reduction(+ : na) schedule(static)
+#pragma omp parallel for num_threads(nThreads) reduction(+ : na, f4) schedule(static)
         for (long long i = 0; i < m; ++i) {
             if (!(flags[i] & 8)) continue;
             const uint32_t id = ids[i];
             const int dir = flags[i] & 7;
-            if (front(tmp, px[id], py[id], pz[id], dir)) continue;
+            const bool refused = front(tmp, px[id], py[id], pz[id], dir);
+            if (filterStats == 1) {
+                /* kernelCountFilteredPerform runs after the perform-and-apply
+                 * kernel has moved the monomer (.cu:3163-3197) and reads the
+                 * bit-packed temporary lattice (UpdaterGPUScBFM_AB_Type.h:30)
+                 * with checkFront's byte fetch (.cu:420-428, :1213) */
+                if (refused) f4 += front_bytes(px[id], py[id], pz[id], dir);
+                else f4 += front_bytes(px[id] + DX[dir], py[id] + DY[dir], pz[id] + DZ[dir], dir);
+            } else {
+                f4 += refused;
+            }
+            if (refused) continue;
             lattice[z(px[id], py[id], pz[id])] = 0;
             px[id] += DX[dir];
             py[id] += DY[dir];
@@ -357,11 +429,30 @@ struct Sweep {
         nAttempt += (uint64_t)m;
         nCandidate += nc;
         nAccept += na;
+        if (filterStats) { /* .cu:3316-3330 */
+            const double x[5] = {(double)f0, (double)f1, (double)f2, (double)f3, (double)f4};
+            for (int f = 0; f < 5; ++f) {
+                const size_t at = (size_t)sp * 5 + f;
+                fsum[at] += x[f];
+                fsum2[at] += x[f] * x[f];
+                fmin[at] = std::min(fmin[at], x[f]);
+                fmax[at] = std::max(fmax[at], x[f]);
+                fcnt[at] += 1.0;
+            }
+        }
     }
 
     /* runSimulationOnGPU (.cu:2902-3400) */
     void run(uint32_t nMCS, R250State &r250)
     {
+        if (filterStats) { /* fresh per call (.cu:2926-2936) */
+            const size_t z = (size_t)nSpecies * 5;
+            fsum.assign(z, 0.0);
+            fsum2.assign(z, 0.0);
+            fmin.assign(z, (double)n);
+            fmax.assign(z, 0.0);
+            fcnt.assign(z, 0.0);
+        }
         for (uint32_t iStep = 0; iStep < nMCS; ++iStep, ++age) {
             if (age % sortEvery == 0) spatialSort();
             for (uint32_t iSub = 0; iSub < nSpecies; ++iSub) {
@@ -516,6 +607,28 @@ uint32_t orc_sweep_slab(void *h, uint32_t sp, uint32_t *out)
     auto *s = (Sweep *)h;
     if (out) std::memcpy(out, s->slab[sp].data(), sizeof(uint32_t) * s->slab[sp].size());
     return (uint32_t)s->slab[sp].size();
+}
+/* the reference's "Stats" filter analysis: on/off, and per species and
+ * filter the min, mean, stddev (.cu:3363-3366), max and number of substeps
+ * of the latest run */
+void orc_sweep_set_filter_stats(void *h, int mode) { ((Sweep *)h)->filterStats = mode; }
+void orc_sweep_filter_stats(void *h, double *out)
+{
+    auto *s = (Sweep *)h;
+    for (size_t i = 0; i < (size_t)s->nSpecies * 5; ++i) {
+        double *o = out + 5 * i;
+        const double n = i < s->fcnt.size() ? s->fcnt[i] : 0.0;
+        o[4] = n;
+        if (n == 0.0) {
+            o[0] = o[1] = o[2] = o[3] = 0.0;
+            continue;
+        }
+        const double mean = s->fsum[i] / n, sum2 = s->fsum2[i] / n;
+        o[0] = s->fmin[i];
+        o[1] = mean;
+        o[2] = std::sqrt(n / (n - 1.0) * (sum2 - mean * mean)); /* NaN when n == 1 */
+        o[3] = s->fmax[i];
+    }
 }
 void orc_sweep_stats(void *h, uint64_t *out3)
 {

@@ -68,6 +68,8 @@ def orc() -> ctypes.CDLL:
         L.orc_sweep_slab.restype = _c.c_uint32
         L.orc_sweep_slab.argtypes = [_P, _c.c_uint32, _P]
         L.orc_sweep_stats.argtypes = [_P, _P]
+        L.orc_sweep_set_filter_stats.argtypes = [_P, _c.c_int]
+        L.orc_sweep_filter_stats.argtypes = [_P, _P]
         L.orc_serial_run.restype = _c.c_uint64
         L.orc_serial_run.argtypes = [_c.c_uint32] * 4 + [_P, _P, _P, _P, _c.c_uint64, _c.c_uint64]
         _orc = L
@@ -151,6 +153,16 @@ class Sweep:
         orc().orc_sweep_stats(self._h, out.ctypes.data)
         return tuple(int(v) for v in out)
 
+    def set_filter_stats(self, mode: int):
+        """0 off; 1 counted as the reference's count kernels do; 2 the moves made"""
+        orc().orc_sweep_set_filter_stats(self._h, int(mode))
+
+    def filter_stats(self) -> np.ndarray:
+        """(species, 5 filters, [min, mean, stddev, max, substeps]) of the latest run"""
+        out = np.zeros((self.nspecies(), 5, 5), np.float64)
+        orc().orc_sweep_filter_stats(self._h, out.ctypes.data)
+        return out
+
     def __del__(self):
         if getattr(self, "_h", None):
             orc().orc_sweep_destroy(self._h)
@@ -221,6 +233,8 @@ def ref_gpu():
         L.ref_run.restype = _c.c_int
         L.ref_run.argtypes = [_P, _c.c_uint32]
         L.ref_get.argtypes = [_P, _P, _c.c_uint32]
+        L.ref_run_stats.restype = _c.c_long
+        L.ref_run_stats.argtypes = [_P, _c.c_uint32, _P, _c.c_size_t]
         L.ref_age.restype = _c.c_int64
         L.ref_age.argtypes = [_P]
         L.ref_destroy.argtypes = [_P]
@@ -261,10 +275,39 @@ class RefUpdater:
         ref_gpu().ref_get(self._h, out.ctypes.data, self.n)
         return out
 
+    def run_stats(self, nmcs: int, r250: np.ndarray) -> str:
+        """run with the reference's "Stats" log active; returns what it printed"""
+        L = ref_gpu()
+        L.ref_r250_set(r250.ctypes.data)
+        buf = ctypes.create_string_buffer(1 << 16)
+        if L.ref_run_stats(self._h, int(nmcs), buf, len(buf)) < 0:
+            raise RuntimeError("reference run failed: " + (L.ref_last_error() or b"").decode())
+        L.ref_r250_get(r250.ctypes.data)
+        return buf.value.decode()
+
     def __del__(self):
         if getattr(self, "_h", None):
             ref_gpu().ref_destroy(self._h)
             self._h = None
+
+
+def parse_filter_analysis(text: str):
+    """The reference's printed filter analysis (.cu:3351-3374, one block
+    "=== Group X (n) ===" per species, then per filter
+    "name: min(p%) | mean(p%) +- stddev | max(p%)") as
+    (group sizes, array (groups, 5, 4) of min, mean, stddev, max)."""
+    sizes, rows = [], []
+    for line in text.splitlines():
+        if line.startswith("=== Group "):
+            sizes.append(int(line.split("(")[1].split(")")[0]))
+            rows.append([])
+        elif rows and len(rows[-1]) < 5 and ": " in line and " | " in line and " +- " in line:
+            vals = line.split(": ", 1)[1]
+            lo, mid, hi = vals.split(" | ")
+            mean, std = mid.split(" +- ")
+            num = lambda t: float(t.split("(")[0])
+            rows[-1].append([num(lo), num(mean), float(std), num(hi)])
+    return sizes, np.array(rows, dtype=np.float64).reshape(len(rows), 5, 4)
 
 
 # ---------------------------------------------------------------- chain analysis

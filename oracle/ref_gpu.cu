@@ -12,6 +12,8 @@
 #include <cstdint>
 #include <cstring>
 #include <exception>
+#include <iostream>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -113,6 +115,29 @@ int ref_run(void *h, uint32_t nmcs)
         g_err = e.what();
         return 1;
     }
+}
+
+/* runSimulationOnGPU with the reference's "Stats" log level active for its
+ * updater (the constructor switches it off, .cu:1416-1423): the filter
+ * analysis it prints to std::cerr (.cu:3348-3387) is returned as text, at
+ * most cap - 1 bytes and NUL-terminated.  Returns the length of the full
+ * text, or -1 when the run failed. */
+long ref_run_stats(void *h, uint32_t nmcs, char *text, size_t cap)
+{
+    auto &logger = SelectiveLogger::getInstance();
+    logger.activate("UpdaterGPUScBFM_AB_Type.cu", "Stats");
+    std::ostringstream out;
+    std::streambuf *saved = std::cerr.rdbuf(out.rdbuf());
+    const int rc = ref_run(h, nmcs);
+    std::cerr.rdbuf(saved);
+    logger.deactivate("UpdaterGPUScBFM_AB_Type.cu", "Stats");
+    const std::string s = out.str();
+    if (text && cap) {
+        const size_t m = s.size() < cap - 1 ? s.size() : cap - 1;
+        std::memcpy(text, s.data(), m);
+        text[m] = 0;
+    }
+    return rc == 0 ? (long)s.size() : -1;
 }
 
 void ref_get(void *h, int32_t *pos3, uint32_t n) { ((RefBase *)h)->get(pos3, n); }

@@ -101,6 +101,8 @@ _SIGS = {
     "bfm_analyze": (_c.c_int, [_P, _c.c_int, _P, _c.c_size_t]),
     "bfm_analyzer_chain_ids": (_c.c_int, [_P, _P, _P, _P, _c.c_uint32]),
     "bfm_analyze_per_chain": (_c.c_int, [_P, _P, _P, _P, _c.c_uint32]),
+    "bfm_set_filter_stats": (_c.c_int, [_P, _c.c_int]),
+    "bfm_get_filter_stats": (_c.c_int, [_P, _P, _c.c_size_t]),
     "bfm_cleanup": (_c.c_int, [_P]),
     "bfm_get_lattice": (_c.c_int, [_P, _P, _c.c_size_t]),
     "bfm_get_lattice_words": (_c.c_int, [_P, _c.POINTER(_c.c_size_t)]),

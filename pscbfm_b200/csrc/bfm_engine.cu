@@ -26,6 +26,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -82,6 +83,9 @@ struct Sys {
     uint32_t *tmp;
     const Species *spec;
     unsigned long long *counters;
+    unsigned long long *fstats; /* filter statistics per substep of a chunk (kFilters each), or null */
+    int fmode;                  /* 1: counted as the reference's count kernels do; 2: the moves made */
+    uint32_t fbytes;            /* Lx*Ly*Lz/8: bytes of the reference's bit-packed target lattice */
     uint32_t npad;
     uint32_t latWords;
     Geometry g;
@@ -98,6 +102,20 @@ __host__ __device__ __forceinline__ size_t bc_index(uint32_t j, uint32_t slot, u
 __device__ __forceinline__ uint32_t *bc_pair(uint16_t *bcode) { return reinterpret_cast<uint32_t *>(bcode); }
 __device__ __forceinline__ const uint32_t *bc_pair(const uint16_t *bcode) { return reinterpret_cast<const uint32_t *>(bcode); }
 
+/* Filter statistics of the reference's "Stats" mode
+ * (UpdaterGPUScBFM_AB_Type.cu:1033-1097, :1192-1216, :2917-2936): moves of a
+ * substep refused by the box walls, by an invalid bond, by an occupied
+ * leading face (whatever the bonds), by an occupied face with valid bonds,
+ * and candidates refused in the perform phase. */
+constexpr int kFilters = 5;
+
+/* warp-aggregated count of a predicate into a 64-bit counter */
+__device__ __forceinline__ void count_warp(unsigned long long *c, bool pred)
+{
+    const unsigned int m = __ballot_sync(0xFFFFFFFFu, pred);
+    if (m && (threadIdx.x & 31u) == 0) atomicAdd(c, (unsigned long long)__popc(m));
+}
+
 /* ------------------------------------------------------------- kernels */
 
 __device__ __forceinline__ bool face_occupied(const uint32_t *__restrict__ lat, uint32_t r0, int dir, const Geometry &g)
@@ -112,6 +130,22 @@ __device__ __forceinline__ bool face_occupied(const uint32_t *__restrict__ lat, 
             any |= __ldg(lat + (s >> 5)) >> (s & 31u);
         }
     return any & 1u;
+}
+
+/* The tests of the reference's kernelCountFilteredCheck (.cu:1033-1097) for
+ * one monomer and direction: the move leaves the box; else a bond becomes
+ * invalid, and (independently) the leading face is occupied. */
+__device__ __forceinline__ void filter_tests(const Sys &s, const uint32_t *forbid, uint32_t slot, uint32_t r0, int dir,
+                                             bool &outside, bool &badBond, bool &front)
+{
+    outside = leaves_box(r0, dir, s.g);
+    if (outside) return;
+    const uint32_t r1 = zstep(r0, dir, s.g);
+    for (uint32_t j = 0; j < s.deg[slot] && !badBond; ++j) {
+        const uint32_t code = zbond(s.pos[s.nbr[(size_t)j * s.npad + slot]], r1);
+        badBond = (forbid[code >> 5] >> (code & 31u)) & 1u;
+    }
+    front = face_occupied(s.lat, r0, dir, s.g);
 }
 
 /* Check phase of one colour substep, plus zeroing of the other temporary
@@ -138,6 +172,7 @@ __global__ void __launch_bounds__(kThreads) k_check(Sys s, const Substep *__rest
     for (uint32_t base = blockIdx.x * blockDim.x; base < sp.n; base += stride) {
         const uint32_t i = base + threadIdx.x;
         int cand = 0;
+        bool outside = false, badBond = false, front = false;
         if (i < sp.n) {
             const uint32_t slot = sp.off + i;
             const uint32_t r0 = s.pos[slot];
@@ -145,14 +180,15 @@ __global__ void __launch_bounds__(kThreads) k_check(Sys s, const Substep *__rest
             const uint32_t r1 = zstep(r0, dir, s.g);
             const uint32_t nb = s.deg[slot];
             bool ok = !leaves_box(r0, dir, s.g);
-            for (uint32_t j = 0; j < nb; ++j) {
-                const uint32_t q = s.pos[s.nbr[(size_t)j * s.npad + slot]];
-                const uint32_t code = zbond(q, r1);
-                if ((forbid[code >> 5] >> (code & 31u)) & 1u) {
-                    ok = false;
-                    break;
+            if (ok)
+                for (uint32_t j = 0; j < nb; ++j) {
+                    const uint32_t q = s.pos[s.nbr[(size_t)j * s.npad + slot]];
+                    const uint32_t code = zbond(q, r1);
+                    if ((forbid[code >> 5] >> (code & 31u)) & 1u) {
+                        ok = false;
+                        break;
+                    }
                 }
-            }
             if (ok) ok = !face_occupied(s.lat, r0, dir, s.g);
             uint8_t f = 0;
             if (ok) {
@@ -161,10 +197,42 @@ __global__ void __launch_bounds__(kThreads) k_check(Sys s, const Substep *__rest
                 cand = 1;
             }
             s.flags[slot] = f;
+            if (s.fstats) {
+                /* the reference's count kernel draws IntHash directions whatever the RNG */
+                const int dc = s.fmode == 1 ? direction(draw<RNG_INTHASH>(d.seed, d.iter, i)) : dir;
+                filter_tests(s, forbid, slot, r0, dc, outside, badBond, front);
+            }
+        }
+        if (s.fstats) {
+            unsigned long long *c = s.fstats + (size_t)k * kFilters;
+            count_warp(c + 0, outside);
+            count_warp(c + 1, badBond);
+            count_warp(c + 2, front);
+            count_warp(c + 3, front && !badBond);
         }
         nCand += __syncthreads_count(cand);
     }
     if (threadIdx.x == 0 && nCand && s.counters) atomicAdd(s.counters + 0, (unsigned long long)nCand);
+}
+
+/* The reference's perform count (kernelCountFilteredPerform, .cu:1192-1216)
+ * calls checkFront with its byte fetch (.cu:420-428) on the bit-packed
+ * target lattice (UpdaterGPUScBFM_AB_Type.h:30): each of the nine face
+ * sites' Z-order index is read as a byte index -- byte b holds the target
+ * bits of sites 8b .. 8b+7 -- and indices past the lattice's Lx*Ly*Lz/8
+ * bytes read zero (a linear texture of that size, .cu:2226-2240). */
+__device__ __noinline__ bool front_bytes(const uint32_t *tmp, uint32_t r, int dir, const Geometry &g, uint32_t nbytes)
+{
+    const int ax = dir >> 1, a1 = ax == 0 ? 1 : 0, a2 = ax == 2 ? 1 : 2;
+    const uint32_t c = zstep(zstep(r, dir, g), dir, g);
+    for (int u = -1; u <= 1; ++u) {
+        const uint32_t cu = u == 0 ? c : zstep(c, 2 * a1 + (u > 0), g);
+        for (int v = -1; v <= 1; ++v) {
+            const uint32_t b = v == 0 ? cu : zstep(cu, 2 * a2 + (v > 0), g);
+            if (b < nbytes && ((tmp[b >> 2] >> (8u * (b & 3u))) & 0xFFu)) return true;
+        }
+    }
+    return false;
 }
 
 /* Perform phase: a candidate moves unless another candidate's target lies
@@ -179,13 +247,20 @@ __global__ void __launch_bounds__(kThreads) k_perform(Sys s, const Substep *__re
     for (uint32_t base = blockIdx.x * blockDim.x; base < sp.n; base += stride) {
         const uint32_t i = base + threadIdx.x;
         int acc = 0;
+        bool counted = false; /* filter [4] of the statistics */
         if (i < sp.n) {
             const uint32_t slot = sp.off + i;
             const uint8_t f = s.flags[slot];
             if (f & 8) {
                 const uint32_t r0 = s.pos[slot];
                 const int dir = f & 7;
-                if (!face_occupied(tmp, r0, dir, s.g)) {
+                const bool refused = face_occupied(tmp, r0, dir, s.g);
+                counted = refused;
+                /* the reference counts after its perform-and-apply kernel has
+                 * moved the monomer (.cu:3163-3197), with its byte fetch */
+                if (s.fstats && s.fmode == 1)
+                    counted = front_bytes(tmp, refused ? r0 : zstep(r0, dir, s.g), dir, s.g, s.fbytes);
+                if (!refused) {
                     const uint32_t r1 = zstep(r0, dir, s.g);
                     const uint32_t w0 = r0 >> 5, w1 = r1 >> 5;
                     const uint32_t b0 = 1u << (r0 & 31u), b1 = 1u << (r1 & 31u);
@@ -203,6 +278,7 @@ __global__ void __launch_bounds__(kThreads) k_perform(Sys s, const Substep *__re
                 }
             }
         }
+        if (s.fstats) count_warp(s.fstats + (size_t)k * kFilters + 4, counted);
         nAcc += __syncthreads_count(acc);
     }
     if (threadIdx.x == 0 && nAcc && s.counters) atomicAdd(s.counters + 1, (unsigned long long)nAcc);
@@ -1082,6 +1158,7 @@ struct Engine {
     int64_t sortEvery = 5000;
     int launchMode = 0;
     int coloringMode = 0; /* 0 host walk (the reference's); 1 device for forests, host otherwise */
+    int filterStats = 0; /* the reference's "Stats" filter analysis: 0 off, 1 counted as the reference, 2 the moves made */
 
     /* ---- derived at initialize */
     bool colorOnDevice = false;
@@ -1160,7 +1237,8 @@ struct Engine {
         dfree(d_pos); dfree(d_pos2); dfree(d_img); dfree(d_img2); dfree(d_nbr); dfree(d_nbr2);
         dfree(d_deg); dfree(d_deg2); dfree(d_rev); dfree(d_rev2); dfree(d_bcode); dfree(d_s2o); dfree(d_s2o2); dfree(d_o2s); dfree(d_flags);
         dfree(d_lat); dfree(d_tmp); dfree(d_spec); dfree(d_counters); dfree(d_perm); dfree(d_inv);
-        dfree(d_iota); dfree(d_keys); dfree(d_out); dfree(d_bar); dfree(d_glist);
+        dfree(d_iota); dfree(d_keys); dfree(d_out); dfree(d_bar); dfree(d_glist); dfree(d_fstats);
+        fcnt.clear();
         releaseAnalyzer();
         if (d_cub) cudaFree(d_cub);
         d_cub = nullptr;
@@ -1200,6 +1278,9 @@ struct Engine {
         s.tmp = d_tmp;
         s.spec = d_spec;
         s.counters = d_counters;
+        s.fstats = filterStats ? d_fstats : nullptr;
+        s.fmode = filterStats;
+        s.fbytes = (uint32_t)(L[0] * L[1] * L[2] / 8);
         s.npad = npad;
         s.latWords = (uint32_t)latWords;
         s.g = g;
@@ -1724,13 +1805,19 @@ struct Engine {
                 }
             graphRng = rng;
         }
+        /* the filter analysis runs the per-substep kernels, which count */
+        const int mode = filterStats ? 2 : launchMode;
+        if (filterStats) {
+            if (!d_fstats) dalloc(d_fstats, (size_t)kChunk * kFilters);
+            resetFilterStats();
+        }
         R250 &r250 = global_r250();
         std::lock_guard<std::mutex> lock(g_r250_mutex);
         CK(cudaEventRecord(ev0, stream));
         uint64_t launches = 0;
         uint32_t iStep = 0;
         int b = 0;
-        const uint32_t cap = launchMode == 1 ? graphSubsteps() : (kChunk / nSpecies) * nSpecies;
+        const uint32_t cap = mode == 1 ? graphSubsteps() : (kChunk / nSpecies) * nSpecies;
         while (iStep < nMCS) {
             /* one schedule chunk: whole MCS only, ending before a re-sort */
             CK(cudaEventSynchronize(schedFree[b]));
@@ -1759,12 +1846,13 @@ struct Engine {
             if (sortFirst && !sortedFresh) spatialSort();
             CK(cudaMemcpyAsync(d_sched[b], hs, m * sizeof(Substep), cudaMemcpyHostToDevice, stream));
             CK(cudaEventRecord(schedFree[b], stream));
-            if (launchMode == 0) {
+            if (filterStats) CK(cudaMemsetAsync(d_fstats, 0, (size_t)m * kFilters * sizeof(unsigned long long), stream));
+            if (mode == 0) {
                 profMark();
                 launchSweep(d_sched[b], 0, m);
                 profMark();
                 launches += 1;
-            } else if (launchMode == 1 && m == cap) {
+            } else if (mode == 1 && m == cap) {
                 if (!graph[b]) buildGraph(b);
                 CK(cudaGraphLaunch(graph[b], stream));
                 launches += 2 * (uint64_t)m;
@@ -1773,18 +1861,19 @@ struct Engine {
                 launches += 2 * (uint64_t)m;
             }
             CK(cudaGetLastError());
+            if (filterStats) accumulateFilterStats(hs, m);
             sortedFresh = false;
             b ^= 1;
         }
         age += nMCS;
         /* the split kernels leave the target buffer of their last substep
          * set; the persistent kernel clears its own before it returns */
-        if (launchMode != 0) {
+        if (mode != 0) {
             CK(cudaMemsetAsync(d_tmp, 0, 2 * latWords * sizeof(uint32_t), stream));
             refreshBondCodes();
         }
         CK(cudaEventRecord(ev1, stream));
-        if (launchMode == 0) CK(cudaMemcpyAsync(h_flag, &d_bar->err, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream));
+        if (mode == 0) CK(cudaMemcpyAsync(h_flag, &d_bar->err, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream));
         CK(cudaEventSynchronize(ev1));
         CK(cudaStreamSynchronize(stream));
         float ms = 0;
@@ -1792,11 +1881,43 @@ struct Engine {
         lastRunMs = ms;
         lastLaunches = launches;
         CK(cudaGetLastError());
-        if (launchMode == 0 && *h_flag) {
+        if (mode == 0 && *h_flag) {
             CK(cudaMemsetAsync(d_bar, 0, sizeof(GridBarrier), stream));
             CK(cudaStreamSynchronize(stream));
             throw DeviceTimeout("a grid barrier of the persistent sweep kernel timed out; the positions of this run are not valid");
         }
+    }
+
+    /* ------------------------------------------ filter statistics */
+    unsigned long long *d_fstats = nullptr;
+    std::vector<double> fsum, fsum2, fmin, fmax, fcnt; /* [species][filter], per run as .cu:2926-2936 */
+
+    void resetFilterStats()
+    {
+        const size_t z = (size_t)nSpecies * kFilters;
+        fsum.assign(z, 0.0);
+        fsum2.assign(z, 0.0);
+        fmin.assign(z, (double)n);
+        fmax.assign(z, 0.0);
+        fcnt.assign(z, 0.0);
+    }
+
+    /* counts of one chunk of m substeps into the per-species statistics (.cu:3316-3330) */
+    void accumulateFilterStats(const Substep *hs, uint32_t m)
+    {
+        std::vector<unsigned long long> c((size_t)m * kFilters);
+        CK(cudaMemcpyAsync(c.data(), d_fstats, c.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        for (uint32_t k = 0; k < m; ++k)
+            for (int f = 0; f < kFilters; ++f) {
+                const size_t at = (size_t)hs[k].species * kFilters + f;
+                const double x = (double)c[(size_t)k * kFilters + f];
+                fsum[at] += x;
+                fsum2[at] += x * x;
+                fmin[at] = std::min(fmin[at], x);
+                fmax[at] = std::max(fmax[at], x);
+                fcnt[at] += 1.0;
+            }
     }
 
     /* ------------------------------------------------ chain analysis */
@@ -2248,6 +2369,38 @@ int bfm_analyze_per_chain(bfm_handle *h, double *re2, double *rg2, double *com, 
         if (com) CK(cudaMemcpyAsync(com, e.d_ccom, 3 * (size_t)n_chains * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
         CK(cudaStreamSynchronize(e.stream));
     });
+}
+
+int bfm_set_filter_stats(bfm_handle *h, int mode)
+{
+    GUARD(h, {
+        if (mode < 0 || mode > 2) throw std::invalid_argument("filter statistics mode must be 0, 1 or 2");
+        h->e.filterStats = mode;
+    });
+}
+
+int bfm_get_filter_stats(const bfm_handle *h, double *out, size_t n_out)
+{
+    if (!h || !out) return BFM_EINVAL;
+    if (!h->e.initialized) return BFM_ENOTINIT;
+    const auto &e = h->e;
+    const size_t z = (size_t)e.nSpecies * kFilters;
+    if (n_out < 5 * z) return BFM_EINVAL;
+    for (size_t i = 0; i < z; ++i) {
+        const double n = i < e.fcnt.size() ? e.fcnt[i] : 0.0;
+        double *o = out + 5 * i;
+        o[4] = n;
+        if (n == 0.0) {
+            o[0] = o[1] = o[2] = o[3] = 0.0;
+            continue;
+        }
+        const double mean = e.fsum[i] / n, sum2 = e.fsum2[i] / n;
+        o[0] = e.fmin[i];
+        o[1] = mean;
+        o[2] = std::sqrt(n / (n - 1.0) * (sum2 - mean * mean)); /* .cu:3363-3366; NaN when n == 1 */
+        o[3] = e.fmax[i];
+    }
+    return BFM_OK;
 }
 
 int bfm_cleanup(bfm_handle *h)

@@ -194,6 +194,27 @@ class UpdaterGPUScBFM_AB_Type:
         self._check(self._lib.bfm_get_coloring(self._h, ctypes.byref(m), ctypes.byref(d)))
         return m.value, bool(d.value)
 
+    # ---- the reference's "Stats" filter analysis
+    FILTERS = ("Box Boundaries", "Invalid Bonds", "Volume Exclusion", "! Invalid Bonds && Volume Exclusion",
+               "! Invalid Bonds && ! Volume Exclusion && Parallel Volume Exclusion")
+
+    def setFilterStats(self, mode: int = 1):
+        """count, in the following runs, the moves each filter refuses per
+        colour substep (the per-substep kernels run while this is on).
+        mode 1: the reference's printed numbers (IntHash directions for
+        filters 0-3; filter 4 after the move, read through the reference's
+        byte fetch of its bit-packed target lattice); 2: the moves this RNG
+        made, filter 4 = candidates refused; 0: off."""
+        self._check(self._lib.bfm_set_filter_stats(self._h, int(mode)))
+        return self
+
+    def getFilterStats(self) -> np.ndarray:
+        """(species, 5 filters, [min, mean, stddev, max, substeps]) over the
+        colour substeps of the last run; filter names in FILTERS"""
+        out = np.zeros((self.getNSpecies(), 5, 5), dtype=np.float64)
+        self._check(self._lib.bfm_get_filter_stats(self._h, out.ctypes.data, out.size))
+        return out
+
     # ---- chain analysis on the device (the reference's AnalyzerMsd)
     def analyzerInit(self) -> int:
         """Find the linear chains (first end, middle, last end) by the

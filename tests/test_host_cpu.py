@@ -140,7 +140,10 @@ int main() {
     u.setLatticeSize(32, 32, 32);
     u.setNrOfAllMonomers(2);
     try { u.setNrOfAllMonomers(2); } catch (std::runtime_error const &) { std::puts("ok"); }
-    return 0;
+    u.mLog.activate("Stats");
+    u.setFilterStats(2);
+    try { u.printFilterAnalysis(std::cerr); } catch (std::runtime_error const &) { std::puts("stats before init"); }
+    return u.mLog.isActive("Stats") ? 0 : 1;
 }
 ''')
     exe = tmp_path / "use"
@@ -148,4 +151,4 @@ int main() {
                     "-L", os.path.dirname(_native.LIBPATH), "-lpscbfm_b200",
                     "-Wl,-rpath," + os.path.dirname(_native.LIBPATH)], check=True)
     out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
-    assert "ok" in out
+    assert "ok" in out and "stats before init" in out
