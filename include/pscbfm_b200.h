@@ -135,6 +135,45 @@ int bfm_analyze_per_chain(bfm_handle *h, double *re2, double *rg2, double *com, 
 int bfm_set_filter_stats(bfm_handle *h, int mode);
 int bfm_get_filter_stats(const bfm_handle *h, double *out, size_t n_out);
 
+/* ---- batched ensembles: many independent systems in one persistent launch.
+ * No counterpart class in the reference; each system follows exactly the
+ * trajectory of a single updater (this library's bfm_* handle, and so the
+ * reference's runSimulationOnGPU, .cu:2902-3400) started from the same
+ * positions, bonds, bond set, RNG, age, sorting interval and R250 state:
+ * the colour and seed of every substep come from the system's own R250
+ * stream, drawn on the device.  Box edges may be any multiple of 8 in
+ * 8 .. 1024 (the reference needs powers of two); boxes are periodic; at
+ * most 16 colours per system. */
+typedef struct bfm_batch bfm_batch;
+int bfm_batch_create(int gpu, bfm_batch **out);
+int bfm_batch_destroy(bfm_batch *b);
+const char *bfm_batch_last_error(const bfm_batch *b);
+/* Adds one system (before bfm_batch_initialize).  pos3: n x (x, y, z)
+ * unfolded corners; deg: bonds per monomer; nbr8: 8 partner ids per monomer;
+ * allowed512: 1 for an allowed bond, index (dx&7)|(dy&7)<<3|(dz&7)<<6
+ * (108 allowed, as initializeBondTable requires, .cu:1516-1559); rng as
+ * BFM_RNG_*; r250_state251: 250 R250 words and the index (as
+ * bfm_r250_get_state gives), or NULL to seed it from r250_seed as
+ * bfm_r250_seed does.  *sys receives the system's index. */
+int bfm_batch_add_system(bfm_batch *b, uint32_t Lx, uint32_t Ly, uint32_t Lz, uint32_t n, const int32_t *pos3, const uint8_t *deg,
+                         const uint32_t *nbr8, const uint8_t *allowed512, int rng, int64_t age, int64_t sort_every,
+                         const uint32_t *r250_state251, uint64_t r250_seed, uint32_t *sys);
+/* colours, slabs, lattices and device state of every system (initialize,
+ * .cu:2393-2537, per system) */
+int bfm_batch_initialize(bfm_batch *b);
+/* system s advances by mcs[s] Monte-Carlo steps (0 leaves it as it is); nsys
+ * must equal the number of systems */
+int bfm_batch_run(bfm_batch *b, const uint32_t *mcs, size_t nsys);
+/* unfolded positions of system sys, original monomer order (doCopyBack, .cu:3402-3484) */
+int bfm_batch_get_positions(bfm_batch *b, uint32_t sys, int32_t *pos3, size_t n);
+/* age, R250 state (251 words) and counters (attempts, candidates, accepts) of system sys; any pointer may be NULL */
+int bfm_batch_get_state(bfm_batch *b, uint32_t sys, int64_t *age, uint32_t *r250_state251, uint64_t *counters3);
+/* occupation bits of system sys (Z-order of the box padded to powers of two); *needed receives the word count */
+int bfm_batch_get_lattice(bfm_batch *b, uint32_t sys, uint32_t *words, size_t nwords, size_t *needed);
+/* systems, monomers, largest colour count; time, launches and attempted moves of the last bfm_batch_run */
+int bfm_batch_info(const bfm_batch *b, uint32_t *nsys, uint64_t *monomers, uint32_t *nspecies_max, double *last_ms,
+                   uint64_t *last_launches, uint64_t *last_attempts);
+
 /* cleanup (.h:487, .cu:3486-3502): frees the set-up; setters may be used again */
 int bfm_cleanup(bfm_handle *h);
 

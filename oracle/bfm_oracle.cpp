@@ -271,7 +271,20 @@ struct Sweep {
         return (0 < c0 && c1 < L - 1) || (c0 == 0 && c1 <= 1) || (c0 == L - 1 && c1 > 1);
     }
 
-    uint32_t z(int64_t x, int64_t y, int64_t zz) const { return zindex(x, y, zz, mx, my, mz); }
+    /* lattice index: Z-order of the wrapped coordinates in the box padded to
+     * powers of two (masking is the wrap when the edges are powers of two,
+     * as in the reference; edges that are only multiples of 8 wrap mod L) */
+    bool pow2 = true;
+    static int64_t wrap(int64_t v, int64_t L)
+    {
+        const int64_t r = v % L;
+        return r < 0 ? r + L : r;
+    }
+    uint32_t z(int64_t x, int64_t y, int64_t zz) const
+    {
+        if (pow2) return zindex(x, y, zz, mx, my, mz);
+        return zindex(wrap(x, Lx), wrap(y, Ly), wrap(zz, Lz), mx, my, mz);
+    }
 
     /* doSpatialSorting (.cu:1835-1943): per species, order by the Z-curve
      * index of the wrapped position.  The keys are unique (excluded volume),
@@ -534,11 +547,20 @@ void *orc_sweep_create(uint32_t Lx, uint32_t Ly, uint32_t Lz, uint32_t n, const 
                        int nThreads)
 {
     try {
-        for (uint32_t L : {Lx, Ly, Lz})
-            if (L < 8 || L > 1024 || (L & (L - 1))) return nullptr; /* power-of-two boxes only */
+        /* the reference takes power-of-two boxes; the batched ensembles also
+         * take edges that are multiples of 8 */
+        uint32_t P[3] = {1, 1, 1};
+        bool pow2 = true;
+        for (int a = 0; a < 3; ++a) {
+            const uint32_t L = a == 0 ? Lx : (a == 1 ? Ly : Lz);
+            if (L < 8 || L > 1024 || (L % 8)) return nullptr;
+            while (P[a] < L) P[a] <<= 1;
+            pow2 = pow2 && P[a] == L;
+        }
         auto *s = new Sweep();
         s->Lx = Lx; s->Ly = Ly; s->Lz = Lz;
-        s->mx = Lx - 1; s->my = Ly - 1; s->mz = Lz - 1;
+        s->mx = P[0] - 1; s->my = P[1] - 1; s->mz = P[2] - 1;
+        s->pow2 = pow2;
         s->n = n;
         s->nnbr.assign(nnbr, nnbr + n);
         s->nbr.assign(nbr8, nbr8 + (size_t)n * 8);
@@ -559,7 +581,7 @@ void *orc_sweep_create(uint32_t Lx, uint32_t Ly, uint32_t Lz, uint32_t n, const 
         s->nSpecies = k;
         s->slab.assign(k, {});
         for (uint32_t i = 0; i < n; ++i) s->slab[s->color[i]].push_back(i); /* .cu:1648-1650 */
-        const uint32_t Lm = std::max(Lx, std::max(Ly, Lz));
+        const uint32_t Lm = std::max(P[0], std::max(P[1], P[2]));
         const size_t sites = (size_t)Lm * Lm * Lm;
         s->lattice.assign(sites, 0);
         s->tmp.assign(sites, 0);

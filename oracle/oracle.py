@@ -180,9 +180,12 @@ def serial_run(system, pos: np.ndarray, nmcs: int, seed: int) -> int:
 
 
 def lattice_words(pos: np.ndarray, box) -> np.ndarray:
-    """Occupation bit lattice (Z-order, 32-bit words) of corner positions."""
+    """Occupation bit lattice (Z-order, 32-bit words) of corner positions;
+    edges that are not powers of two are padded to the next one."""
     from pscbfm_b200.systems import System  # noqa: F401  (keeps import graph explicit)
-    Lm = max(box)
+    Lm = 1
+    while Lm < max(box):
+        Lm *= 2
     words = np.zeros(Lm ** 3 // 32, np.uint32)
     p = np.asarray(pos, dtype=np.int64) % np.array(box)
     code = _zcode(p[:, 0]) | (_zcode(p[:, 1]) << 1) | (_zcode(p[:, 2]) << 2)

@@ -20,3 +20,4 @@ from .updater import (  # noqa: F401
     r250_seed_words,
     r250_set_state,
 )
+from .batch import Batch, BatchError  # noqa: F401,E402

@@ -18,7 +18,7 @@ LIBNAME = "libpscbfm_b200.so"
 LIBPATH = os.path.join(HERE, LIBNAME)
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["bfm_engine.cu", "bfm_diag.cu", "bfm_color.cu"]
+SOURCES = ["bfm_engine.cu", "bfm_diag.cu", "bfm_color.cu", "bfm_batch.cu"]
 HEADERS = ["bfm_device.cuh", "bfm_host.hpp", "bfm_sweep.cuh", "bfm_analyze.cuh", "bfm_color.hpp", "../../include/pscbfm_b200.h"]
 
 NVCC_FLAGS = [
@@ -104,6 +104,17 @@ _SIGS = {
     "bfm_set_filter_stats": (_c.c_int, [_P, _c.c_int]),
     "bfm_get_filter_stats": (_c.c_int, [_P, _P, _c.c_size_t]),
     "bfm_cleanup": (_c.c_int, [_P]),
+    "bfm_batch_create": (_c.c_int, [_c.c_int, _c.POINTER(_P)]),
+    "bfm_batch_destroy": (_c.c_int, [_P]),
+    "bfm_batch_last_error": (_c.c_char_p, [_P]),
+    "bfm_batch_add_system": (_c.c_int, [_P, _c.c_uint32, _c.c_uint32, _c.c_uint32, _c.c_uint32, _P, _P, _P, _P, _c.c_int,
+                                         _c.c_int64, _c.c_int64, _P, _c.c_uint64, _P]),
+    "bfm_batch_initialize": (_c.c_int, [_P]),
+    "bfm_batch_run": (_c.c_int, [_P, _P, _c.c_size_t]),
+    "bfm_batch_get_positions": (_c.c_int, [_P, _c.c_uint32, _P, _c.c_size_t]),
+    "bfm_batch_get_state": (_c.c_int, [_P, _c.c_uint32, _P, _P, _P]),
+    "bfm_batch_get_lattice": (_c.c_int, [_P, _c.c_uint32, _P, _c.c_size_t, _P]),
+    "bfm_batch_info": (_c.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "bfm_get_lattice": (_c.c_int, [_P, _P, _c.c_size_t]),
     "bfm_get_lattice_words": (_c.c_int, [_P, _c.POINTER(_c.c_size_t)]),
     "bfm_get_nspecies": (_c.c_int, [_P, _c.POINTER(_c.c_uint32)]),

@@ -378,3 +378,131 @@ def chain_observables(pos: np.ndarray, chains) -> tuple[float, float]:
         re2.append(float(((c[-1] - c[0]) ** 2).sum()))
         rg2.append(float(((c - c.mean(axis=0)) ** 2).sum(axis=1).mean()))
     return float(np.mean(re2)), float(np.mean(rg2))
+
+
+def _grid_path(L):
+    """Sites (2i, 2j, 2k) of an L^3 box in a boustrophedon order: rows along
+    x alternate direction, layers alternate as a whole, so consecutive sites
+    are one grid step (a (2,0,0)-type bond) apart and no step wraps."""
+    g = L // 2
+    i = np.arange(g)
+    layer = []
+    for j in range(g):
+        row = i if j % 2 == 0 else i[::-1]
+        layer.append(np.stack([row, np.full(g, j), np.zeros(g, np.int64)], axis=1))
+    layer = np.concatenate(layer)
+    out = []
+    for k in range(g):
+        lay = (layer if k % 2 == 0 else layer[::-1]).copy()
+        lay[:, 2] = k
+        out.append(lay)
+    return 2 * np.concatenate(out)
+
+
+def ensemble_system(L: int, n_per_molecule: int, phi: float, star: bool = False, seed: int = 0) -> System:
+    """One system of a batched ensemble: linear chains of n_per_molecule
+    monomers, or 3-arm stars (a core and three arms of (n-1)//3), placed
+    along a grid path through the L^3 box (L a multiple of 8) at volume
+    fraction about phi (8 sites per monomer), with gaps between molecules so
+    that the density is even.  At least one molecule is placed."""
+    rng = np.random.default_rng(seed)
+    path = _grid_path(L)
+    n_sites = len(path)
+    where = np.full((L // 2,) * 3, -1, np.int64)
+    where[path[:, 0] // 2, path[:, 1] // 2, path[:, 2] // 2] = np.arange(n_sites)
+    used = np.zeros(n_sites, bool)
+    arm = max(1, (n_per_molecule - 1) // 3) if star else 0
+    size = 1 + 3 * arm if star else n_per_molecule
+    target = max(size, int(round(phi * L ** 3 / 8)))
+    gap = max(0, int(round(size * (1.0 - min(phi, 0.999)) / max(phi, 1e-3))))
+    pos_l, bonds = [], []
+    cursor = int(rng.integers(0, max(1, gap + 1)))
+    placed = 0
+
+    def free_run(start, length):
+        """first start >= start with path[start:start+length] free"""
+        while start + length <= n_sites:
+            u = np.flatnonzero(used[start:start + length])
+            if u.size == 0:
+                return start
+            start += int(u[-1]) + 1
+        return -1
+
+    while placed + size <= target:
+        first = len(pos_l)
+        if not star:
+            s0 = free_run(cursor, size)
+            if s0 < 0:
+                break
+            used[s0:s0 + size] = True
+            pos_l.extend(path[s0:s0 + size])
+            bonds.extend((first + q, first + q + 1) for q in range(size - 1))
+            cursor = s0 + size + gap
+        else:
+            s0 = free_run(cursor, 2 * arm + 1)
+            ok = False
+            while s0 >= 0:
+                c = s0 + arm
+                ci, cj, ck = path[c] // 2
+                for dk in (1, -1):
+                    kk = ck + dk
+                    if kk < 0 or kk >= L // 2:
+                        continue
+                    q = int(where[ci, cj, kk])
+                    for sgn in (1, -1):
+                        idx = np.arange(q, q + sgn * arm, sgn)
+                        if idx.min() < 0 or idx.max() >= n_sites or used[idx].any():
+                            continue
+                        if np.any((idx >= s0) & (idx <= s0 + 2 * arm)):
+                            continue
+                        ok = True
+                        break
+                    if ok:
+                        break
+                if ok:
+                    break
+                s0 = free_run(s0 + 1, 2 * arm + 1)
+            if not ok:
+                break
+            # core first, then arm 1 (outwards), arm 2 (outwards), arm 3
+            a1 = np.arange(c - 1, s0 - 1, -1)
+            a2 = np.arange(c + 1, s0 + 2 * arm + 1)
+            order = [c, *a1, *a2, *idx]
+            used[np.array(order)] = True
+            pos_l.extend(path[np.array(order)])
+            for arm_ids in (range(1, 1 + arm), range(1 + arm, 1 + 2 * arm), range(1 + 2 * arm, 1 + 3 * arm)):
+                prev = 0
+                for m in arm_ids:
+                    bonds.append((first + prev, first + m))
+                    prev = m
+            cursor = s0 + 2 * arm + 1 + gap
+        placed += size
+    n = len(pos_l)
+    if n == 0:
+        raise ValueError("no molecule fits the box")
+    deg, nbr = _empty_topology(n)
+    for a, b in bonds:
+        _connect(deg, nbr, a, b)
+    pos = np.array(pos_l, dtype=np.int32).reshape(n, 3)
+    chains = [] if star else [(c * size, size) for c in range(n // size)]
+    kind = "star" if star else "linear"
+    return System((L, L, L), pos, deg, nbr, chains=chains,
+                  name=f"{kind}{size}_phi{placed * 8 / L ** 3:.2f}_L{L}")
+
+
+def ensemble(n_systems: int, seed: int = 12345, boxes=(32, 48, 64, 96, 128), n_range=(16, 512), phi_range=(0.1, 0.5),
+             star_fraction: float = 0.5):
+    """A batched ensemble: per system a box edge drawn from boxes, monomers
+    per molecule log-uniform in n_range, volume fraction uniform in
+    phi_range, linear chains or 3-arm stars; returns (systems, parameters)."""
+    rng = np.random.default_rng(seed)
+    out, params = [], []
+    for s in range(n_systems):
+        L = int(rng.choice(boxes))
+        n = int(round(np.exp(rng.uniform(np.log(n_range[0]), np.log(n_range[1])))))
+        phi = float(rng.uniform(*phi_range))
+        star = bool(rng.random() < star_fraction)
+        n = min(n, (L // 2) ** 3 // 3)
+        out.append(ensemble_system(L, n, phi, star, seed=seed + 1 + s))
+        params.append({"L": L, "n": n, "phi": phi, "star": star})
+    return out, params
