@@ -57,6 +57,12 @@ def parse():
                         "with chains of L monomers, states beyond L2)")
     p.add_argument("--sweep-shape", type=int, default=-1,
                    help="persistent-kernel shape (-1 automatic; see bfm_set_sweep_shape)")
+    p.add_argument("--batch", type=int, default=0,
+                   help="time a batched ensemble of this many systems instead (box edges 32..128, chains or "
+                        "3-arm stars of 16..512 monomers, volume fraction 0.1..0.5), against the same systems "
+                        "run one after another through the single-system updater")
+    p.add_argument("--plain-sample", type=int, default=48,
+                   help="systems of the ensemble timed one by one for the plain comparison")
     return p.parse_args()
 
 
@@ -353,6 +359,98 @@ def run_b200(args, ranks):
         print(json.dumps(line), flush=True)
 
 
+def run_batch(args, ranks):
+    """Batched ensemble: every system advances args.mcs_per_step MCS per step
+    in one bfm_batch_run (persistent kernel, one CTA per system).  The plain
+    comparison runs a random sample of the same systems one after another
+    through the single-system updater (its own persistent kernel per
+    system), the way a plain ensemble would be run, and reports the
+    aggregate rate of that sample."""
+    import torch
+
+    import pscbfm_b200 as pb
+    from pscbfm_b200 import systems
+    gpu = ranks.local
+    torch.cuda.set_device(gpu)
+    t = time.perf_counter()
+    sys_, params = systems.ensemble(args.batch, seed=12345 + 1000 * ranks.rank)
+    t_gen = time.perf_counter() - t
+    b = pb.Batch(gpu)
+    for i, s in enumerate(sys_):
+        b.add(s, rng=pb.Rng.Saru, r250_seed=12345 + i)
+    t = time.perf_counter()
+    b.initialize()
+    t_init = time.perf_counter() - t
+    S = args.mcs_per_step
+    for _ in range(args.warmup):
+        b.run(S)
+    clocks = Clocks(gpu)
+    torch.cuda.synchronize()
+    ranks.barrier()
+    clocks.start()
+    dev_ms, e2e_s, attempts, launches = 0.0, 0.0, 0, 0
+    d2h = 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        b.run(S)
+        info = b.info()
+        # read back one system per step (the observable a driver would look at)
+        b.positions(_ % len(sys_))
+        e2e_s += time.perf_counter() - t0
+        dev_ms += info["last_ms"]
+        attempts += info["last_attempts"]
+        launches += info["last_launches"]
+        d2h += sys_[_ % len(sys_)].n * 12
+    torch.cuda.synchronize()
+    ranks.barrier()
+    clk = clocks.stop()
+    value, e2e, total = aggregate(ranks, attempts, dev_ms / 1e3, e2e_s)
+
+    # plain: a sample of the same systems one by one through the single-system updater
+    rng = np.random.default_rng(7)
+    pick = rng.choice(len(sys_), size=min(args.plain_sample, len(sys_)), replace=False)
+    p_att, p_ms, p_wall, p_n = 0, 0.0, 0.0, 0
+    for i in pick:
+        s = sys_[i]
+        if any(v & (v - 1) for v in s.box):
+            continue      # the single-system updater, like the reference, takes powers of two only
+        pb.r250_seed(12345 + int(i))
+        u = pb.UpdaterGPUScBFM_AB_Type().setup(s, gpu=gpu, rng=pb.Rng.Saru)
+        u.runSimulationOnGPU(1)
+        t0 = time.perf_counter()
+        u.runSimulationOnGPU(S)
+        p_wall += time.perf_counter() - t0
+        p_ms += u.getLastRunMs()
+        p_att += s.n * S
+        p_n += 1
+        u.cleanup()
+    plain = p_att / (p_ms / 1e3) if p_ms else None
+    boxes = {}
+    for prm in params:
+        boxes[prm["L"]] = boxes.get(prm["L"], 0) + 1
+    line = {
+        "metric": "attempted moves/s, batched ensemble on 1 B200",
+        "value": value, "unit": UNIT, "n_gpus": ranks.world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic (seeded ensemble generator)",
+        "config": {"workload": f"batched ensemble: {len(sys_)} systems, {total // max(1, args.steps * S) // ranks.world:,} "
+                               f"monomers, box edges {dict(sorted(boxes.items()))}, chains or 3-arm stars of 16..512 "
+                               f"monomers, volume fraction 0.1..0.5, Saru, 2 colours per system",
+                   "mcs_per_step": S, "systems": len(sys_), "generate_s": t_gen, "initialize_s": t_init,
+                   "l2": "ensemble state beyond L2 (lattices and monomer arrays of all systems)"},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": len(sys_) * 16 + 4 * len(sys_),
+                "d2h_bytes_per_step": d2h // max(1, args.steps)},
+        "gpu_launches": launches,
+        "plain": {"value": plain, "unit": UNIT, "systems_timed": p_n,
+                  "wall_rate": p_att / p_wall if p_wall else None,
+                  "how": "sampled systems of the same ensemble, each through the single-system updater in turn"},
+        "speedup_vs_plain": (value / plain) if plain else None,
+        "clocks": clk,
+    }
+    if ranks.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_reference(args, ranks):
     if ranks.rank != 0:
         return
@@ -412,6 +510,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, ranks)
+        elif args.batch:
+            run_batch(args, ranks)
         else:
             run_b200(args, ranks)
     finally:

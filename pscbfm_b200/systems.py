@@ -399,6 +399,26 @@ def _grid_path(L):
     return 2 * np.concatenate(out)
 
 
+def _topology_from_bonds(n, bonds):
+    """deg/nbr from a bond list, partner slots in the order _connect would
+    fill them (bond by bond, first end then second end)."""
+    bonds = np.asarray(bonds, np.int64).reshape(-1, 2)
+    ends = np.empty((2 * len(bonds), 2), np.int64)
+    ends[0::2, 0], ends[0::2, 1] = bonds[:, 0], bonds[:, 1]
+    ends[1::2, 0], ends[1::2, 1] = bonds[:, 1], bonds[:, 0]
+    order = np.argsort(ends[:, 0], kind="stable")
+    node = ends[order, 0]
+    first = np.searchsorted(node, node, side="left")
+    rank = np.arange(len(node)) - first
+    if len(rank) and rank.max() >= 8:
+        raise ValueError("more than 8 bonds on a monomer")
+    deg = np.zeros(n, np.uint8)
+    nbr = np.zeros((n, 8), np.uint32)
+    nbr[node, rank] = ends[order, 1]
+    np.add.at(deg, node, 1)
+    return deg, nbr
+
+
 def ensemble_system(L: int, n_per_molecule: int, phi: float, star: bool = False, seed: int = 0) -> System:
     """One system of a batched ensemble: linear chains of n_per_molecule
     monomers, or 3-arm stars (a core and three arms of (n-1)//3), placed
@@ -408,19 +428,34 @@ def ensemble_system(L: int, n_per_molecule: int, phi: float, star: bool = False,
     rng = np.random.default_rng(seed)
     path = _grid_path(L)
     n_sites = len(path)
-    where = np.full((L // 2,) * 3, -1, np.int64)
-    where[path[:, 0] // 2, path[:, 1] // 2, path[:, 2] // 2] = np.arange(n_sites)
-    used = np.zeros(n_sites, bool)
     arm = max(1, (n_per_molecule - 1) // 3) if star else 0
     size = 1 + 3 * arm if star else n_per_molecule
     target = max(size, int(round(phi * L ** 3 / 8)))
     gap = max(0, int(round(size * (1.0 - min(phi, 0.999)) / max(phi, 1e-3))))
-    pos_l, bonds = [], []
     cursor = int(rng.integers(0, max(1, gap + 1)))
-    placed = 0
+    count = target // size
+    if not star:
+        starts = cursor + np.arange(count) * (size + gap)
+        starts = starts[starts + size <= n_sites]
+        if starts.size == 0:
+            starts = np.array([0])
+        idx = (starts[:, None] + np.arange(size)[None, :]).reshape(-1)
+        n = idx.size
+        pos = path[idx]
+        mol = np.arange(n) // size
+        q = np.arange(n) % size
+        a = np.flatnonzero(q < size - 1)
+        bonds = np.stack([a, a + 1], axis=1)
+        deg, nbr = _topology_from_bonds(n, bonds)
+        chains = [(c * size, size) for c in range(n // size)]
+        name = f"linear{size}_phi{n * 8 / L ** 3:.2f}_L{L}"
+        return System((L, L, L), pos.astype(np.int32), deg, nbr, chains=chains, name=name)
+    where = np.full((L // 2,) * 3, -1, np.int64)
+    where[path[:, 0] // 2, path[:, 1] // 2, path[:, 2] // 2] = np.arange(n_sites)
+    used = np.zeros(n_sites, bool)
+    mols = []
 
     def free_run(start, length):
-        """first start >= start with path[start:start+length] free"""
         while start + length <= n_sites:
             u = np.flatnonzero(used[start:start + length])
             if u.size == 0:
@@ -428,66 +463,54 @@ def ensemble_system(L: int, n_per_molecule: int, phi: float, star: bool = False,
             start += int(u[-1]) + 1
         return -1
 
-    while placed + size <= target:
-        first = len(pos_l)
-        if not star:
-            s0 = free_run(cursor, size)
-            if s0 < 0:
-                break
-            used[s0:s0 + size] = True
-            pos_l.extend(path[s0:s0 + size])
-            bonds.extend((first + q, first + q + 1) for q in range(size - 1))
-            cursor = s0 + size + gap
-        else:
-            s0 = free_run(cursor, 2 * arm + 1)
-            ok = False
-            while s0 >= 0:
-                c = s0 + arm
-                ci, cj, ck = path[c] // 2
-                for dk in (1, -1):
-                    kk = ck + dk
-                    if kk < 0 or kk >= L // 2:
+    steps = np.arange(arm)
+    while len(mols) < max(1, count):
+        s0 = free_run(cursor, 2 * arm + 1)
+        found = None
+        while s0 >= 0 and found is None:
+            c = s0 + arm
+            ci, cj, ck = path[c] // 2
+            for dk in (1, -1):
+                kk = ck + dk
+                if kk < 0 or kk >= L // 2:
+                    continue
+                qq = int(where[ci, cj, kk])
+                for sgn in (1, -1):
+                    idx3 = qq + sgn * steps
+                    if idx3.min() < 0 or idx3.max() >= n_sites or used[idx3].any():
                         continue
-                    q = int(where[ci, cj, kk])
-                    for sgn in (1, -1):
-                        idx = np.arange(q, q + sgn * arm, sgn)
-                        if idx.min() < 0 or idx.max() >= n_sites or used[idx].any():
-                            continue
-                        if np.any((idx >= s0) & (idx <= s0 + 2 * arm)):
-                            continue
-                        ok = True
-                        break
-                    if ok:
-                        break
-                if ok:
+                    if np.any((idx3 >= s0) & (idx3 <= s0 + 2 * arm)):
+                        continue
+                    found = idx3
                     break
+                if found is not None:
+                    break
+            if found is None:
                 s0 = free_run(s0 + 1, 2 * arm + 1)
-            if not ok:
-                break
-            # core first, then arm 1 (outwards), arm 2 (outwards), arm 3
-            a1 = np.arange(c - 1, s0 - 1, -1)
-            a2 = np.arange(c + 1, s0 + 2 * arm + 1)
-            order = [c, *a1, *a2, *idx]
-            used[np.array(order)] = True
-            pos_l.extend(path[np.array(order)])
-            for arm_ids in (range(1, 1 + arm), range(1 + arm, 1 + 2 * arm), range(1 + 2 * arm, 1 + 3 * arm)):
-                prev = 0
-                for m in arm_ids:
-                    bonds.append((first + prev, first + m))
-                    prev = m
-            cursor = s0 + 2 * arm + 1 + gap
-        placed += size
-    n = len(pos_l)
-    if n == 0:
+        if found is None:
+            break
+        c = s0 + arm
+        order = np.concatenate([[c], np.arange(c - 1, s0 - 1, -1), np.arange(c + 1, s0 + 2 * arm + 1), found])
+        used[order] = True
+        mols.append(order)
+        cursor = s0 + 2 * arm + 1 + gap
+    if not mols:
         raise ValueError("no molecule fits the box")
-    deg, nbr = _empty_topology(n)
-    for a, b in bonds:
-        _connect(deg, nbr, a, b)
-    pos = np.array(pos_l, dtype=np.int32).reshape(n, 3)
-    chains = [] if star else [(c * size, size) for c in range(n // size)]
-    kind = "star" if star else "linear"
-    return System((L, L, L), pos, deg, nbr, chains=chains,
-                  name=f"{kind}{size}_phi{placed * 8 / L ** 3:.2f}_L{L}")
+    idx = np.concatenate(mols)
+    n = idx.size
+    pos = path[idx]
+    # per star: core -> arm k's first monomer, then along each arm
+    base = (np.arange(len(mols)) * size)[:, None]
+    tmpl = []
+    for k in range(3):
+        first = 1 + k * arm
+        tmpl.append((0, first))
+        tmpl.extend((first + t, first + t + 1) for t in range(arm - 1))
+    tmpl = np.array(tmpl, np.int64)
+    bonds = (base[:, :, None] + tmpl[None, :, :]).reshape(-1, 2)
+    deg, nbr = _topology_from_bonds(n, bonds)
+    name = f"star{size}_phi{n * 8 / L ** 3:.2f}_L{L}"
+    return System((L, L, L), pos.astype(np.int32), deg, nbr, name=name)
 
 
 def ensemble(n_systems: int, seed: int = 12345, boxes=(32, 48, 64, 96, 128), n_range=(16, 512), phi_range=(0.1, 0.5),
