@@ -174,6 +174,32 @@ int bfm_batch_get_lattice(bfm_batch *b, uint32_t sys, uint32_t *words, size_t nw
 int bfm_batch_info(const bfm_batch *b, uint32_t *nsys, uint64_t *monomers, uint32_t *nspecies_max, double *last_ms,
                    uint64_t *last_launches, uint64_t *last_attempts);
 
+/* ---- the learned schedule's network (no counterpart in the reference):
+ * in -> hidden -> hidden -> out with ReLU, trained and evaluated on the GPU
+ * by the library's own tensor-core kernels (bf16 operands, fp32
+ * accumulation; fp32 master parameters and Adam moments).  Parameters are
+ * one fp32 vector [W1 (hidden x in), b1, W2 (hidden x hidden), b2,
+ * W3 (out x hidden), b3], row-major (out x in); He-uniform start from seed.
+ * Widths: in and out 1..64, hidden 1..512.  x: batch x in, y and targets:
+ * batch x out, row-major host arrays; out_weight (NULL = all 1) weights the
+ * squared error of each output; loss = sum_o w_o (y - t)^2 averaged over the
+ * batch. */
+typedef struct bfm_mlp bfm_mlp;
+int bfm_mlp_create(int gpu, uint32_t n_in, uint32_t n_hidden, uint32_t n_out, uint64_t seed, bfm_mlp **out);
+int bfm_mlp_destroy(bfm_mlp *m);
+const char *bfm_mlp_last_error(const bfm_mlp *m);
+int bfm_mlp_num_params(const bfm_mlp *m, size_t *n);
+/* setting the parameters also resets the Adam moments */
+int bfm_mlp_set_params(bfm_mlp *m, const float *params, size_t n);
+int bfm_mlp_get_params(bfm_mlp *m, float *params, size_t n);
+int bfm_mlp_forward(bfm_mlp *m, const float *x, uint32_t batch, float *y);
+/* loss and its gradient with respect to every parameter (no update) */
+int bfm_mlp_gradients(bfm_mlp *m, const float *x, const float *y_target, const float *out_weight, uint32_t batch, float *grad,
+                      size_t n, float *loss);
+/* one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the batch; *loss is the loss before the step */
+int bfm_mlp_train_step(bfm_mlp *m, const float *x, const float *y_target, const float *out_weight, uint32_t batch, float lr,
+                       float *loss);
+
 /* cleanup (.h:487, .cu:3486-3502): frees the set-up; setters may be used again */
 int bfm_cleanup(bfm_handle *h);
 

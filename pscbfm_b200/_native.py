@@ -18,7 +18,7 @@ LIBNAME = "libpscbfm_b200.so"
 LIBPATH = os.path.join(HERE, LIBNAME)
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["bfm_engine.cu", "bfm_diag.cu", "bfm_color.cu", "bfm_batch.cu"]
+SOURCES = ["bfm_engine.cu", "bfm_diag.cu", "bfm_color.cu", "bfm_batch.cu", "bfm_mlp.cu"]
 HEADERS = ["bfm_device.cuh", "bfm_host.hpp", "bfm_sweep.cuh", "bfm_analyze.cuh", "bfm_color.hpp", "../../include/pscbfm_b200.h"]
 
 NVCC_FLAGS = [
@@ -115,6 +115,15 @@ _SIGS = {
     "bfm_batch_get_state": (_c.c_int, [_P, _c.c_uint32, _P, _P, _P]),
     "bfm_batch_get_lattice": (_c.c_int, [_P, _c.c_uint32, _P, _c.c_size_t, _P]),
     "bfm_batch_info": (_c.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    "bfm_mlp_create": (_c.c_int, [_c.c_int, _c.c_uint32, _c.c_uint32, _c.c_uint32, _c.c_uint64, _c.POINTER(_P)]),
+    "bfm_mlp_destroy": (_c.c_int, [_P]),
+    "bfm_mlp_last_error": (_c.c_char_p, [_P]),
+    "bfm_mlp_num_params": (_c.c_int, [_P, _P]),
+    "bfm_mlp_set_params": (_c.c_int, [_P, _P, _c.c_size_t]),
+    "bfm_mlp_get_params": (_c.c_int, [_P, _P, _c.c_size_t]),
+    "bfm_mlp_forward": (_c.c_int, [_P, _P, _c.c_uint32, _P]),
+    "bfm_mlp_gradients": (_c.c_int, [_P, _P, _P, _P, _c.c_uint32, _P, _c.c_size_t, _P]),
+    "bfm_mlp_train_step": (_c.c_int, [_P, _P, _P, _P, _c.c_uint32, _c.c_float, _P]),
     "bfm_get_lattice": (_c.c_int, [_P, _P, _c.c_size_t]),
     "bfm_get_lattice_words": (_c.c_int, [_P, _c.POINTER(_c.c_size_t)]),
     "bfm_get_nspecies": (_c.c_int, [_P, _c.POINTER(_c.c_uint32)]),

@@ -187,43 +187,64 @@ __global__ void __launch_bounds__(kThreads, 2)
         const Work wk = work[sid];
         const uint32_t base = s.base, nSp = s.nSpecies;
         unsigned int myCand = 0, myAcc = 0;
+        /* colour and seed of the first substep; later ones are drawn by
+         * thread 0 while the targets are cleared */
+        if (tid == 0 && wk.steps) {
+            s_sp = r250_next(st) % nSp; /* .cu:3065 */
+            s_seed = r250_next(st);     /* .cu:3066 */
+        }
+        __syncthreads();
         for (uint32_t iStep = 0; iStep < wk.steps; ++iStep) {
             const uint64_t a = (uint64_t)(wk.age + iStep); /* mAge, advanced once per MCS (.cu:3002) */
             const uint64_t callStep = (uint64_t)wk.done + iStep;
             for (uint32_t sub = 0; sub < nSp; ++sub) {
-                if (tid == 0) {
-                    s_sp = r250_next(st) % nSp; /* .cu:3065 */
-                    s_seed = r250_next(st);     /* .cu:3066 */
-                }
-                __syncthreads();
                 const uint32_t sp = s_sp, seed = s_seed;
                 const uint64_t currentAge = a + callStep * nSp + sub; /* .cu:3049 */
                 const uint32_t iter = (uint32_t)currentAge, iterHi = (uint32_t)(currentAge >> 32);
                 const uint32_t off = base + s.spOff[sp], cnt = s.spOff[sp + 1] - s.spOff[sp];
                 if (tid == 0) s_att += cnt;
 
-                /* check (.cu:930-1028) */
-                for (uint32_t i = tid; i < cnt; i += blockDim.x) {
-                    const uint32_t slot = off + i;
-                    const uint32_t r0 = A.pos[slot];
-                    const int dir = direction(draw_any(s.rng, seed, iter, i, iterHi));
-                    bool w;
-                    const uint32_t r1 = wmove(r0, dir, s, w);
-                    bool ok = true;
-                    const uint32_t dg = A.deg[slot];
-                    for (uint32_t j = 0; j < dg; ++j) {
-                        const uint32_t code = zbond(A.pos[A.nbr[(size_t)j * A.T + slot]], r1);
-                        if ((s.forbidden[code >> 5] >> (code & 31u)) & 1u) {
-                            ok = false;
-                            break;
+                /* check (.cu:930-1028), two monomers in flight per thread */
+                for (uint32_t i0 = tid; i0 < cnt; i0 += 2u * blockDim.x) {
+                    uint32_t slot[2], r0[2], r1[2], dg[2];
+                    int dir[2];
+                    bool live[2], ok[2];
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        const uint32_t i = i0 + (uint32_t)u * blockDim.x;
+                        live[u] = i < cnt;
+                        slot[u] = off + (live[u] ? i : 0u);
+                        r0[u] = live[u] ? A.pos[slot[u]] : 0u;
+                        dg[u] = live[u] ? A.deg[slot[u]] : 0u;
+                        ok[u] = live[u];
+                    }
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        dir[u] = direction(draw_any(s.rng, seed, iter, i0 + (uint32_t)u * blockDim.x, iterHi));
+                        bool w;
+                        r1[u] = wmove(r0[u], dir[u], s, w);
+                    }
+                    const uint32_t dmax = dg[0] > dg[1] ? dg[0] : dg[1];
+                    for (uint32_t j = 0; j < dmax; ++j) {
+#pragma unroll
+                        for (int u = 0; u < 2; ++u)
+                            if (ok[u] && j < dg[u]) {
+                                const uint32_t code = zbond(A.pos[A.nbr[(size_t)j * A.T + slot[u]]], r1[u]);
+                                if ((s.forbidden[code >> 5] >> (code & 31u)) & 1u) ok[u] = false;
+                            }
+                    }
+#pragma unroll
+                    for (int u = 0; u < 2; ++u)
+                        if (ok[u]) ok[u] = !face9(lat, r0[u], dir[u], s);
+#pragma unroll
+                    for (int u = 0; u < 2; ++u)
+                        if (live[u]) {
+                            if (ok[u]) {
+                                atomicOr(tmp + (r1[u] >> 5), 1u << (r1[u] & 31u));
+                                ++myCand;
+                            }
+                            A.flags[slot[u]] = ok[u] ? (uint8_t)(dir[u] | 8) : (uint8_t)0;
                         }
-                    }
-                    if (ok) ok = !face9(lat, r0, dir, s);
-                    if (ok) {
-                        atomicOr(tmp + (r1 >> 5), 1u << (r1 & 31u));
-                        ++myCand;
-                    }
-                    A.flags[slot] = ok ? (uint8_t)(dir | 8) : (uint8_t)0;
                 }
                 __syncthreads();
 
@@ -252,14 +273,24 @@ __global__ void __launch_bounds__(kThreads, 2)
                 }
                 __syncthreads();
 
-                /* clear this substep's targets */
-                for (uint32_t i = tid; i < cnt; i += blockDim.x) {
-                    const uint32_t slot = off + i;
-                    const uint8_t f = A.flags[slot];
-                    if (!(f & 8)) continue;
-                    bool w;
-                    const uint32_t r1 = (f & 16) ? A.pos[slot] : wmove(A.pos[slot], f & 7, s, w);
-                    tmp[r1 >> 5] = 0u;
+                /* clear this substep's targets: the whole buffer when it is in
+                 * shared memory, the candidates' words otherwise */
+                if (tid == 0 && !(iStep + 1 == wk.steps && sub + 1 == nSp)) {
+                    s_sp = r250_next(st) % nSp;
+                    s_seed = r250_next(st);
+                }
+                if (inSmem) {
+                    uint4 *t4 = reinterpret_cast<uint4 *>(tmp);
+                    for (uint32_t w = tid; w < lw / 4; w += blockDim.x) t4[w] = make_uint4(0u, 0u, 0u, 0u);
+                } else {
+                    for (uint32_t i = tid; i < cnt; i += blockDim.x) {
+                        const uint32_t slot = off + i;
+                        const uint8_t f = A.flags[slot];
+                        if (!(f & 8)) continue;
+                        bool w;
+                        const uint32_t r1 = (f & 16) ? A.pos[slot] : wmove(A.pos[slot], f & 7, s, w);
+                        tmp[r1 >> 5] = 0u;
+                    }
                 }
                 __syncthreads();
             }

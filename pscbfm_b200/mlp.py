@@ -1,0 +1,91 @@
+"""The learned schedule's network on the GPU (``bfm_mlp_*`` in
+include/pscbfm_b200.h): in -> hidden -> hidden -> out with ReLU, bf16
+tensor-core products with fp32 accumulation, fp32 masters and Adam."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native
+
+
+class MLP:
+    def __init__(self, n_in: int = 6, n_hidden: int = 128, n_out: int = 4, seed: int = 0, gpu: int = 0):
+        self._lib = _native.lib()
+        h = ctypes.c_void_p()
+        st = self._lib.bfm_mlp_create(int(gpu), int(n_in), int(n_hidden), int(n_out), int(seed), ctypes.byref(h))
+        if st != _native.BFM_OK:
+            raise (ValueError if st == _native.BFM_EINVAL else RuntimeError)(f"bfm_mlp_create failed with status {st}")
+        self._h = h
+        self.shape = (int(n_in), int(n_hidden), int(n_out))
+        n = ctypes.c_size_t()
+        self._check(self._lib.bfm_mlp_num_params(self._h, ctypes.byref(n)))
+        self.n_params = n.value
+
+    def _check(self, st):
+        if st == _native.BFM_OK:
+            return
+        msg = (self._lib.bfm_mlp_last_error(self._h) or b"").decode()
+        raise (ValueError if st == _native.BFM_EINVAL else RuntimeError)(f"status {st}: {msg}")
+
+    @staticmethod
+    def _f32(a, cols=None):
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        if cols is not None and (a.ndim != 2 or a.shape[1] != cols):
+            raise ValueError(f"expected an array of shape (batch, {cols})")
+        return a
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.n_params, np.float32)
+        self._check(self._lib.bfm_mlp_get_params(self._h, out.ctypes.data, out.size))
+        return out
+
+    def set_params(self, p):
+        p = self._f32(p).ravel()
+        self._check(self._lib.bfm_mlp_set_params(self._h, p.ctypes.data, p.size))
+
+    def forward(self, x) -> np.ndarray:
+        x = self._f32(x, self.shape[0])
+        y = np.empty((x.shape[0], self.shape[2]), np.float32)
+        self._check(self._lib.bfm_mlp_forward(self._h, x.ctypes.data, x.shape[0], y.ctypes.data))
+        return y
+
+    def gradients(self, x, t, w=None):
+        x, t = self._f32(x, self.shape[0]), self._f32(t, self.shape[2])
+        wv = None if w is None else self._f32(w)
+        g = np.empty(self.n_params, np.float32)
+        loss = ctypes.c_float()
+        self._check(self._lib.bfm_mlp_gradients(self._h, x.ctypes.data, t.ctypes.data, None if wv is None else wv.ctypes.data,
+                                                x.shape[0], g.ctypes.data, g.size, ctypes.byref(loss)))
+        return loss.value, g
+
+    def train_step(self, x, t, w=None, lr: float = 1e-3) -> float:
+        x, t = self._f32(x, self.shape[0]), self._f32(t, self.shape[2])
+        wv = None if w is None else self._f32(w)
+        loss = ctypes.c_float()
+        self._check(self._lib.bfm_mlp_train_step(self._h, x.ctypes.data, t.ctypes.data, None if wv is None else wv.ctypes.data,
+                                                 x.shape[0], float(lr), ctypes.byref(loss)))
+        return loss.value
+
+    def fit(self, x, t, w=None, epochs: int = 200, batch: int = 256, lr: float = 1e-3, seed: int = 0):
+        """mini-batch Adam over shuffled data; returns the loss per epoch"""
+        x, t = self._f32(x, self.shape[0]), self._f32(t, self.shape[2])
+        rng = np.random.default_rng(seed)
+        hist = []
+        for _ in range(epochs):
+            idx = rng.permutation(len(x))
+            tot = 0.0
+            for b0 in range(0, len(x), batch):
+                sel = idx[b0:b0 + batch]
+                tot += self.train_step(x[sel], t[sel], w, lr) * len(sel)
+            hist.append(tot / len(x))
+        return hist
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.bfm_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
