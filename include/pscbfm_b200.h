@@ -166,6 +166,9 @@ int bfm_batch_initialize(bfm_batch *b);
 int bfm_batch_run(bfm_batch *b, const uint32_t *mcs, size_t nsys);
 /* unfolded positions of system sys, original monomer order (doCopyBack, .cu:3402-3484) */
 int bfm_batch_get_positions(bfm_batch *b, uint32_t sys, int32_t *pos3, size_t n);
+/* positions of every system at once: systems in the order added, each in
+ * its original monomer order (n_total >= all monomers; 3 ints each) */
+int bfm_batch_get_all_positions(bfm_batch *b, int32_t *pos3, size_t n_total);
 /* age, R250 state (251 words) and counters (attempts, candidates, accepts) of system sys; any pointer may be NULL */
 int bfm_batch_get_state(bfm_batch *b, uint32_t sys, int64_t *age, uint32_t *r250_state251, uint64_t *counters3);
 /* occupation bits of system sys (Z-order of the box padded to powers of two); *needed receives the word count */

@@ -77,6 +77,14 @@ class Batch:
         self._check(self._lib.bfm_batch_get_positions(self._h, int(sys), out.ctypes.data, self._sizes[sys]))
         return out
 
+    def all_positions(self) -> list:
+        """positions of every system (one bulk read-back), as a list of (n, 3) arrays"""
+        total = sum(self._sizes)
+        out = np.empty((total, 3), np.int32)
+        self._check(self._lib.bfm_batch_get_all_positions(self._h, out.ctypes.data, total))
+        cuts = np.cumsum([0] + self._sizes)
+        return [out[cuts[i]:cuts[i + 1]] for i in range(len(self._sizes))]
+
     def state(self, sys: int):
         """(age, R250 state of 251 words, (attempts, candidates, accepts))"""
         age = ctypes.c_int64()

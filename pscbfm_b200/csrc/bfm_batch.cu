@@ -817,6 +817,28 @@ struct Batch {
         BCK(cudaStreamSynchronize(stream));
     }
 
+    /* every system's unfolded positions, systems in order, each in its original monomer order */
+    void allPositions(int32_t *out, size_t n)
+    {
+        if (!initialized) throw Err("bfm_batch_initialize must be called first");
+        if (n < T) throw ArgErr("output buffer too small");
+        BCK(cudaSetDevice(gpu));
+        if (outCap < 3 * (size_t)T) {
+            bfree(d_out);
+            balloc(d_out, 3 * (size_t)T);
+            outCap = 3 * (size_t)T;
+        }
+        for (const SysDesc &d : desc) {
+            int32_t L[3];
+            for (int a = 0; a < 3; ++a) L[a] = (int32_t)undilate3(d.top[a] >> a) + 1;
+            const int blocks = (int)std::min<uint32_t>((d.n + 255) / 256, 148 * 8);
+            k_unfold<<<blocks, 256, 0, stream>>>(d_pos, d_img, d_s2o, T, d.base, d.n, L[0], L[1], L[2], d_out + 3 * (size_t)d.base);
+        }
+        BCK(cudaGetLastError());
+        BCK(cudaMemcpyAsync(out, d_out, 3 * (size_t)T * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+        BCK(cudaStreamSynchronize(stream));
+    }
+
     void state(uint32_t sI, int64_t *a, uint32_t *r250, uint64_t *counters)
     {
         if (!initialized) throw Err("bfm_batch_initialize must be called first");
@@ -904,6 +926,8 @@ int bfm_batch_initialize(bfm_batch *h) { BGUARD(h, { h->b.initialize(); }); }
 int bfm_batch_run(bfm_batch *h, const uint32_t *mcs, size_t nsys) { BGUARD(h, { h->b.run(mcs, nsys); }); }
 
 int bfm_batch_get_positions(bfm_batch *h, uint32_t sys, int32_t *pos3, size_t n) { BGUARD(h, { h->b.positions(sys, pos3, n); }); }
+
+int bfm_batch_get_all_positions(bfm_batch *h, int32_t *pos3, size_t n_total) { BGUARD(h, { h->b.allPositions(pos3, n_total); }); }
 
 int bfm_batch_get_state(bfm_batch *h, uint32_t sys, int64_t *age, uint32_t *r250_state251, uint64_t *counters3)
 {

@@ -1,0 +1,83 @@
+"""The learned run schedule (pscbfm_b200/schedule.py).
+
+CPU: the label extraction on synthetic series with known answers
+(exponential approach to a plateau, end vectors of an AR(1) process), the
+molecule bookkeeping of the ensemble generator, and the schedule
+comparison: with exact predictions of spread equilibration times the
+learned budgets cost less than the smallest fixed budget of equal R_e^2
+error, and a too-small prediction is extended by the measured drift check.
+GPU: the whole pipeline on a small ensemble (record with the batched
+simulator, train the network with the library's kernels, compare)."""
+import math
+
+import numpy as np
+import pytest
+
+from pscbfm_b200 import schedule as sch
+from pscbfm_b200 import systems
+
+
+def _series(tau, plateau=100.0, n=500, T=20000.0, every=100.0, seed=0):
+    rng = np.random.default_rng(seed)
+    t = np.arange(0, T + every, every)
+    re2 = plateau * (1 - 0.8 * np.exp(-t / tau)) * (1 + 0.003 * rng.normal(size=t.size))
+    return {"t": t, "re2": re2, "rg2": re2 / 6, "ends": np.zeros((t.size, 4, 3), np.float32), "n": n}
+
+
+def test_equilibration_time_of_an_exponential_approach():
+    s = _series(1000.0)
+    teq, plat = sch.equilibration_time(s["t"], s["re2"])
+    # 0.8 exp(-t/tau) <= 0.1 at t = tau ln 8
+    assert abs(teq - 1000.0 * math.log(8)) < 400 and abs(plat - 100.0) < 1.0
+
+
+def test_relaxation_time_of_ar1_end_vectors():
+    rng = np.random.default_rng(2)
+    tau, dt = 500.0, 50.0
+    a = math.exp(-dt / tau)
+    e = np.zeros((600, 400, 3))
+    e[0] = rng.normal(size=(400, 3))
+    for k in range(1, 600):
+        e[k] = a * e[k - 1] + math.sqrt(1 - a * a) * rng.normal(size=(400, 3))
+    t = np.arange(600) * dt
+    assert abs(sch.relaxation_time(t, e, 0) - tau) < 0.15 * tau
+
+
+@pytest.mark.parametrize("star", [False, True])
+def test_molecule_bookkeeping_matches_the_generator(star):
+    s = systems.ensemble_system(32, 25, 0.3, star, seed=4)
+    m = sch.molecules(s, 25, star)
+    assert m["count"] * m["size"] == s.n
+    re2, rg2, ends = sch.observables(s.pos, m)
+    assert re2 > 0 and rg2 > 0 and len(ends) == m["count"] * (3 if star else 1)
+    if not star:
+        a, b = m["ends"]
+        assert (s.deg[a] == 1).all() and (s.deg[b] == 1).all()
+    else:
+        core, tips = m["ends"]
+        assert (s.deg[core] == 3).all() and (s.deg[tips] == 1).all()
+
+
+def test_learned_budgets_beat_a_fixed_budget_with_exact_predictions():
+    taus = np.exp(np.random.default_rng(5).uniform(np.log(100), np.log(5000), 60))
+    ser = [_series(tau, seed=i) for i, tau in enumerate(taus)]
+    pred = np.log10(taus * math.log(8))
+    b = sch.learned_budgets(pred, ser)
+    rep = sch.compare(ser, b)
+    assert rep["systems_per_hour_ratio"] > 1.5
+    assert rep["plain"]["mean_rel_err_re2"] <= rep["learned"]["mean_rel_err_re2"] + 1e-12
+
+
+def test_drift_check_extends_an_underbudgeted_run():
+    s = _series(3000.0)
+    b = sch.learned_budgets(np.array([np.log10(50.0)]), [s], factor=1.0)
+    assert b[0] > 3000.0
+
+
+@pytest.mark.gpu
+def test_pipeline_on_a_small_ensemble():
+    rep = sch.run(n_systems=192, mcs=3000, every=100, epochs=60, seed=3)
+    assert rep["systems"] == 192 and rep["batch_rate_moves_per_s"] > 1e8
+    assert rep["train_loss_first_last"][1] < rep["train_loss_first_last"][0]
+    assert rep["schedule"]["learned"]["cost_moves"] > 0 and rep["schedule"]["plain"]["cost_moves"] > 0
+    assert all(np.isfinite(v) for v in rep["test_rmse"].values())
