@@ -161,6 +161,9 @@ int bfm_batch_add_system(bfm_batch *b, uint32_t Lx, uint32_t Ly, uint32_t Lz, ui
 /* colours, slabs, lattices and device state of every system (initialize,
  * .cu:2393-2537, per system) */
 int bfm_batch_initialize(bfm_batch *b);
+/* systems whose lattice exceeds 64^3 (padded) are shared by a cluster of 4
+ * CTAs (default on); off: one CTA per system for every system */
+int bfm_batch_set_clusters(bfm_batch *b, int on);
 /* system s advances by mcs[s] Monte-Carlo steps (0 leaves it as it is); nsys
  * must equal the number of systems */
 int bfm_batch_run(bfm_batch *b, const uint32_t *mcs, size_t nsys);

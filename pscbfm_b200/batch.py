@@ -60,6 +60,11 @@ class Batch:
         self._sizes.append(int(system.n))
         return sid.value
 
+    def set_clusters(self, on: bool):
+        """large systems shared by a cluster of 4 CTAs (default) or one CTA each"""
+        self._check(self._lib.bfm_batch_set_clusters(self._h, int(bool(on))))
+        return self
+
     def initialize(self):
         self._check(self._lib.bfm_batch_initialize(self._h))
         return self

@@ -148,6 +148,144 @@ struct Arrays {
     unsigned long long *counters; /* 3 per system: attempts, candidates, accepts */
 };
 
+/* every synchronisation of the phases of one system: the CTA, or the
+ * whole cluster when a cluster shares the system (release/acquire at cluster
+ * scope, which orders the global-memory lattice and target updates too) */
+__device__ __forceinline__ void cluster_barrier()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+template <bool CL>
+__device__ __forceinline__ void group_sync()
+{
+    if (CL)
+        cluster_barrier();
+    else
+        __syncthreads();
+}
+
+/* wk.steps MCS of one system: this thread takes monomers first, first +
+ * stride, ... of every species slab (stride = threads sharing the system);
+ * the leader thread of each CTA draws the colour / seed sequence into its
+ * CTA's shared copy (every CTA of a cluster draws the same sequence) */
+template <bool CL>
+__device__ __forceinline__ void advance(const SysDesc &s, uint32_t *st, const Work wk, uint32_t *lat, uint32_t *tmp, bool inSmem,
+                                        uint32_t lw, uint32_t first, uint32_t stride, const Arrays &A, uint32_t &s_sp,
+                                        uint32_t &s_seed, unsigned long long &s_att, bool leader, unsigned int &myCand,
+                                        unsigned int &myAcc, bool countAtt = true)
+{
+    const uint32_t base = s.base, nSp = s.nSpecies;
+        /* colour and seed of the first substep; later ones are drawn by
+         * thread 0 while the targets are cleared */
+        if (leader && wk.steps) {
+            s_sp = r250_next(st) % nSp; /* .cu:3065 */
+            s_seed = r250_next(st);     /* .cu:3066 */
+        }
+        group_sync<CL>();
+        for (uint32_t iStep = 0; iStep < wk.steps; ++iStep) {
+            const uint64_t a = (uint64_t)(wk.age + iStep); /* mAge, advanced once per MCS (.cu:3002) */
+            const uint64_t callStep = (uint64_t)wk.done + iStep;
+            for (uint32_t sub = 0; sub < nSp; ++sub) {
+                const uint32_t sp = s_sp, seed = s_seed;
+                const uint64_t currentAge = a + callStep * nSp + sub; /* .cu:3049 */
+                const uint32_t iter = (uint32_t)currentAge, iterHi = (uint32_t)(currentAge >> 32);
+                const uint32_t off = base + s.spOff[sp], cnt = s.spOff[sp + 1] - s.spOff[sp];
+                if (leader && countAtt) s_att += cnt;
+
+                /* check (.cu:930-1028), two monomers in flight per thread */
+                for (uint32_t i0 = first; i0 < cnt; i0 += 2u * stride) {
+                    uint32_t slot[2], r0[2], r1[2], dg[2];
+                    int dir[2];
+                    bool live[2], ok[2];
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        const uint32_t i = i0 + (uint32_t)u * stride;
+                        live[u] = i < cnt;
+                        slot[u] = off + (live[u] ? i : 0u);
+                        r0[u] = live[u] ? A.pos[slot[u]] : 0u;
+                        dg[u] = live[u] ? A.deg[slot[u]] : 0u;
+                        ok[u] = live[u];
+                    }
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        dir[u] = direction(draw_any(s.rng, seed, iter, i0 + (uint32_t)u * stride, iterHi));
+                        bool w;
+                        r1[u] = wmove(r0[u], dir[u], s, w);
+                    }
+                    const uint32_t dmax = dg[0] > dg[1] ? dg[0] : dg[1];
+                    for (uint32_t j = 0; j < dmax; ++j) {
+#pragma unroll
+                        for (int u = 0; u < 2; ++u)
+                            if (ok[u] && j < dg[u]) {
+                                const uint32_t code = zbond(A.pos[A.nbr[(size_t)j * A.T + slot[u]]], r1[u]);
+                                if ((s.forbidden[code >> 5] >> (code & 31u)) & 1u) ok[u] = false;
+                            }
+                    }
+#pragma unroll
+                    for (int u = 0; u < 2; ++u)
+                        if (ok[u]) ok[u] = !face9(lat, r0[u], dir[u], s);
+#pragma unroll
+                    for (int u = 0; u < 2; ++u)
+                        if (live[u]) {
+                            if (ok[u]) {
+                                atomicOr(tmp + (r1[u] >> 5), 1u << (r1[u] & 31u));
+                                ++myCand;
+                            }
+                            A.flags[slot[u]] = ok[u] ? (uint8_t)(dir[u] | 8) : (uint8_t)0;
+                        }
+                }
+                group_sync<CL>();
+
+                /* perform (.cu:1148-1190) */
+                for (uint32_t i = first; i < cnt; i += stride) {
+                    const uint32_t slot = off + i;
+                    const uint8_t f = A.flags[slot];
+                    if (!(f & 8)) continue;
+                    const uint32_t r0 = A.pos[slot];
+                    const int dir = f & 7;
+                    if (face9(tmp, r0, dir, s)) continue;
+                    bool wrapped;
+                    const uint32_t r1 = wmove(r0, dir, s, wrapped);
+                    const uint32_t w0 = r0 >> 5, w1 = r1 >> 5;
+                    const uint32_t b0 = 1u << (r0 & 31u), b1 = 1u << (r1 & 31u);
+                    if (w0 == w1) {
+                        atomicXor(lat + w0, b0 | b1);
+                    } else {
+                        atomicXor(lat + w0, b0);
+                        atomicXor(lat + w1, b1);
+                    }
+                    A.pos[slot] = r1;
+                    if (wrapped) A.img[(size_t)(dir >> 1) * A.T + slot] += (dir & 1) ? 1 : -1;
+                    A.flags[slot] = f | 16;
+                    ++myAcc;
+                }
+                group_sync<CL>();
+
+                /* clear this substep's targets: the whole buffer when it is in
+                 * shared memory, the candidates' words otherwise */
+                if (leader && !(iStep + 1 == wk.steps && sub + 1 == nSp)) {
+                    s_sp = r250_next(st) % nSp;
+                    s_seed = r250_next(st);
+                }
+                if (inSmem) {
+                    uint4 *t4 = reinterpret_cast<uint4 *>(tmp);
+                    for (uint32_t w = first; w < lw / 4; w += stride) t4[w] = make_uint4(0u, 0u, 0u, 0u);
+                } else {
+                    for (uint32_t i = first; i < cnt; i += stride) {
+                        const uint32_t slot = off + i;
+                        const uint8_t f = A.flags[slot];
+                        if (!(f & 8)) continue;
+                        bool w;
+                        const uint32_t r1 = (f & 16) ? A.pos[slot] : wmove(A.pos[slot], f & 7, s, w);
+                        tmp[r1 >> 5] = 0u;
+                    }
+                }
+                group_sync<CL>();
+            }
+        }
+
+}
+
 __global__ void __launch_bounds__(kThreads, 2)
     k_batch(const SysDesc *__restrict__ desc, const Work *__restrict__ work, const uint32_t *__restrict__ order,
             uint32_t nOrder, unsigned int *next, Arrays A)
@@ -185,116 +323,8 @@ __global__ void __launch_bounds__(kThreads, 2)
         __syncthreads();
 
         const Work wk = work[sid];
-        const uint32_t base = s.base, nSp = s.nSpecies;
         unsigned int myCand = 0, myAcc = 0;
-        /* colour and seed of the first substep; later ones are drawn by
-         * thread 0 while the targets are cleared */
-        if (tid == 0 && wk.steps) {
-            s_sp = r250_next(st) % nSp; /* .cu:3065 */
-            s_seed = r250_next(st);     /* .cu:3066 */
-        }
-        __syncthreads();
-        for (uint32_t iStep = 0; iStep < wk.steps; ++iStep) {
-            const uint64_t a = (uint64_t)(wk.age + iStep); /* mAge, advanced once per MCS (.cu:3002) */
-            const uint64_t callStep = (uint64_t)wk.done + iStep;
-            for (uint32_t sub = 0; sub < nSp; ++sub) {
-                const uint32_t sp = s_sp, seed = s_seed;
-                const uint64_t currentAge = a + callStep * nSp + sub; /* .cu:3049 */
-                const uint32_t iter = (uint32_t)currentAge, iterHi = (uint32_t)(currentAge >> 32);
-                const uint32_t off = base + s.spOff[sp], cnt = s.spOff[sp + 1] - s.spOff[sp];
-                if (tid == 0) s_att += cnt;
-
-                /* check (.cu:930-1028), two monomers in flight per thread */
-                for (uint32_t i0 = tid; i0 < cnt; i0 += 2u * blockDim.x) {
-                    uint32_t slot[2], r0[2], r1[2], dg[2];
-                    int dir[2];
-                    bool live[2], ok[2];
-#pragma unroll
-                    for (int u = 0; u < 2; ++u) {
-                        const uint32_t i = i0 + (uint32_t)u * blockDim.x;
-                        live[u] = i < cnt;
-                        slot[u] = off + (live[u] ? i : 0u);
-                        r0[u] = live[u] ? A.pos[slot[u]] : 0u;
-                        dg[u] = live[u] ? A.deg[slot[u]] : 0u;
-                        ok[u] = live[u];
-                    }
-#pragma unroll
-                    for (int u = 0; u < 2; ++u) {
-                        dir[u] = direction(draw_any(s.rng, seed, iter, i0 + (uint32_t)u * blockDim.x, iterHi));
-                        bool w;
-                        r1[u] = wmove(r0[u], dir[u], s, w);
-                    }
-                    const uint32_t dmax = dg[0] > dg[1] ? dg[0] : dg[1];
-                    for (uint32_t j = 0; j < dmax; ++j) {
-#pragma unroll
-                        for (int u = 0; u < 2; ++u)
-                            if (ok[u] && j < dg[u]) {
-                                const uint32_t code = zbond(A.pos[A.nbr[(size_t)j * A.T + slot[u]]], r1[u]);
-                                if ((s.forbidden[code >> 5] >> (code & 31u)) & 1u) ok[u] = false;
-                            }
-                    }
-#pragma unroll
-                    for (int u = 0; u < 2; ++u)
-                        if (ok[u]) ok[u] = !face9(lat, r0[u], dir[u], s);
-#pragma unroll
-                    for (int u = 0; u < 2; ++u)
-                        if (live[u]) {
-                            if (ok[u]) {
-                                atomicOr(tmp + (r1[u] >> 5), 1u << (r1[u] & 31u));
-                                ++myCand;
-                            }
-                            A.flags[slot[u]] = ok[u] ? (uint8_t)(dir[u] | 8) : (uint8_t)0;
-                        }
-                }
-                __syncthreads();
-
-                /* perform (.cu:1148-1190) */
-                for (uint32_t i = tid; i < cnt; i += blockDim.x) {
-                    const uint32_t slot = off + i;
-                    const uint8_t f = A.flags[slot];
-                    if (!(f & 8)) continue;
-                    const uint32_t r0 = A.pos[slot];
-                    const int dir = f & 7;
-                    if (face9(tmp, r0, dir, s)) continue;
-                    bool wrapped;
-                    const uint32_t r1 = wmove(r0, dir, s, wrapped);
-                    const uint32_t w0 = r0 >> 5, w1 = r1 >> 5;
-                    const uint32_t b0 = 1u << (r0 & 31u), b1 = 1u << (r1 & 31u);
-                    if (w0 == w1) {
-                        atomicXor(lat + w0, b0 | b1);
-                    } else {
-                        atomicXor(lat + w0, b0);
-                        atomicXor(lat + w1, b1);
-                    }
-                    A.pos[slot] = r1;
-                    if (wrapped) A.img[(size_t)(dir >> 1) * A.T + slot] += (dir & 1) ? 1 : -1;
-                    A.flags[slot] = f | 16;
-                    ++myAcc;
-                }
-                __syncthreads();
-
-                /* clear this substep's targets: the whole buffer when it is in
-                 * shared memory, the candidates' words otherwise */
-                if (tid == 0 && !(iStep + 1 == wk.steps && sub + 1 == nSp)) {
-                    s_sp = r250_next(st) % nSp;
-                    s_seed = r250_next(st);
-                }
-                if (inSmem) {
-                    uint4 *t4 = reinterpret_cast<uint4 *>(tmp);
-                    for (uint32_t w = tid; w < lw / 4; w += blockDim.x) t4[w] = make_uint4(0u, 0u, 0u, 0u);
-                } else {
-                    for (uint32_t i = tid; i < cnt; i += blockDim.x) {
-                        const uint32_t slot = off + i;
-                        const uint8_t f = A.flags[slot];
-                        if (!(f & 8)) continue;
-                        bool w;
-                        const uint32_t r1 = (f & 16) ? A.pos[slot] : wmove(A.pos[slot], f & 7, s, w);
-                        tmp[r1 >> 5] = 0u;
-                    }
-                }
-                __syncthreads();
-            }
-        }
+        advance<false>(s, st, wk, lat, tmp, inSmem, lw, tid, blockDim.x, A, s_sp, s_seed, s_att, tid == 0, myCand, myAcc);
 
         /* write back */
         atomicAdd(&s_cand, (unsigned long long)myCand);
@@ -309,6 +339,76 @@ __global__ void __launch_bounds__(kThreads, 2)
             A.counters[3 * (size_t)sid + 2] += s_acc;
         }
         __syncthreads();
+    }
+}
+
+/* Systems whose lattice is in global memory, shared by a cluster of
+ * kCluster CTAs: the cluster takes one system at a time from its own queue
+ * and splits every species slab over its CTAs; phases are separated by
+ * hardware cluster barriers (no spin wait).  The system's target lattice is
+ * the cluster's slice of the scratch. */
+constexpr int kCluster = 4;
+
+__device__ __forceinline__ uint32_t cluster_rank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cluster_index()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+    return r;
+}
+
+__global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads, 2)
+    k_batch_cl(const SysDesc *__restrict__ desc, const Work *__restrict__ work, const uint32_t *__restrict__ order,
+               uint32_t nOrder, unsigned int *next, uint32_t *clusterItem, Arrays A)
+{
+    __shared__ SysDesc s;
+    __shared__ uint32_t st[251];
+    __shared__ uint32_t s_sp, s_seed;
+    __shared__ unsigned long long s_cand, s_acc, s_att;
+    const uint32_t tid = threadIdx.x, rank = cluster_rank(), cid = cluster_index();
+    const uint32_t first = rank * blockDim.x + tid, stride = kCluster * blockDim.x;
+
+    for (;;) {
+        if (rank == 0 && tid == 0) clusterItem[cid] = atomicAdd(next, 1u);
+        cluster_barrier();
+        const uint32_t item = *reinterpret_cast<volatile const uint32_t *>(clusterItem + cid);
+        cluster_barrier(); /* every CTA has read the item before the next one is taken */
+        if (item >= nOrder) return;
+        const uint32_t sid = order[item];
+        for (uint32_t w = tid; w < (uint32_t)kDescWords; w += blockDim.x)
+            reinterpret_cast<uint32_t *>(&s)[w] = reinterpret_cast<const uint32_t *>(desc + sid)[w];
+        for (uint32_t w = tid; w < 251u; w += blockDim.x) st[w] = A.r250[(size_t)sid * 251 + w];
+        if (tid == 0) {
+            s_cand = 0;
+            s_acc = 0;
+            s_att = 0;
+        }
+        __syncthreads();
+        const uint32_t lw = s.latWords;
+        uint32_t *lat = A.latPool + s.latOff;
+        uint32_t *tmp = A.tmpScratch + (size_t)cid * A.maxLatWords;
+        for (uint32_t w = first; w < lw; w += stride) tmp[w] = 0u;
+        cluster_barrier();
+        const Work wk = work[sid];
+        unsigned int myCand = 0, myAcc = 0;
+        advance<true>(s, st, wk, lat, tmp, false, lw, first, stride, A, s_sp, s_seed, s_att, tid == 0, myCand, myAcc,
+                      rank == 0);
+        atomicAdd(&s_cand, (unsigned long long)myCand);
+        atomicAdd(&s_acc, (unsigned long long)myAcc);
+        if (rank == 0)
+            for (uint32_t w = tid; w < 251u; w += blockDim.x) A.r250[(size_t)sid * 251 + w] = st[w];
+        __syncthreads();
+        if (tid == 0) {
+            if (rank == 0) atomicAdd(A.counters + 3 * (size_t)sid + 0, s_att);
+            atomicAdd(A.counters + 3 * (size_t)sid + 1, s_cand);
+            atomicAdd(A.counters + 3 * (size_t)sid + 2, s_acc);
+        }
+        cluster_barrier();
     }
 }
 
@@ -444,6 +544,10 @@ struct Batch {
     int32_t *d_out = nullptr;
     size_t outCap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t stream2 = nullptr; /* the single-CTA kernel runs beside the cluster kernel */
+    cudaEvent_t evFork = nullptr, evJoin = nullptr;
+    uint32_t *d_clItem = nullptr;
+    bool useClusters = true;
 
     double lastMs = 0;
     uint64_t lastLaunches = 0, lastAttempts = 0;
@@ -463,7 +567,12 @@ struct Batch {
         d_cub = nullptr;
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
-        ev0 = ev1 = nullptr;
+        if (evFork) cudaEventDestroy(evFork);
+        if (evJoin) cudaEventDestroy(evJoin);
+        ev0 = ev1 = evFork = evJoin = nullptr;
+        bfree(d_clItem);
+        if (stream2) cudaStreamDestroy(stream2);
+        stream2 = nullptr;
         if (stream) cudaStreamDestroy(stream);
         stream = nullptr;
         initialized = false;
@@ -658,10 +767,13 @@ struct Batch {
         BCK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         BCK(cudaEventCreate(&ev0));
         BCK(cudaEventCreate(&ev1));
+        BCK(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking));
+        BCK(cudaEventCreateWithFlags(&evFork, cudaEventDisableTiming));
+        BCK(cudaEventCreateWithFlags(&evJoin, cudaEventDisableTiming));
         balloc(d_desc, S);
         balloc(d_work, S);
         balloc(d_order, S);
-        balloc(d_next, 1);
+        balloc(d_next, 2);
         balloc(d_pos, T); balloc(d_pos2, T);
         balloc(d_img, 3 * (size_t)T); balloc(d_img2, 3 * (size_t)T);
         balloc(d_nbr, (size_t)rows * T); balloc(d_nbr2, (size_t)rows * T);
@@ -683,6 +795,7 @@ struct Batch {
         BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, gpu));
         grid = std::max(1, perSm) * sms;
         if (maxLatWords > kSmemLatWords) balloc(d_tmp, (size_t)grid * maxLatWords);
+        balloc(d_clItem, (size_t)grid / kCluster + 1);
         size_t bytes = 0;
         BCK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, d_keys, d_keys2, d_iota, d_perm, (int)T, 0, 64, stream));
         cubBytes = bytes;
@@ -772,14 +885,36 @@ struct Batch {
             std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
                 return (uint64_t)hw[a].steps * desc[a].n > (uint64_t)hw[b].steps * desc[b].n;
             });
+            /* systems with a global-memory lattice go to the cluster kernel
+             * (first part of the order), the others to the single-CTA kernel */
+            std::vector<uint32_t> big, small;
+            for (uint32_t sI : order) ((useClusters && desc[sI].latWords > kSmemLatWords) ? big : small).push_back(sI);
+            order = big;
+            order.insert(order.end(), small.begin(), small.end());
             BCK(cudaMemcpyAsync(d_work, hw.data(), S * sizeof(Work), cudaMemcpyHostToDevice, stream));
             BCK(cudaMemcpyAsync(d_order, order.data(), order.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
-            BCK(cudaMemsetAsync(d_next, 0, sizeof(unsigned int), stream));
+            BCK(cudaMemsetAsync(d_next, 0, 2 * sizeof(unsigned int), stream));
+            BCK(cudaEventRecord(evFork, stream));
+            BCK(cudaStreamWaitEvent(stream2, evFork, 0));
             Arrays A{d_pos, d_img, d_nbr, d_deg, d_flags, T, d_lat, d_tmp, maxLatWords, d_r250, d_cnt};
-            const int g = (int)std::min<size_t>((size_t)grid, order.size());
-            k_batch<<<g, kThreads, 2 * kSmemLatWords * 4, stream>>>(d_desc, d_work, d_order, (uint32_t)order.size(), d_next, A);
-            BCK(cudaGetLastError());
-            ++lastLaunches;
+            /* the clusters (longest work) are launched first, the single-CTA
+             * kernel fills the remaining slots and those the clusters free */
+            if (!big.empty()) {
+                const size_t clusters = std::min<size_t>((size_t)grid / kCluster, big.size());
+                k_batch_cl<<<(int)(clusters * kCluster), kThreads, 0, stream>>>(d_desc, d_work, d_order, (uint32_t)big.size(),
+                                                                              d_next, d_clItem, A);
+                BCK(cudaGetLastError());
+                ++lastLaunches;
+            }
+            if (!small.empty()) {
+                const int g = (int)std::min<size_t>((size_t)grid, small.size());
+                k_batch<<<g, kThreads, 2 * kSmemLatWords * 4, stream2>>>(d_desc, d_work, d_order + big.size(),
+                                                                          (uint32_t)small.size(), d_next + 1, A);
+                BCK(cudaGetLastError());
+                ++lastLaunches;
+            }
+            BCK(cudaEventRecord(evJoin, stream2));
+            BCK(cudaStreamWaitEvent(stream, evJoin, 0));
             /* the host buffers are reused by the next round */
             BCK(cudaStreamSynchronize(stream));
             for (uint32_t sI : order) {
@@ -922,6 +1057,8 @@ int bfm_batch_add_system(bfm_batch *h, uint32_t Lx, uint32_t Ly, uint32_t Lz, ui
 }
 
 int bfm_batch_initialize(bfm_batch *h) { BGUARD(h, { h->b.initialize(); }); }
+
+int bfm_batch_set_clusters(bfm_batch *h, int on) { BGUARD(h, { h->b.useClusters = on != 0; }); }
 
 int bfm_batch_run(bfm_batch *h, const uint32_t *mcs, size_t nsys) { BGUARD(h, { h->b.run(mcs, nsys); }); }
 

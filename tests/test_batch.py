@@ -98,9 +98,11 @@ def _run_oracle(s, rng, age, sort_every, st, calls):
 
 
 @pytest.mark.gpu
-def test_batch_matches_oracle_and_single_runs():
+@pytest.mark.parametrize("clusters", [True, False])
+def test_batch_matches_oracle_and_single_runs(clusters):
+    """clusters: the 128^3 system is shared by a cluster of 4 CTAs, or run by one CTA"""
     made = [(make(), rng, age, se) for make, rng, age, se in CASES]
-    b = pb.Batch()
+    b = pb.Batch().set_clusters(clusters)
     states = [oracle.r250_state(100 + i) for i in range(len(made))]
     for (s, rng, age, se), st in zip(made, states):
         b.add(s, rng=rng, age=age, sort_every=se, r250_state=st)
