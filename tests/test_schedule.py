@@ -76,7 +76,7 @@ def test_drift_check_extends_an_underbudgeted_run():
 
 @pytest.mark.gpu
 def test_pipeline_on_a_small_ensemble():
-    rep = sch.run(n_systems=192, mcs=3000, every=100, epochs=60, seed=3)
+    rep = sch.run(n_systems=192, mcs=4000, every=100, epochs=60, seed=3)
     assert rep["systems"] == 192 and rep["batch_rate_moves_per_s"] > 1e8
     assert rep["train_loss_first_last"][1] < rep["train_loss_first_last"][0]
     assert rep["schedule"]["learned"]["cost_moves"] > 0 and rep["schedule"]["plain"]["cost_moves"] > 0
