@@ -346,20 +346,22 @@ def run(n_systems: int = 4096, mcs: int = 20000, every: int = 200, test_fraction
     # within 0.5% against the same fixed-budget rule
     train_series = [series[i] for i in tr_j]
     pred_tr = model.predict(x[tr_j])
+    # budgets scale with the predicted end-to-end autocorrelation time, the
+    # target the network predicts best
     factor, calib = 8.0, {}
-    for f in (4.0, 6.0, 8.0, 12.0, 16.0, 24.0):
-        c = compare(train_series, learned_budgets(pred_tr[:, 0], train_series, factor=f))
+    for f in (2.0, 3.0, 4.0, 6.0, 8.0, 12.0, 16.0):
+        c = compare(train_series, learned_budgets(pred_tr[:, 3], train_series, factor=f))
         calib[f] = {"bias": c["learned"]["bias_re2"], "ratio": c["systems_per_hour_ratio"]}
     ok = [f for f in calib if abs(calib[f]["bias"]) <= 0.005]
     if ok:
         factor = max(ok, key=lambda f: calib[f]["ratio"])
-    budgets = learned_budgets(pred[:, 0], test_series, factor=factor)
+    budgets = learned_budgets(pred[:, 3], test_series, factor=factor)
     cmp = compare(test_series, budgets)
     # the same schedule fed the constant (training-mean) prediction: what the network adds
-    const_budgets = learned_budgets(np.full(len(te), y[tr, 0].mean()), test_series, factor=factor)
+    const_budgets = learned_budgets(np.full(len(te), y[tr, 3].mean()), test_series, factor=factor)
     cmp_const = compare(test_series, const_budgets)
     per_hour = lambda cost: len(te) / (cost / rate) * 3600.0
-    order = admission_order(pred[:, 0], [series[i]["n"] for i in te])
+    order = admission_order(pred[:, 3], [series[i]["n"] for i in te])
     return {
         "systems": n_systems, "test_systems": int(n_te), "test_systems_judged": int(len(te)), "recorded_mcs": mcs, "snapshot_every": every,
         "ensemble": "boxes 16/24/32, linear chains or 3-arm stars of 8..48 monomers, volume fraction 0.1..0.5, Saru",
