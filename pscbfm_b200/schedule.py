@@ -5,8 +5,8 @@ own tensor-core kernels) maps a system's architecture -- monomers per
 molecule N, molecule count, volume fraction, arms, box edge, side-chain
 spacing -- to its equilibration time, equilibrium R_e^2 and R_g^2 (per
 monomer) and the end-to-end relaxation (Rouse) time.  The schedule gives
-each system an MCS budget of a few predicted equilibration times and admits
-the longest first; a measured check on every system's own R_e^2 series
+each system an MCS budget of a calibrated multiple of its predicted
+end-to-end autocorrelation time and admits the longest first; a measured check on every system's own R_e^2 series
 (the mean of the last quarter of the run against the quarter before, and
 the end-to-end autocorrelation) extends any run the prediction
 under-budgeted.  The plain schedule, and the fallback, is one fixed budget
@@ -373,6 +373,7 @@ def run(n_systems: int = 4096, mcs: int = 20000, every: int = 200, test_fraction
         "systems_per_hour": {"learned": per_hour(cmp["learned"]["cost_moves"]), "plain": per_hour(cmp["plain"]["cost_moves"])},
         "schedule_without_network": {"cost_moves": cmp_const["learned"]["cost_moves"],
                                      "mean_rel_err_re2": cmp_const["learned"]["mean_rel_err_re2"],
+                                     "bias_re2": cmp_const["learned"]["bias_re2"],
                                      "ratio_vs_plain": cmp_const["systems_per_hour_ratio"]},
         "admission_order_head": [int(te[i]) for i in order[:8]],
     }
@@ -383,8 +384,8 @@ def main(argv=None):
     import json
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--systems", type=int, default=4096)
-    ap.add_argument("--mcs", type=int, default=20000)
-    ap.add_argument("--every", type=int, default=200)
+    ap.add_argument("--mcs", type=int, default=200000)
+    ap.add_argument("--every", type=int, default=1000)
     ap.add_argument("--epochs", type=int, default=300)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--out", default=None)
