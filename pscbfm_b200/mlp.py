@@ -89,3 +89,31 @@ class MLP:
 
     def __del__(self):
         self.close()
+
+
+def main(argv=None):
+    """time training steps of the schedule network on a synthetic batch"""
+    import argparse
+    import json
+    import time
+    ap = argparse.ArgumentParser(description="train-step timing of the schedule network")
+    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--hidden", type=int, default=128)
+    ap.add_argument("--steps", type=int, default=50)
+    a = ap.parse_args(argv)
+    rng = np.random.default_rng(0)
+    x = rng.normal(size=(a.batch, 6)).astype(np.float32)
+    t = np.stack([np.sin(x[:, 0]), x[:, 1] * x[:, 2], np.cos(x[:, 3]), x[:, 4] - x[:, 5]], 1).astype(np.float32)
+    m = MLP(6, a.hidden, 4, seed=1)
+    first = m.train_step(x, t, lr=1e-3)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        last = m.train_step(x, t, lr=1e-3)
+    dt = (time.perf_counter() - t0) / a.steps
+    flops = 3 * 2 * a.batch * (6 * a.hidden + a.hidden * a.hidden + a.hidden * 4)
+    print(json.dumps({"batch": a.batch, "hidden": a.hidden, "ms_per_step": dt * 1e3, "loss_first": first, "loss_last": last,
+                      "tflops_per_s_incl_host": flops / dt / 1e12}))
+
+
+if __name__ == "__main__":
+    main()
