@@ -36,8 +36,13 @@ namespace mlp {
  * One warp per 16 x 8 tile of C. */
 __global__ void k_gemm(uint32_t M, uint32_t N, uint32_t K, const __nv_bfloat16 *__restrict__ A, uint32_t sam, uint32_t sak,
                        const __nv_bfloat16 *__restrict__ B, uint32_t sbk, uint32_t sbn, float *__restrict__ C, uint32_t ldc,
-                       int accumulate)
+                       int accumulate, uint32_t kChunk)
 {
+    /* split K: blockIdx.y takes k in [y * kChunk, (y + 1) * kChunk) and
+     * writes its partial tile to C + y * M * ldc (summed by k_sum_parts) */
+    const uint32_t kBegin = blockIdx.y * kChunk;
+    const uint32_t kEnd = kBegin + kChunk < K ? kBegin + kChunk : K;
+    C += (size_t)blockIdx.y * M * ldc;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t tilesN = (N + 7) / 8;
@@ -47,22 +52,22 @@ __global__ void k_gemm(uint32_t M, uint32_t N, uint32_t K, const __nv_bfloat16 *
     const uint32_t m0 = tm * 16 + g, m1 = m0 + 8, n = tn * 8 + g;
     float c[4] = {0.f, 0.f, 0.f, 0.f};
     const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
-    for (uint32_t k0 = 0; k0 < K; k0 += 16) {
+    for (uint32_t k0 = kBegin; k0 < kEnd; k0 += 16) {
         /* A fragment: rows g and g+8, columns 2t, 2t+1 and 2t+8, 2t+9 */
         __nv_bfloat16 a[8];
         const uint32_t ks[4] = {k0 + 2 * t, k0 + 2 * t + 1, k0 + 2 * t + 8, k0 + 2 * t + 9};
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const uint32_t k = ks[q];
-            a[(q >> 1) * 4 + (q & 1)] = (m0 < M && k < K) ? A[(size_t)m0 * sam + (size_t)k * sak] : zero;
-            a[(q >> 1) * 4 + 2 + (q & 1)] = (m1 < M && k < K) ? A[(size_t)m1 * sam + (size_t)k * sak] : zero;
+            a[(q >> 1) * 4 + (q & 1)] = (m0 < M && k < kEnd) ? A[(size_t)m0 * sam + (size_t)k * sak] : zero;
+            a[(q >> 1) * 4 + 2 + (q & 1)] = (m1 < M && k < kEnd) ? A[(size_t)m1 * sam + (size_t)k * sak] : zero;
         }
         /* B fragment: rows (k) 2t, 2t+1 and 2t+8, 2t+9, column g */
         __nv_bfloat16 b[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const uint32_t k = ks[q];
-            b[q] = (n < N && k < K) ? B[(size_t)k * sbk + (size_t)n * sbn] : zero;
+            b[q] = (n < N && k < kEnd) ? B[(size_t)k * sbk + (size_t)n * sbn] : zero;
         }
         uint32_t ra[4], rb[2];
 #pragma unroll
@@ -93,6 +98,17 @@ __global__ void k_gemm(uint32_t M, uint32_t N, uint32_t K, const __nv_bfloat16 *
             float *p = C + (size_t)mm * ldc + nn;
             *p = accumulate ? *p + c[r] : c[r];
         }
+    }
+}
+
+/* C = sum of the split-K partial tiles, in a fixed order (deterministic) */
+__global__ void k_sum_parts(uint32_t M, uint32_t N, uint32_t ldc, uint32_t parts, const float *__restrict__ P, float *__restrict__ C)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < M * N; i += gridDim.x * blockDim.x) {
+        const uint32_t m = i / N, n = i % N;
+        float v = 0.f;
+        for (uint32_t y = 0; y < parts; ++y) v += P[(size_t)y * M * ldc + (size_t)m * ldc + n];
+        C[(size_t)m * ldc + n] = v;
     }
 }
 
@@ -223,7 +239,7 @@ struct Net {
     ~Net()
     {
         if (stream) cudaStreamSynchronize(stream);
-        free_n(d_p); free_n(d_g); free_n(d_m1); free_n(d_m2); free_n(d_loss); free_n(d_pb);
+        free_n(d_p); free_n(d_g); free_n(d_m1); free_n(d_m2); free_n(d_loss); free_n(d_pb); free_n(d_parts);
         freeActs();
         if (stream) cudaStreamDestroy(stream);
     }
@@ -319,13 +335,33 @@ struct Net {
         cap = B;
     }
 
+    /* split-K scratch for products with few output tiles and a long K */
+    float *d_parts = nullptr;
+    size_t partsCap = 0;
+
     void gemm(uint32_t M, uint32_t N, uint32_t K, const __nv_bfloat16 *A, uint32_t sam, uint32_t sak, const __nv_bfloat16 *B,
               uint32_t sbk, uint32_t sbn, float *C, uint32_t ldc, bool acc)
     {
         const size_t warps = (size_t)((M + 15) / 16) * ((N + 7) / 8);
         const int threads = 128;
         const int blocks = (int)((warps * 32 + threads - 1) / threads);
-        k_gemm<<<blocks, threads, 0, stream>>>(M, N, K, A, sam, sak, B, sbk, sbn, C, ldc, acc ? 1 : 0);
+        /* fewer than ~1024 warps and a long K: split K into chunks of at
+         * least 256, partial tiles summed in order afterwards */
+        uint32_t parts = 1;
+        while (!acc && warps * parts < 1024 && K / (parts * 2) >= 256) parts *= 2;
+        if (parts == 1) {
+            k_gemm<<<blocks, threads, 0, stream>>>(M, N, K, A, sam, sak, B, sbk, sbn, C, ldc, acc ? 1 : 0, K);
+        } else {
+            const size_t need = (size_t)parts * M * ldc;
+            if (need > partsCap) {
+                free_n(d_parts);
+                malloc_n(d_parts, need);
+                partsCap = need;
+            }
+            const uint32_t chunk = ((K + parts - 1) / parts + 15) / 16 * 16;
+            k_gemm<<<dim3(blocks, parts), threads, 0, stream>>>(M, N, K, A, sam, sak, B, sbk, sbn, d_parts, ldc, 0, chunk);
+            k_sum_parts<<<blocks_for((size_t)M * N), 256, 0, stream>>>(M, N, ldc, parts, d_parts, C);
+        }
         MCK(cudaGetLastError());
     }
 
