@@ -382,8 +382,10 @@ def run_batch(args, ranks):
     b.initialize()
     t_init = time.perf_counter() - t
     S = args.mcs_per_step
+    b.set_autotune(True)          # the first warm-up launches time the cluster sizes
     for _ in range(args.warmup):
         b.run(S)
+    tuning = b.clusters()
     clocks = Clocks(gpu)
     torch.cuda.synchronize()
     ranks.barrier()
@@ -437,6 +439,7 @@ def run_batch(args, ranks):
                                f"monomers, box edges {dict(sorted(boxes.items()))}, chains or 3-arm stars of 16..512 "
                                f"monomers, volume fraction 0.1..0.5, Saru, 2 colours per system",
                    "mcs_per_step": S, "systems": len(sys_), "generate_s": t_gen, "initialize_s": t_init,
+                   "clusters": tuning,
                    "l2": "ensemble state beyond L2 (lattices and monomer arrays of all systems)"},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": len(sys_) * 16 + 4 * len(sys_),
                 "d2h_bytes_per_step": d2h // max(1, args.steps)},

@@ -161,9 +161,17 @@ int bfm_batch_add_system(bfm_batch *b, uint32_t Lx, uint32_t Ly, uint32_t Lz, ui
 /* colours, slabs, lattices and device state of every system (initialize,
  * .cu:2393-2537, per system) */
 int bfm_batch_initialize(bfm_batch *b);
-/* systems whose lattice exceeds 64^3 (padded) are shared by a cluster of 4
- * CTAs (default on); off: one CTA per system for every system */
-int bfm_batch_set_clusters(bfm_batch *b, int on);
+/* systems whose lattice exceeds 64^3 (padded) are shared by a cluster of
+ * `size` CTAs: 2, 4 (default; 1 also selects it) or 8; 0 runs every system
+ * on one CTA.  Every size gives the same trajectories. */
+int bfm_batch_set_clusters(bfm_batch *b, int size);
+/* autotuner: the next bfm_batch_run times cluster sizes 4, 2, 8 and off on
+ * four trial launches of 2 MCS each (part of the run, same trajectories) and
+ * keeps the fastest per attempted move */
+int bfm_batch_set_autotune(bfm_batch *b, int on);
+/* the cluster size in use, whether the autotuner has chosen it, and its four
+ * trial times (ns per attempted move, sizes 4, 2, 8, off; any pointer may be NULL) */
+int bfm_batch_get_clusters(const bfm_batch *b, int *size, int *tuned, double *trial_ns_per_move4);
 /* system s advances by mcs[s] Monte-Carlo steps (0 leaves it as it is); nsys
  * must equal the number of systems */
 int bfm_batch_run(bfm_batch *b, const uint32_t *mcs, size_t nsys);

@@ -60,10 +60,23 @@ class Batch:
         self._sizes.append(int(system.n))
         return sid.value
 
-    def set_clusters(self, on: bool):
-        """large systems shared by a cluster of 4 CTAs (default) or one CTA each"""
-        self._check(self._lib.bfm_batch_set_clusters(self._h, int(bool(on))))
+    def set_clusters(self, size):
+        """CTAs sharing a system whose lattice is in global memory: 2, 4
+        (default; True selects it), 8, or 0 / False for one CTA each"""
+        size = 4 if size is True else (0 if size is False else int(size))
+        self._check(self._lib.bfm_batch_set_clusters(self._h, size))
         return self
+
+    def set_autotune(self, on: bool = True):
+        """time cluster sizes 4, 2, 8 and off on the next run's first launches, keep the fastest"""
+        self._check(self._lib.bfm_batch_set_autotune(self._h, int(bool(on))))
+        return self
+
+    def clusters(self) -> dict:
+        size, tuned = ctypes.c_int(), ctypes.c_int()
+        ns = np.zeros(4, np.float64)
+        self._check(self._lib.bfm_batch_get_clusters(self._h, ctypes.byref(size), ctypes.byref(tuned), ns.ctypes.data))
+        return {"size": size.value, "tuned": bool(tuned.value), "trial_ns_per_move": dict(zip((4, 2, 8, 0), ns.tolist()))}
 
     def initialize(self):
         self._check(self._lib.bfm_batch_initialize(self._h))

@@ -345,17 +345,22 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
 }
 
-/* Systems whose lattice is in global memory, shared by a cluster of
- * kCluster CTAs: the cluster takes one system at a time from its own queue
- * and splits every species slab over its CTAs; phases are separated by
- * hardware cluster barriers (no spin wait).  The system's target lattice is
- * the cluster's slice of the scratch. */
-constexpr int kCluster = 4;
+/* Systems whose lattice is in global memory, shared by a cluster of CTAs
+ * (2, 4 or 8, chosen at launch): the cluster takes one system at a time from
+ * its own queue and splits every species slab over its CTAs; phases are
+ * separated by hardware cluster barriers (no spin wait).  The system's
+ * target lattice is the cluster's slice of the scratch. */
 
 __device__ __forceinline__ uint32_t cluster_rank()
 {
     uint32_t r;
     asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cluster_size()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
     return r;
 }
 __device__ __forceinline__ uint32_t cluster_index()
@@ -365,7 +370,7 @@ __device__ __forceinline__ uint32_t cluster_index()
     return r;
 }
 
-__global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, 2)
     k_batch_cl(const SysDesc *__restrict__ desc, const Work *__restrict__ work, const uint32_t *__restrict__ order,
                uint32_t nOrder, unsigned int *next, uint32_t *clusterItem, Arrays A)
 {
@@ -374,7 +379,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads, 2)
     __shared__ uint32_t s_sp, s_seed;
     __shared__ unsigned long long s_cand, s_acc, s_att;
     const uint32_t tid = threadIdx.x, rank = cluster_rank(), cid = cluster_index();
-    const uint32_t first = rank * blockDim.x + tid, stride = kCluster * blockDim.x;
+    const uint32_t first = rank * blockDim.x + tid, stride = cluster_size() * blockDim.x;
 
     for (;;) {
         if (rank == 0 && tid == 0) clusterItem[cid] = atomicAdd(next, 1u);
@@ -548,9 +553,12 @@ struct Batch {
     size_t outCap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaStream_t stream2 = nullptr; /* the single-CTA kernel runs beside the cluster kernel */
-    cudaEvent_t evFork = nullptr, evJoin = nullptr;
+    cudaEvent_t evFork = nullptr, evJoin = nullptr, evT0 = nullptr, evT1 = nullptr;
     uint32_t *d_clItem = nullptr;
-    bool useClusters = true;
+    int clusterSize = 4;     /* CTAs per system with a global-memory lattice; 0: one CTA */
+    bool autotune = false;   /* time each cluster size on the first launches of a run, keep the fastest */
+    bool tuned = false;
+    std::vector<double> trialNsPerMove; /* per candidate of the autotuner */
 
     double lastMs = 0;
     uint64_t lastLaunches = 0, lastAttempts = 0;
@@ -572,7 +580,9 @@ struct Batch {
         if (ev1) cudaEventDestroy(ev1);
         if (evFork) cudaEventDestroy(evFork);
         if (evJoin) cudaEventDestroy(evJoin);
-        ev0 = ev1 = evFork = evJoin = nullptr;
+        if (evT0) cudaEventDestroy(evT0);
+        if (evT1) cudaEventDestroy(evT1);
+        ev0 = ev1 = evFork = evJoin = evT0 = evT1 = nullptr;
         bfree(d_clItem);
         if (stream2) cudaStreamDestroy(stream2);
         stream2 = nullptr;
@@ -773,6 +783,8 @@ struct Batch {
         BCK(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking));
         BCK(cudaEventCreateWithFlags(&evFork, cudaEventDisableTiming));
         BCK(cudaEventCreateWithFlags(&evJoin, cudaEventDisableTiming));
+        BCK(cudaEventCreate(&evT0));
+        BCK(cudaEventCreate(&evT1));
         balloc(d_desc, S);
         balloc(d_work, S);
         balloc(d_order, S);
@@ -798,7 +810,7 @@ struct Batch {
         BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, gpu));
         grid = std::max(1, perSm) * sms;
         if (maxLatWords > kSmemLatWords) balloc(d_tmp, (size_t)grid * maxLatWords);
-        balloc(d_clItem, (size_t)grid / kCluster + 1);
+        balloc(d_clItem, (size_t)grid / 2 + 1);
         size_t bytes = 0;
         BCK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, d_keys, d_keys2, d_iota, d_perm, (int)T, 0, 64, stream));
         cubBytes = bytes;
@@ -855,6 +867,27 @@ struct Batch {
         std::swap(d_s2o, d_s2o2);
     }
 
+    /* clusters of cs CTAs of k_batch_cl that can be resident at once (0: none) */
+    int activeClusters(int cs)
+    {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)cs);
+        cfg.blockDim = dim3(kThreads);
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = (unsigned)cs;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, k_batch_cl, &cfg) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return 0;
+        }
+        return n;
+    }
+
     /* every system advances by mcs[s] MCS */
     void run(const uint32_t *mcs, size_t count)
     {
@@ -867,8 +900,23 @@ struct Batch {
         std::vector<uint32_t> order;
         lastLaunches = 0;
         lastAttempts = 0;
+        /* the autotuner's candidates; only systems with a global-memory
+         * lattice are affected, and every choice gives the same trajectory */
+        static const int kCand[4] = {4, 2, 8, 0};
+        bool anyBig = false;
+        for (const SysDesc &d : desc) anyBig |= d.latWords > kSmemLatWords;
+        if (autotune && !tuned && !anyBig) tuned = true;
+        size_t trial = autotune && !tuned ? trialNsPerMove.size() : 4;
         BCK(cudaEventRecord(ev0, stream));
         for (;;) {
+            const bool trying = trial < 4;
+            int cs = trying ? kCand[trial] : clusterSize;
+            bool unlaunchable = false;
+            if (cs > 0 && activeClusters(cs) == 0) {
+                if (!trying) throw Err("clusters of " + std::to_string(cs) + " CTAs cannot be launched on this GPU");
+                unlaunchable = true; /* the trial runs on single CTAs and is not chosen */
+                cs = 0;
+            }
             /* re-sort every system that starts an MCS at a sorting point (.cu:3005) */
             std::vector<uint8_t> due(S, 0);
             order.clear();
@@ -879,7 +927,7 @@ struct Batch {
                 if (!left[sI]) continue;
                 due[sI] = age[sI] % sortEvery[sI] == 0;
                 const uint64_t toNext = (uint64_t)(sortEvery[sI] - age[sI] % sortEvery[sI]);
-                hw[sI].steps = (uint32_t)std::min<uint64_t>(left[sI], std::min<uint64_t>(toNext, 0xFFFFFFFFull));
+                hw[sI].steps = (uint32_t)std::min<uint64_t>(left[sI], std::min<uint64_t>(toNext, trying ? 2ull : 0xFFFFFFFFull));
                 order.push_back((uint32_t)sI);
             }
             if (order.empty()) break;
@@ -891,22 +939,34 @@ struct Batch {
             /* systems with a global-memory lattice go to the cluster kernel
              * (first part of the order), the others to the single-CTA kernel */
             std::vector<uint32_t> big, small;
-            for (uint32_t sI : order) ((useClusters && desc[sI].latWords > kSmemLatWords) ? big : small).push_back(sI);
+            for (uint32_t sI : order) ((cs > 0 && desc[sI].latWords > kSmemLatWords) ? big : small).push_back(sI);
             order = big;
             order.insert(order.end(), small.begin(), small.end());
             BCK(cudaMemcpyAsync(d_work, hw.data(), S * sizeof(Work), cudaMemcpyHostToDevice, stream));
             BCK(cudaMemcpyAsync(d_order, order.data(), order.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
             BCK(cudaMemsetAsync(d_next, 0, 2 * sizeof(unsigned int), stream));
+            BCK(cudaEventRecord(evT0, stream));
             BCK(cudaEventRecord(evFork, stream));
             BCK(cudaStreamWaitEvent(stream2, evFork, 0));
             Arrays A{d_pos, d_img, d_nbr, d_deg, d_flags, T, d_lat, d_tmp, maxLatWords, d_r250, d_cnt};
             /* the clusters (longest work) are launched first, the single-CTA
              * kernel fills the remaining slots and those the clusters free */
             if (!big.empty()) {
-                const size_t clusters = std::max<size_t>(1, std::min<size_t>((size_t)grid / kCluster, big.size()));
-                k_batch_cl<<<(int)(clusters * kCluster), kThreads, 0, stream>>>(d_desc, d_work, d_order, (uint32_t)big.size(),
-                                                                              d_next, d_clItem, A);
-                BCK(cudaGetLastError());
+                const size_t clusters = std::max<size_t>(1, std::min<size_t>((size_t)grid / (size_t)cs, big.size()));
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3((unsigned)(clusters * (size_t)cs));
+                cfg.blockDim = dim3(kThreads);
+                cfg.dynamicSmemBytes = 0;
+                cfg.stream = stream;
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeClusterDimension;
+                attr[0].val.clusterDim.x = (unsigned)cs;
+                attr[0].val.clusterDim.y = 1;
+                attr[0].val.clusterDim.z = 1;
+                cfg.attrs = attr;
+                cfg.numAttrs = 1;
+                BCK(cudaLaunchKernelEx(&cfg, k_batch_cl, (const SysDesc *)d_desc, (const Work *)d_work, (const uint32_t *)d_order,
+                                       (uint32_t)big.size(), d_next, d_clItem, A));
                 ++lastLaunches;
             }
             if (!small.empty()) {
@@ -918,8 +978,23 @@ struct Batch {
             }
             BCK(cudaEventRecord(evJoin, stream2));
             BCK(cudaStreamWaitEvent(stream, evJoin, 0));
+            BCK(cudaEventRecord(evT1, stream));
             /* the host buffers are reused by the next round */
             BCK(cudaStreamSynchronize(stream));
+            uint64_t moves = 0;
+            for (uint32_t sI : order) moves += (uint64_t)hw[sI].steps * desc[sI].n;
+            if (trying) {
+                float tms = 0;
+                BCK(cudaEventElapsedTime(&tms, evT0, evT1));
+                trialNsPerMove.push_back(unlaunchable ? 1e30 : (moves ? tms * 1e6 / (double)moves : 0.0));
+                if (++trial == 4) {
+                    size_t best = 0;
+                    for (size_t c = 1; c < 4; ++c)
+                        if (trialNsPerMove[c] < trialNsPerMove[best]) best = c;
+                    clusterSize = kCand[best];
+                    tuned = true;
+                }
+            }
             for (uint32_t sI : order) {
                 lastAttempts += (uint64_t)hw[sI].steps * desc[sI].n;
                 age[sI] += hw[sI].steps;
@@ -1061,7 +1136,34 @@ int bfm_batch_add_system(bfm_batch *h, uint32_t Lx, uint32_t Ly, uint32_t Lz, ui
 
 int bfm_batch_initialize(bfm_batch *h) { BGUARD(h, { h->b.initialize(); }); }
 
-int bfm_batch_set_clusters(bfm_batch *h, int on) { BGUARD(h, { h->b.useClusters = on != 0; }); }
+int bfm_batch_set_clusters(bfm_batch *h, int size)
+{
+    BGUARD(h, {
+        if (size != 0 && size != 1 && size != 2 && size != 4 && size != 8)
+            throw bfm::ens::ArgErr("cluster size must be 0 (off), 1 (default, 4), 2, 4 or 8");
+        h->b.clusterSize = size == 1 ? 4 : size;
+        h->b.autotune = false;
+    });
+}
+
+int bfm_batch_set_autotune(bfm_batch *h, int on)
+{
+    BGUARD(h, {
+        h->b.autotune = on != 0;
+        h->b.tuned = false;
+        h->b.trialNsPerMove.clear();
+    });
+}
+
+int bfm_batch_get_clusters(const bfm_batch *h, int *size, int *tuned, double *trial_ns_per_move4)
+{
+    if (!h) return BFM_EINVAL;
+    if (size) *size = h->b.clusterSize;
+    if (tuned) *tuned = h->b.tuned ? 1 : 0;
+    if (trial_ns_per_move4)
+        for (size_t c = 0; c < 4; ++c) trial_ns_per_move4[c] = c < h->b.trialNsPerMove.size() ? h->b.trialNsPerMove[c] : 0.0;
+    return BFM_OK;
+}
 
 int bfm_batch_run(bfm_batch *h, const uint32_t *mcs, size_t nsys) { BGUARD(h, { h->b.run(mcs, nsys); }); }
 

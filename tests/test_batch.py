@@ -76,6 +76,9 @@ def test_batch_argument_checks_without_a_gpu():
         b.add(s, r250_state=np.zeros(10, np.uint32))
     assert b.add(s) == 0 and b.add(s, rng=pb.Rng.IntHash) == 1
     assert b.info()["systems"] == 2
+    with pytest.raises(ValueError):
+        b.set_clusters(3)
+    assert b.set_clusters(8).clusters()["size"] == 8
 
 
 CASES = [
@@ -98,11 +101,17 @@ def _run_oracle(s, rng, age, sort_every, st, calls):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("clusters", [True, False])
+@pytest.mark.parametrize("clusters", [4, 0, 2, 8, "auto"])
 def test_batch_matches_oracle_and_single_runs(clusters):
-    """clusters: the 128^3 system is shared by a cluster of 4 CTAs, or run by one CTA"""
+    """the 128^3 system shared by a cluster of 4, 2 or 8 CTAs, run by one CTA,
+    or by the size the autotuner picks after timing all four on the first
+    launches of the run: the trajectories are the same"""
     made = [(make(), rng, age, se) for make, rng, age, se in CASES]
-    b = pb.Batch().set_clusters(clusters)
+    b = pb.Batch()
+    if clusters == "auto":
+        b.set_autotune(True)
+    else:
+        b.set_clusters(clusters)
     states = [oracle.r250_state(100 + i) for i in range(len(made))]
     for (s, rng, age, se), st in zip(made, states):
         b.add(s, rng=rng, age=age, sort_every=se, r250_state=st)
@@ -127,6 +136,12 @@ def test_batch_matches_oracle_and_single_runs(clusters):
             if m[i]:
                 u.runSimulationOnGPU(int(m[i]))
         assert np.array_equal(u.getAllMonomerPositions(), b.positions(i)), f"system {i}"
+    info = b.clusters()
+    if clusters == "auto":
+        assert info["tuned"] and info["size"] in (0, 2, 4, 8)
+        assert all(v > 0 for v in info["trial_ns_per_move"].values())
+    else:
+        assert info["size"] == clusters
 
 
 @pytest.mark.gpu
