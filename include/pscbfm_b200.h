@@ -166,8 +166,9 @@ int bfm_batch_initialize(bfm_batch *b);
  * on one CTA.  Every size gives the same trajectories. */
 int bfm_batch_set_clusters(bfm_batch *b, int size);
 /* autotuner: the next bfm_batch_run times cluster sizes 4, 2, 8 and off on
- * four trial launches of 2 MCS each (part of the run, same trajectories) and
- * keeps the fastest per attempted move */
+ * four trial launches (each an eighth of the longest pending work, 2 .. 50
+ * MCS; part of the run, same trajectories) and keeps the fastest per
+ * attempted move; the default 4 stays unless another is more than 3% faster */
 int bfm_batch_set_autotune(bfm_batch *b, int on);
 /* the cluster size in use, whether the autotuner has chosen it, and its four
  * trial times (ns per attempted move, sizes 4, 2, 8, off; any pointer may be NULL) */

@@ -917,6 +917,16 @@ struct Batch {
                 unlaunchable = true; /* the trial runs on single CTAs and is not chosen */
                 cs = 0;
             }
+            /* a trial launch runs an eighth of the longest pending work
+             * (2 .. 50 MCS) so that its timing represents a full launch */
+            uint64_t trialSteps = 2;
+            if (trying) {
+                uint64_t most = 0;
+                for (size_t sI = 0; sI < S; ++sI)
+                    if (left[sI])
+                        most = std::max<uint64_t>(most, std::min<uint64_t>(left[sI], (uint64_t)(sortEvery[sI] - age[sI] % sortEvery[sI])));
+                trialSteps = std::min<uint64_t>(50, std::max<uint64_t>(2, most / 8));
+            }
             /* re-sort every system that starts an MCS at a sorting point (.cu:3005) */
             std::vector<uint8_t> due(S, 0);
             order.clear();
@@ -927,7 +937,7 @@ struct Batch {
                 if (!left[sI]) continue;
                 due[sI] = age[sI] % sortEvery[sI] == 0;
                 const uint64_t toNext = (uint64_t)(sortEvery[sI] - age[sI] % sortEvery[sI]);
-                hw[sI].steps = (uint32_t)std::min<uint64_t>(left[sI], std::min<uint64_t>(toNext, trying ? 2ull : 0xFFFFFFFFull));
+                hw[sI].steps = (uint32_t)std::min<uint64_t>(left[sI], std::min<uint64_t>(toNext, trying ? trialSteps : 0xFFFFFFFFull));
                 order.push_back((uint32_t)sI);
             }
             if (order.empty()) break;
@@ -988,9 +998,10 @@ struct Batch {
                 BCK(cudaEventElapsedTime(&tms, evT0, evT1));
                 trialNsPerMove.push_back(unlaunchable ? 1e30 : (moves ? tms * 1e6 / (double)moves : 0.0));
                 if (++trial == 4) {
+                    /* the default (4) stays unless another size is more than 3% faster */
                     size_t best = 0;
                     for (size_t c = 1; c < 4; ++c)
-                        if (trialNsPerMove[c] < trialNsPerMove[best]) best = c;
+                        if (trialNsPerMove[c] < 0.97 * trialNsPerMove[best]) best = c;
                     clusterSize = kCand[best];
                     tuned = true;
                 }
