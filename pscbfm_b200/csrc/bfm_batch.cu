@@ -601,6 +601,8 @@ struct Batch {
         if (rng != BFM_RNG_INTHASH && rng != BFM_RNG_SARU && rng != BFM_RNG_PHILOX)
             throw ArgErr("random number generator must be IntHash (1), Saru (2) or Philox (3)");
         if (a < 0 || sortEv <= 0) throw ArgErr("age must be >= 0 and the sorting interval > 0");
+        for (uint32_t i = 0; i < n; ++i)
+            if (deg[i] > 8) throw ArgErr("at most 8 bonds per monomer (monomer " + std::to_string(i) + ")");
         Pending p;
         std::memcpy(p.L, L, sizeof(p.L));
         p.n = n;

@@ -72,6 +72,10 @@ def test_batch_argument_checks_without_a_gpu():
         b.add(systems.System((20, 32, 32), s.pos, s.deg, s.nbr), rng=pb.Rng.Saru)   # not a multiple of 8
     with pytest.raises(ValueError):
         b.add(s, rng=pb.Rng.Pcg)
+    bad = systems.System(s.box, s.pos, s.deg.copy(), s.nbr, s.allowed)
+    bad.deg[0] = 9
+    with pytest.raises(ValueError, match="8 bonds"):
+        b.add(bad)
     with pytest.raises(ValueError):
         b.add(s, r250_state=np.zeros(10, np.uint32))
     assert b.add(s) == 0 and b.add(s, rng=pb.Rng.IntHash) == 1
