@@ -103,7 +103,9 @@ int bfm_analyzer_init(bfm_handle *h, uint32_t *n_chains);
  * time origin (first, middle, last monomer, chain centre of mass -- each
  * minus the box centre-of-mass drift when there is more than one chain --
  * and middle monomer minus chain centre of mass; AnalyzerMsd.tpp:392-421;
- * zero before an origin is set), out[8..10] the box centre of mass.
+ * zero before an origin is set), out[8..10] the box centre of mass, and
+ * with n_out >= 12 out[11] the end-to-end vector autocorrelation against the
+ * origin, sum_c R_c(t).R_c(0) / sum_c |R_c(0)|^2 (0 before an origin).
  * set_origin != 0 makes the current state the time origin afterwards. */
 int bfm_analyze(bfm_handle *h, int set_origin, double *out, size_t n_out);
 /* original monomer ids of every chain's first end, middle and last end */

@@ -364,10 +364,14 @@ def chain_observables(pos, first, middle, last, members, origin=None):
     box = com.mean(axis=0)
     vals = [p[first], p[middle], p[last], com, p[middle] - com]
     g = [0.0] * 5
+    ac = 0.0
     if origin is not None:
+        r0 = origin["vals"][2] - origin["vals"][0]
+        den = float((r0 * r0).sum())
+        ac = float(((p[last] - p[first]) * r0).sum() / den) if den > 0 else 0.0
         drift = box - origin["box"] if len(members) > 1 else np.zeros(3)
         for k in range(5):
             d = vals[k] - origin["vals"][k] - (drift if k < 4 else 0.0)
             g[k] = float((d * d).sum(axis=1).mean())
     return {"re2": float(re2.mean()), "rg2": float(rg2.mean()), "re2_chain": re2, "rg2_chain": rg2,
-            "com": com, "box": box, "vals": vals, "g": g}
+            "com": com, "box": box, "vals": vals, "g": g, "end_autocorr": ac}

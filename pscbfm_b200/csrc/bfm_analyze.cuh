@@ -142,7 +142,7 @@ __device__ __forceinline__ double block_sum(double v, double *red)
 }
 
 /* One block of kAnalyzeThreads.  out: [chains, <R_e^2>, <R_g^2>, g1..g5,
- * box COM x, y, z]; per-chain R_e^2, R_g^2 and centre of mass; with
+ * box COM x, y, z, end-to-end autocorrelation]; per-chain R_e^2, R_g^2 and centre of mass; with
  * setOrigin the current values become the time origin. */
 __global__ void __launch_bounds__(kAnalyzeThreads)
     k_chain_observables(const int32_t *__restrict__ xyz, const ChainSums *__restrict__ sums, const uint32_t *__restrict__ off,
@@ -182,6 +182,7 @@ __global__ void __launch_bounds__(kAnalyzeThreads)
 
     /* pass 2: mean-square displacements against the origin */
     double gs[5] = {0, 0, 0, 0, 0};
+    double acNum = 0, acDen = 0; /* end-to-end vector autocorrelation against the origin */
     if (haveOrigin) {
         const double dbx = nchains > 1 ? bx - boxOrigin[0] : 0.0;
         const double dby = nchains > 1 ? by - boxOrigin[1] : 0.0;
@@ -196,6 +197,11 @@ __global__ void __launch_bounds__(kAnalyzeThreads)
                 now[3][d] = com[3 * (size_t)c + d];
                 now[4][d] = now[1][d] - now[3][d];
             }
+            for (int d = 0; d < 3; ++d) {
+                const double r0 = o.p[2][d] - o.p[0][d];
+                acNum += (now[2][d] - now[0][d]) * r0;
+                acDen += r0 * r0;
+            }
             const double drift[3] = {dbx, dby, dbz};
             for (int k = 0; k < 5; ++k) {
                 double q = 0;
@@ -208,6 +214,8 @@ __global__ void __launch_bounds__(kAnalyzeThreads)
         }
     }
     for (int k = 0; k < 5; ++k) gs[k] = block_sum(gs[k], red) * inv;
+    acNum = block_sum(acNum, red);
+    acDen = block_sum(acDen, red);
 
     if (setOrigin) {
         for (uint32_t c = threadIdx.x; c < nchains; c += kAnalyzeThreads) {
@@ -235,6 +243,7 @@ __global__ void __launch_bounds__(kAnalyzeThreads)
         out[8] = bx;
         out[9] = by;
         out[10] = bz;
+        out[11] = acDen > 0.0 ? acNum / acDen : 0.0;
     }
 }
 

@@ -1971,7 +1971,7 @@ struct Engine {
         k_chain_observables<<<1, kAnalyzeThreads, 0, stream>>>(d_out, d_csum, d_coff, d_cfirst, d_cmid, d_clast, nc, d_corg, d_cbox,
                                                                haveOrigin ? 1 : 0, setOrigin ? 1 : 0, d_cre2, d_crg2, d_ccom, d_cout);
         CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(out, d_cout, 11 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(out, d_cout, 12 * sizeof(double), cudaMemcpyDeviceToHost, stream));
         CK(cudaStreamSynchronize(stream));
         if (setOrigin) haveOrigin = true;
     }
@@ -2340,10 +2340,10 @@ int bfm_analyze(bfm_handle *h, int set_origin, double *out, size_t n_out)
         return BFM_ENOTINIT;
     }
     GUARD(h, {
-        if (!out || n_out < 11) throw InvalidArgument("bfm_analyze needs an output array of 11 doubles");
-        double tmp[11];
+        if (!out || n_out < 11) throw InvalidArgument("bfm_analyze needs an output array of at least 11 doubles");
+        double tmp[12];
         h->e.analyze(tmp, set_origin != 0);
-        std::memcpy(out, tmp, sizeof(tmp));
+        std::memcpy(out, tmp, (n_out < 12 ? 11 : 12) * sizeof(double));
     });
 }
 

@@ -228,12 +228,13 @@ class UpdaterGPUScBFM_AB_Type:
     def analyze(self, set_origin: bool = False) -> dict:
         """Chain observables of the current state, computed on the GPU:
         <R_e^2>, <R_g^2>, g1..g5 against the time origin (zero before one is
-        set) and the box centre of mass.  set_origin makes the current state
-        the origin of later calls."""
-        out = np.zeros(11, dtype=np.float64)
+        set), the box centre of mass and the end-to-end vector
+        autocorrelation against the origin.  set_origin makes the current
+        state the origin of later calls."""
+        out = np.zeros(12, dtype=np.float64)
         self._check(self._lib.bfm_analyze(self._h, int(bool(set_origin)), out.ctypes.data, out.size))
         return {"chains": int(out[0]), "re2": float(out[1]), "rg2": float(out[2]),
-                "g": [float(v) for v in out[3:8]], "box_com": out[8:11].copy()}
+                "g": [float(v) for v in out[3:8]], "box_com": out[8:11].copy(), "end_autocorr": float(out[11])}
 
     def analyzerChainIds(self):
         nc = self._nchains

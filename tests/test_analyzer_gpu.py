@@ -53,6 +53,7 @@ def _check(obs, ref, u, rel_means=1e-9):
     np.testing.assert_allclose(obs["box_com"], ref["box"], rtol=1e-12, atol=1e-9)
     for a, b in zip(obs["g"], ref["g"]):
         assert a == pytest.approx(b, rel=rel_means, abs=1e-9)
+    assert obs["end_autocorr"] == pytest.approx(ref["end_autocorr"], rel=1e-9, abs=1e-12)
 
 
 @pytest.mark.parametrize("name", list(CASES))
