@@ -6,8 +6,11 @@ molecule bookkeeping of the ensemble generator, and the schedule
 comparison: with exact predictions of spread equilibration times the
 learned budgets cost less than the smallest fixed budget of equal R_e^2
 error, and a too-small prediction is extended by the measured drift check.
-GPU: the whole pipeline on a small ensemble (record with the batched
-simulator, train the network with the library's kernels, compare)."""
+GPU: the whole pipeline on a 1024-system ensemble (record with the batched
+simulator, train the network with the library's kernels, compare), and
+that the network predicts the end-to-end autocorrelation time, which the
+budgets scale with, better than a constant does (the pipeline is
+deterministic: bit-exact simulation, fixed-order sums in training)."""
 import math
 
 import numpy as np
@@ -75,9 +78,13 @@ def test_drift_check_extends_an_underbudgeted_run():
 
 
 @pytest.mark.gpu
-def test_pipeline_on_a_small_ensemble():
-    rep = sch.run(n_systems=192, mcs=4000, every=100, epochs=60, seed=3)
-    assert rep["systems"] == 192 and rep["batch_rate_moves_per_s"] > 1e8
+def test_pipeline_and_what_the_network_adds():
+    rep = sch.run(n_systems=1024, mcs=20000, every=250, epochs=200, seed=3)
+    assert rep["systems"] == 1024 and rep["batch_rate_moves_per_s"] > 1e8
     assert rep["train_loss_first_last"][1] < rep["train_loss_first_last"][0]
     assert rep["schedule"]["learned"]["cost_moves"] > 0 and rep["schedule"]["plain"]["cost_moves"] > 0
     assert all(np.isfinite(v) for v in rep["test_rmse"].values())
+    # what the network adds: its prediction of the end-to-end autocorrelation
+    # time (the quantity the budgets scale with) beats the constant predictor
+    key = "log10 end-to-end autocorrelation MCS"
+    assert rep["test_rmse"][key] < rep["test_rmse_constant_predictor"][key]
