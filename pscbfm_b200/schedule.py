@@ -332,11 +332,11 @@ def run(n_systems: int = 4096, mcs: int = 20000, every: int = 200, test_fraction
     rmse = np.sqrt(((pred - y[te]) ** 2).mean(0))
     rmse_const = np.sqrt(((y[tr].mean(0) - y[te]) ** 2).mean(0))
     # systems whose fitted relaxation time exceeds a twelfth of the recorded
-    # window cannot be judged by it (neither schedule equilibrates them in
+    # window cannot be assessed by it (neither schedule equilibrates them in
     # the record); they are left out of the schedule comparison
-    judge = y[:, 0] <= math.log10(mcs / 12.0)
-    if judge[te].any() and judge[tr].any():
-        te, tr_j = te[judge[te]], tr[judge[tr]]
+    assessable = y[:, 0] <= math.log10(mcs / 12.0)
+    if assessable[te].any() and assessable[tr].any():
+        te, tr_j = te[assessable[te]], tr[assessable[tr]]
     else:
         tr_j = tr
     pred = model.predict(x[te])
@@ -363,7 +363,7 @@ def run(n_systems: int = 4096, mcs: int = 20000, every: int = 200, test_fraction
     per_hour = lambda cost: len(te) / (cost / rate) * 3600.0
     order = admission_order(pred[:, 3], [series[i]["n"] for i in te])
     return {
-        "systems": n_systems, "test_systems": int(n_te), "test_systems_judged": int(len(te)), "recorded_mcs": mcs, "snapshot_every": every,
+        "systems": n_systems, "test_systems": int(n_te), "test_systems_assessed": int(len(te)), "recorded_mcs": mcs, "snapshot_every": every,
         "ensemble": "boxes 16/24/32, linear chains or 3-arm stars of 8..48 monomers, volume fraction 0.1..0.5, Saru",
         "batch_rate_moves_per_s": rate, "record_s": t_rec, "fit_s": t_fit,
         "train_loss_first_last": [hist[0], hist[-1]],
