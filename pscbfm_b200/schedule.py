@@ -3,14 +3,14 @@
 A small network (pscbfm_b200.mlp.MLP, trained on the GPU by the library's
 own tensor-core kernels) maps a system's architecture -- monomers per
 molecule N, molecule count, volume fraction, arms, box edge, side-chain
-spacing -- to its equilibration time, equilibrium R_e^2 and R_g^2 (per
-monomer) and the end-to-end relaxation (Rouse) time.  The schedule gives
+spacing -- to the relaxation time of R_e^2, equilibrium R_e^2 and R_g^2
+(per monomer) and the end-to-end autocorrelation time.  The schedule gives
 each system an MCS budget of a calibrated multiple of its predicted
 end-to-end autocorrelation time and admits the longest first; a measured
 check on every system's own R_e^2 series (a straight-line fit over the
 second half of the run: a significant change of more than 2% means drift)
-extends any run the prediction under-budgeted.  The plain schedule, and the fallback, is one fixed budget
-for every system.
+extends any run the prediction under-budgeted.  The plain schedule, and
+the fallback, is one fixed budget for every system.
 
 The MC arithmetic is never touched: budgets only decide how long each
 system runs.  Training data come from the batched simulator itself.
