@@ -88,3 +88,44 @@ def test_pipeline_and_what_the_network_adds():
     # time (the quantity the budgets scale with) beats the constant predictor
     key = "log10 end-to-end autocorrelation MCS"
     assert rep["test_rmse"][key] < rep["test_rmse_constant_predictor"][key]
+
+
+def test_driver_logic_with_a_synthetic_record(monkeypatch):
+    """schedule.run end to end on the CPU: the batched recorder is replaced by
+    synthetic series whose relaxation grows with N, the network by a
+    least-squares stand-in; checks the report's structure and that budgets,
+    calibration and comparison run."""
+    def fake_record(params, total_mcs, every, seed=0, gpu=0, max_vectors=32):
+        rng = np.random.default_rng(seed)
+        t = np.arange(total_mcs // every + 1) * float(every)
+        out = []
+        for p in params:
+            tau = 20.0 * p["n"] ** 1.5
+            re2 = p["n"] * 3.0 * (1 + 0.5 * np.exp(-t / tau)) * (1 + 0.01 * rng.normal(size=t.size))
+            a = math.exp(-every / tau)
+            e = np.zeros((t.size, 8, 3), np.float32)
+            e[0] = rng.normal(size=(8, 3))
+            for k in range(1, t.size):
+                e[k] = a * e[k - 1] + math.sqrt(1 - a * a) * rng.normal(size=(8, 3))
+            out.append({"t": t, "re2": re2, "rg2": re2 / 6, "ends": e, "n": 500, "mol": {"count": 20}})
+        return out, None, 1e10
+
+    class Stand:
+        def __init__(self, *a, **k):
+            pass
+
+        def fit(self, x, y, epochs=1, **k):
+            X = np.c_[x, np.ones(len(x))]
+            self.w, *_ = np.linalg.lstsq(X, y, rcond=None)
+            return [1.0, 0.5]
+
+        def predict(self, x):
+            return np.c_[x, np.ones(len(x))] @ self.w
+
+    monkeypatch.setattr(sch, "record", fake_record)
+    monkeypatch.setattr(sch, "Surrogate", Stand)
+    rep = sch.run(n_systems=96, mcs=20000, every=200, epochs=1, seed=2)
+    assert rep["systems"] == 96 and rep["test_systems"] == 24 and rep["test_systems_assessed"] >= 1
+    assert rep["schedule"]["learned"]["cost_moves"] > 0 and rep["schedule"]["plain"]["cost_moves"] > 0
+    assert rep["budget_factor"] in (2.0, 3.0, 4.0, 6.0, 8.0, 12.0, 16.0)
+    assert set(rep["test_rmse"]) == set(sch.TARGETS)
