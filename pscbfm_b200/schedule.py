@@ -28,8 +28,9 @@ TARGETS = ("log10 R_e^2 relaxation MCS", "R_e^2 / N", "R_g^2 / N", "log10 end-to
 # ----------------------------------------------------------- molecules
 def molecules(system, n_per_molecule: int, star: bool):
     """index arrays of the ensemble generator's molecules (contiguous ids):
-    linear: (first, last, members); star: (core, tips, members)"""
-    n = system.n
+    linear: (first, last, members); star: (core, tips, members).  Side
+    chains (attribute 2, ids after every backbone) are not part of them."""
+    n = system.n if system.attributes is None else int(np.count_nonzero(np.asarray(system.attributes) == 1))
     if not star:
         size = n_per_molecule
         m = n // size
@@ -150,7 +151,10 @@ def ensemble_params(n_systems: int, seed: int, boxes=(16, 24, 32), n_range=(8, 4
         star = bool(rng.random() < 0.5)
         if star:
             n = 1 + 3 * max(1, (n - 1) // 3)
-        out.append({"L": L, "n": n, "phi": float(rng.uniform(*phi_range)), "star": star, "side_every": 0})
+        side_every = int(rng.choice((0, 0, 4, 8)))
+        side_len = int(rng.integers(2, 5)) if side_every else 0
+        out.append({"L": L, "n": n, "phi": float(rng.uniform(*phi_range)), "star": star, "side_every": side_every,
+                    "side_len": side_len})
     return out
 
 
@@ -161,7 +165,8 @@ def record(params, total_mcs: int, every: int, seed: int = 0, gpu: int = 0, max_
     from . import systems as gen
     from .batch import Batch
     from .updater import Rng
-    sys_ = [gen.ensemble_system(p["L"], p["n"], p["phi"], p["star"], seed=seed + i) for i, p in enumerate(params)]
+    sys_ = [gen.ensemble_system(p["L"], p["n"], p["phi"], p["star"], seed=seed + i, side_every=p.get("side_every", 0),
+                                side_len=p.get("side_len", 0)) for i, p in enumerate(params)]
     mols = [molecules(s, p["n"], p["star"]) for s, p in zip(sys_, params)]
     b = Batch(gpu)
     for i, s in enumerate(sys_):
@@ -364,7 +369,8 @@ def run(n_systems: int = 4096, mcs: int = 20000, every: int = 200, test_fraction
     order = admission_order(pred[:, 3], [series[i]["n"] for i in te])
     return {
         "systems": n_systems, "test_systems": int(n_te), "test_systems_assessed": int(len(te)), "recorded_mcs": mcs, "snapshot_every": every,
-        "ensemble": "boxes 16/24/32, linear chains or 3-arm stars of 8..48 monomers, volume fraction 0.1..0.5, Saru",
+        "ensemble": "boxes 16/24/32, linear chains or 3-arm stars of 8..48 backbone monomers, half of them combs (a side "
+                    "chain of 2..4 on every 4th or 8th backbone monomer), volume fraction 0.1..0.5, Saru",
         "batch_rate_moves_per_s": rate, "record_s": t_rec, "fit_s": t_fit,
         "train_loss_first_last": [hist[0], hist[-1]],
         "test_rmse": dict(zip(TARGETS, map(float, rmse))),

@@ -419,18 +419,65 @@ def _topology_from_bonds(n, bonds):
     return deg, nbr
 
 
-def ensemble_system(L: int, n_per_molecule: int, phi: float, star: bool = False, seed: int = 0) -> System:
+def _with_side_chains(L, path, used, idx, seqs, side_every, side_len):
+    """Side chains of side_len monomers on every side_every-th monomer of each
+    backbone sequence (a chain, or a star arm from the core outwards): each
+    starts on the grid site above (or below) its anchor and follows the path
+    over free sites; an anchor with no free run gets none.  Returns
+    (path indices of all monomers, bonds of the side chains)."""
+    n_sites = len(path)
+    where = np.full((L // 2,) * 3, -1, np.int64)
+    where[path[:, 0] // 2, path[:, 1] // 2, path[:, 2] // 2] = np.arange(n_sites)
+    steps = np.arange(side_len)
+    extra, bonds = [], []
+    nxt = len(idx)
+    for seq in seqs:
+        for q in range(side_every - 1, len(seq), side_every):
+            anchor = int(seq[q])
+            ci, cj, ck = path[idx[anchor]] // 2
+            found = None
+            for dk in (1, -1):
+                kk = ck + dk
+                if 0 <= kk < L // 2:
+                    s0 = int(where[ci, cj, kk])
+                    for sgn in (1, -1):
+                        run = s0 + sgn * steps
+                        if run.min() >= 0 and run.max() < n_sites and not used[run].any():
+                            found = run
+                            break
+                if found is not None:
+                    break
+            if found is None:
+                continue
+            used[found] = True
+            extra.append(found)
+            bonds.append((anchor, nxt))
+            bonds.extend((nxt + t, nxt + t + 1) for t in range(side_len - 1))
+            nxt += side_len
+    allidx = np.concatenate([idx] + extra) if extra else idx
+    return allidx, np.array(bonds, np.int64).reshape(-1, 2)
+
+
+def ensemble_system(L: int, n_per_molecule: int, phi: float, star: bool = False, seed: int = 0, side_every: int = 0,
+                    side_len: int = 0) -> System:
     """One system of a batched ensemble: linear chains of n_per_molecule
     monomers, or 3-arm stars (a core and three arms of (n-1)//3), placed
     along a grid path through the L^3 box (L a multiple of 8) at volume
     fraction about phi (8 sites per monomer), with gaps between molecules so
-    that the density is even.  At least one molecule is placed."""
+    that the density is even.  At least one molecule is placed.  With
+    side_every > 0, combs: a side chain of side_len monomers on every
+    side_every-th backbone monomer where there is room (attribute 2; the
+    backbone is attribute 1 and its monomers keep the ids 0 .. n_backbone-1,
+    molecule by molecule)."""
     rng = np.random.default_rng(seed)
     path = _grid_path(L)
     n_sites = len(path)
     arm = max(1, (n_per_molecule - 1) // 3) if star else 0
     size = 1 + 3 * arm if star else n_per_molecule
+    combs = side_every > 0 and side_len > 0
     target = max(size, int(round(phi * L ** 3 / 8)))
+    if combs:
+        target = max(size, int(round(target / (1.0 + side_len / side_every))))
     gap = max(0, int(round(size * (1.0 - min(phi, 0.999)) / max(phi, 1e-3))))
     cursor = int(rng.integers(0, max(1, gap + 1)))
     count = target // size
@@ -440,16 +487,26 @@ def ensemble_system(L: int, n_per_molecule: int, phi: float, star: bool = False,
         if starts.size == 0:
             starts = np.array([0])
         idx = (starts[:, None] + np.arange(size)[None, :]).reshape(-1)
-        n = idx.size
-        pos = path[idx]
-        mol = np.arange(n) // size
-        q = np.arange(n) % size
+        nb = idx.size
+        q = np.arange(nb) % size
         a = np.flatnonzero(q < size - 1)
         bonds = np.stack([a, a + 1], axis=1)
+        chains = [(c * size, size) for c in range(nb // size)]
+        kind = "linear"
+        if combs:
+            used = np.zeros(n_sites, bool)
+            used[idx] = True
+            seqs = [np.arange(c * size, (c + 1) * size) for c in range(nb // size)]
+            idx, side = _with_side_chains(L, path, used, idx, seqs, side_every, side_len)
+            bonds = np.concatenate([bonds, side])
+            chains = []
+            kind = f"comb{side_every}x{side_len}_"
+        n = idx.size
+        pos = path[idx]
         deg, nbr = _topology_from_bonds(n, bonds)
-        chains = [(c * size, size) for c in range(n // size)]
-        name = f"linear{size}_phi{n * 8 / L ** 3:.2f}_L{L}"
-        return System((L, L, L), pos.astype(np.int32), deg, nbr, chains=chains, name=name)
+        attrs = np.where(np.arange(n) < nb, 1, 2).astype(np.int32)
+        name = f"{kind}linear{size}_phi{n * 8 / L ** 3:.2f}_L{L}" if combs else f"linear{size}_phi{n * 8 / L ** 3:.2f}_L{L}"
+        return System((L, L, L), pos.astype(np.int32), deg, nbr, chains=chains, attributes=attrs, name=name)
     where = np.full((L // 2,) * 3, -1, np.int64)
     where[path[:, 0] // 2, path[:, 1] // 2, path[:, 2] // 2] = np.arange(n_sites)
     used = np.zeros(n_sites, bool)
@@ -497,8 +554,7 @@ def ensemble_system(L: int, n_per_molecule: int, phi: float, star: bool = False,
     if not mols:
         raise ValueError("no molecule fits the box")
     idx = np.concatenate(mols)
-    n = idx.size
-    pos = path[idx]
+    nb = idx.size
     # per star: core -> arm k's first monomer, then along each arm
     base = (np.arange(len(mols)) * size)[:, None]
     tmpl = []
@@ -508,9 +564,17 @@ def ensemble_system(L: int, n_per_molecule: int, phi: float, star: bool = False,
         tmpl.extend((first + t, first + t + 1) for t in range(arm - 1))
     tmpl = np.array(tmpl, np.int64)
     bonds = (base[:, :, None] + tmpl[None, :, :]).reshape(-1, 2)
+    name = f"star{size}_phi{nb * 8 / L ** 3:.2f}_L{L}"
+    if combs:
+        seqs = [c * size + 1 + k * arm + np.arange(arm) for c in range(len(mols)) for k in range(3)]
+        idx, side = _with_side_chains(L, path, used, idx, seqs, side_every, side_len)
+        bonds = np.concatenate([bonds, side])
+        name = f"starcomb{size}_{side_every}x{side_len}_phi{idx.size * 8 / L ** 3:.2f}_L{L}"
+    n = idx.size
+    pos = path[idx]
     deg, nbr = _topology_from_bonds(n, bonds)
-    name = f"star{size}_phi{n * 8 / L ** 3:.2f}_L{L}"
-    return System((L, L, L), pos.astype(np.int32), deg, nbr, name=name)
+    attrs = np.where(np.arange(n) < nb, 1, 2).astype(np.int32)
+    return System((L, L, L), pos.astype(np.int32), deg, nbr, attributes=attrs, name=name)
 
 
 def ensemble(n_systems: int, seed: int = 12345, boxes=(32, 48, 64, 96, 128), n_range=(16, 512), phi_range=(0.1, 0.5),

@@ -37,12 +37,13 @@ def _valid(s, pos):
     return True
 
 
-@pytest.mark.parametrize("L,n,phi,star", [(32, 16, 0.5, False), (48, 100, 0.3, True), (64, 512, 0.1, False),
-                                          (40, 40, 0.45, True), (96, 24, 0.2, False)])
-def test_ensemble_systems_are_valid(L, n, phi, star):
-    s = systems.ensemble_system(L, n, phi, star, seed=5)
+@pytest.mark.parametrize("L,n,phi,star,side", [(32, 16, 0.5, False, 0), (48, 100, 0.3, True, 0), (64, 512, 0.1, False, 0),
+                                               (40, 40, 0.45, True, 0), (96, 24, 0.2, False, 0), (32, 25, 0.4, False, 8),
+                                               (48, 40, 0.3, True, 4)])
+def test_ensemble_systems_are_valid(L, n, phi, star, side):
+    s = systems.ensemble_system(L, n, phi, star, seed=5, side_every=side, side_len=3 if side else 0)
     assert _valid(s, s.pos)
-    assert s.deg.max() == (3 if star else 2)
+    assert s.deg.max() == (3 if star or side else 2)
     assert abs(s.n * 8 / L ** 3 - phi) < 0.05 or s.n <= (1 + 3 * ((n - 1) // 3) if star else n)
 
 
@@ -154,6 +155,7 @@ def test_batch_matches_oracle_and_single_runs(clusters):
     lambda: systems.ensemble_system(40, 16, 0.3, True, seed=7),
     lambda: systems.ensemble_system(96, 50, 0.3, False, seed=8),
     lambda: systems.saw_chains(20, 12, box=(24, 40, 32), seed=41),
+    lambda: systems.ensemble_system(48, 30, 0.35, True, seed=9, side_every=4, side_len=3),
 ])
 def test_batch_on_boxes_that_are_not_powers_of_two(make):
     s = make()

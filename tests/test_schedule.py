@@ -46,19 +46,21 @@ def test_relaxation_time_of_ar1_end_vectors():
     assert abs(sch.relaxation_time(t, e, 0) - tau) < 0.15 * tau
 
 
-@pytest.mark.parametrize("star", [False, True])
-def test_molecule_bookkeeping_matches_the_generator(star):
-    s = systems.ensemble_system(32, 25, 0.3, star, seed=4)
+@pytest.mark.parametrize("star,side", [(False, 0), (True, 0), (False, 4), (True, 8)])
+def test_molecule_bookkeeping_matches_the_generator(star, side):
+    s = systems.ensemble_system(32, 25, 0.3, star, seed=4, side_every=side, side_len=3 if side else 0)
     m = sch.molecules(s, 25, star)
-    assert m["count"] * m["size"] == s.n
+    assert m["count"] * m["size"] == int((s.attributes == 1).sum())
+    if side:
+        assert (s.attributes == 2).sum() > 0
     re2, rg2, ends = sch.observables(s.pos, m)
     assert re2 > 0 and rg2 > 0 and len(ends) == m["count"] * (3 if star else 1)
-    if not star:
+    if not star and not side:
         a, b = m["ends"]
         assert (s.deg[a] == 1).all() and (s.deg[b] == 1).all()
-    else:
+    elif star:
         core, tips = m["ends"]
-        assert (s.deg[core] == 3).all() and (s.deg[tips] == 1).all()
+        assert (s.deg[core] == 3).all() and (s.deg[tips] <= 2).all()
 
 
 def test_learned_budgets_beat_a_fixed_budget_with_exact_predictions():
