@@ -292,13 +292,27 @@ def compare(series, budgets, plain_grid=None, bias_floor: float = 0.005):
     _, rel_f = _errors(series, tmax, truth)
     est_l = np.array([window_estimate(s, b) for s, b in zip(series, budgets)])
     est_f = np.array([window_estimate(s, tmax) for s in series])
-    per_n = lambda e: float(np.mean(e / n))
+    # ensemble R_e^2 / N over molecules: every molecule counts once, N its length
+    cnt = np.array([s.get("mol", {}).get("count", 1) for s in series], np.float64)
+    size = np.array([s.get("mol", {}).get("size", s["n"]) for s in series], np.float64)
+    wts = cnt / size
+
+    def ens(e, k=slice(None)):
+        return float(np.sum(wts[k] * e[k]) / np.sum(cnt[k]))
+
+    dev = ens(est_l) / ens(est_f) - 1.0
+    rng = np.random.default_rng(0)
+    boot = []
+    for _ in range(200):
+        k = rng.integers(0, len(series), len(series))
+        boot.append(ens(est_l, k) / ens(est_f, k) - 1.0)
     out = {"learned": {"cost_moves": cost_l, "mean_rel_err_re2": float(np.abs(rel_l).mean()), "bias_re2": float(rel_l.mean()),
                        "within_2pct": float(np.mean(np.abs(rel_l) <= 0.02)), "mean_budget_mcs": float(budgets.mean())},
            "plain": {"cost_moves": float(np.sum(n * chosen)), "mean_rel_err_re2": float(np.abs(rel_p).mean()),
                      "bias_re2": float(rel_p.mean()), "within_2pct": float(np.mean(np.abs(rel_p) <= 0.02)), "budget_mcs": chosen},
            "plain_full_window": {"cost_moves": float(np.sum(n * tmax)), "bias_re2": float(rel_f.mean()), "budget_mcs": tmax},
-           "ensemble_re2_per_n_learned_vs_full_window": per_n(est_l) / per_n(est_f) - 1.0}
+           "ensemble_re2_per_n_learned_vs_full_window": dev,
+           "ensemble_re2_per_n_learned_vs_full_window_bootstrap_sd": float(np.std(boot))}
     out["systems_per_hour_ratio"] = out["plain"]["cost_moves"] / cost_l
     out["systems_per_hour_ratio_vs_full_window"] = out["plain_full_window"]["cost_moves"] / cost_l
     return out

@@ -109,7 +109,7 @@ def test_driver_logic_with_a_synthetic_record(monkeypatch):
             e[0] = rng.normal(size=(8, 3))
             for k in range(1, t.size):
                 e[k] = a * e[k - 1] + math.sqrt(1 - a * a) * rng.normal(size=(8, 3))
-            out.append({"t": t, "re2": re2, "rg2": re2 / 6, "ends": e, "n": 500, "mol": {"count": 20}})
+            out.append({"t": t, "re2": re2, "rg2": re2 / 6, "ends": e, "n": 500, "mol": {"count": 20, "size": p["n"]}})
         return out, None, 1e10
 
     class Stand:
