@@ -895,7 +895,7 @@ struct Batch {
     {
         if (!initialized) throw Err("bfm_batch_initialize must be called first");
         const size_t S = desc.size();
-        if (count != S) throw ArgErr("one MCS count per system is needed");
+        if (count != S || !mcs) throw ArgErr("one MCS count per system is needed");
         BCK(cudaSetDevice(gpu));
         std::vector<uint64_t> left(mcs, mcs + S), done(S, 0);
         std::vector<Work> hw(S);
