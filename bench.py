@@ -1,11 +1,18 @@
 #!/usr/bin/env python
 """Throughput of the colored BFM sweep: attempted moves per second on one B200.
 
-Workload: dense linear melt, 4096 chains x N=256 (1,048,576 monomers) on a
-256^3 periodic lattice, volume fraction 0.5, standard 108-vector bond set,
-two colours (bipartite chains), Saru RNG.  The start is a serpentine crystal
-melted by the sweep itself before warm-up.  A "step" is --mcs-per-step
-Monte-Carlo steps (default 1000; 100 steps = the 100,000 MCS run).
+Workloads (--config):
+  c2 (default)  dense linear melt, 4096 chains x N=256 (1,048,576 monomers) on
+                a 256^3 periodic lattice, volume fraction 0.5, two colours,
+                Saru RNG; the start is a serpentine crystal melted by the sweep
+                itself before warm-up.  A step is 1000 MCS.
+  c1            dilute linear chains, 128 self-avoiding walks x N=64 (8,192
+                monomers) on a 128^3 periodic lattice, Saru RNG.  A step is
+                1000 MCS (10 steps = the 10,000 MCS run).
+  c3            dense melt of 3-arm star-combs (arm 64, a 16-monomer side
+                chain on every 8th backbone monomer), 115,600 stars x 577 =
+                66,701,200 monomers on a 1024^3 periodic lattice, volume
+                fraction 0.497, Saru RNG.  A step is 100 MCS.
 
   value  attempted moves/s from CUDA events around each step's kernels on the
          library stream, state resident in HBM (L2 flushed before each step)
@@ -17,8 +24,10 @@ Multi-GPU (torchrun): independent replicas, one system per rank, no
 collective on the data path ("weak" scaling); times are the max over ranks.
 
 --impl reference runs the reference's own UpdaterGPUScBFM_AB_Type (built for
-sm_100a from its sources into oracle/_ref/) on the same workload through its
-own API; without that library it times the CPU oracle port on all host cores.
+sm_100a from its sources into oracle/_ref/) on the same workload, from the
+same R250 state, through its own API: value from CUDA events around its
+runSimulationOnGPU, e2e on the host clock including its position getters.
+Without that library it times the CPU oracle port on all host cores.
 """
 from __future__ import annotations
 
@@ -41,6 +50,20 @@ WORKLOAD = ("dense linear melt: 4096 chains x N=256 (1,048,576 monomers), 256^3 
 METRIC = "attempted moves/s on 1 B200; batched+surrogate vs plain at equal R_e² error"
 UNIT = "attempted moves/s"
 
+# per workload: generator, MCS per step, untimed melt, the reference
+# instantiation (coordinate type) and where the state lives
+CONFIGS = {
+    "c1": {"mcs_per_step": 1000, "melt_mcs": 0, "ref_ctype": 0, "ref_type": "int32_t", "resident": "l2",
+           "desc": "dilute linear chains: 128 chains x N=64 (8,192 monomers), self-avoiding walks from seed 12345, "
+                   "128^3 periodic lattice, volume fraction 0.031, 108-vector bond set, Saru RNG"},
+    "c2": {"mcs_per_step": 1000, "melt_mcs": 2000, "ref_ctype": 1, "ref_type": "uint8_t", "resident": "l2",
+           "desc": WORKLOAD},
+    "c3": {"mcs_per_step": 100, "melt_mcs": 200, "ref_ctype": None, "ref_type": None, "resident": "hbm",
+           "desc": "dense star-comb melt: 115,600 3-arm stars (arm 64, side chain of 16 on every 8th backbone "
+                   "monomer) x 577 = 66,701,200 monomers, 1024^3 periodic lattice, volume fraction 0.497, "
+                   "108-vector bond set, Saru RNG"},
+}
+
 
 def parse():
     p = argparse.ArgumentParser()
@@ -48,8 +71,10 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--mcs-per-step", type=int, default=1000)
-    p.add_argument("--melt-mcs", type=int, default=2000)
+    p.add_argument("--config", default="c2", choices=sorted(CONFIGS),
+                   help="c2: the 256^3 linear melt (default); c1: 128 chains x 64 on 128^3; c3: the 1024^3 star-comb melt")
+    p.add_argument("--mcs-per-step", type=int, default=None, help="default: 1000 (c1, c2), 100 (c3)")
+    p.add_argument("--melt-mcs", type=int, default=None, help="untimed MCS before warm-up (default per config)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--box", type=int, default=256,
@@ -63,7 +88,15 @@ def parse():
                         "run one after another through the single-system updater")
     p.add_argument("--plain-sample", type=int, default=48,
                    help="systems of the ensemble timed one by one for the plain comparison")
-    return p.parse_args()
+    a = p.parse_args()
+    cfg = CONFIGS[a.config]
+    if a.mcs_per_step is None:
+        a.mcs_per_step = cfg["mcs_per_step"]
+    if a.melt_mcs is None:
+        a.melt_mcs = cfg["melt_mcs"]
+    if a.config != "c2" and a.box != 256:
+        p.error("--box applies to the linear melt (c2) only")
+    return a
 
 
 # ------------------------------------------------------------------ ranks
@@ -190,31 +223,42 @@ def peaks():
 
 
 # --------------------------------------------------------------- workload
-def make_workload(box: int = 256):
+def make_workload(config: str = "c2", box: int = 256):
     from pscbfm_b200 import systems
+    if config == "c1":
+        return systems.saw_chains(128, 64, box=(128, 128, 128), seed=12345)
+    if config == "c3":
+        return systems.star_comb_melt(1024)
     return systems.ordered_melt(box)
 
 
-def workload_name(box: int, system) -> str:
-    if box == 256:
-        return WORKLOAD
+def workload_name(config: str, box: int, system) -> str:
+    if config != "c2" or box == 256:
+        return CONFIGS[config]["desc"]
     chains = len(system.chains)
     return (f"dense linear melt: {chains} chains x N={system.n // chains} ({system.n:,} monomers), {box}^3 periodic "
             f"lattice, volume fraction 0.5, 108-vector bond set, 2 colours, Saru RNG")
 
 
+def workload_tag(config: str, box: int) -> str:
+    """file tag of the committed ncu summaries for this workload"""
+    return {"c1": "c1_128", "c3": "starcomb1024"}.get(config, f"melt{box}")
+
+
 def algorithmic_bytes(c: float, a: float, kbar: float, C: int = 4):
     """Bytes per attempted move of the check and perform kernels: own
-    coordinate C, bond count 1, per bond a 4-byte id and an 8-byte coordinate
-    gather, nine 4-byte lattice probes, the target bit for candidates (c);
-    perform: nine probes of the target lattice for candidates, coordinate
-    write and two lattice bit updates for accepted moves (a)."""
+    coordinate C (4 B up to 256 per axis, 8 B beyond, the reference's
+    coordinate record), bond count 1, per bond a 4-byte id and an 8-byte
+    coordinate gather, nine 4-byte lattice probes, the target bit for
+    candidates (c); perform: nine probes of the target lattice for
+    candidates, coordinate write and two lattice bit updates for accepted
+    moves (a)."""
     check = C + 1 + 12 * kbar + 36 + 4 * c
     perform = 36 * c + C * a + 8 * a
     return check, perform
 
 
-def cpu_baseline(system, pos_now, seconds: float):
+def cpu_baseline(system, pos_now, seconds: float, what: str = "256^3 melt"):
     """The oracle (CPU restatement of the colored sweep, OpenMP over the
     monomers of a colour) on a bounded sample: as many MCS of the same melt
     as fit in about `seconds` of host time, on all host cores; plus the
@@ -239,10 +283,10 @@ def cpu_baseline(system, pos_now, seconds: float):
     dts = time.perf_counter() - t
     serial = s.n / dts
     return {"value": colored, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{m} MCS of the same 256^3 melt ({s.n * m:.3g} attempted moves), colored two-phase "
+            "sample": f"{m} MCS of the same {what} ({s.n * m:.3g} attempted moves), colored two-phase "
                       f"algorithm, OpenMP over the monomers of a colour",
             "serial_1core": {"value": serial, "unit": UNIT, "cores": 1,
-                             "sample": "1 MCS random-sequential Metropolis BFM on the same melt"}}
+                             "sample": f"1 MCS random-sequential Metropolis BFM on the same {what}"}}
 
 
 # ------------------------------------------------------------------- arms
@@ -252,13 +296,15 @@ def run_b200(args, ranks):
     import pscbfm_b200 as pb
     gpu = ranks.local
     torch.cuda.set_device(gpu)
-    system = make_workload(args.box)
+    cfg = CONFIGS[args.config]
+    system = make_workload(args.config, args.box)
     pb.r250_seed(1000 + ranks.rank)
     u = pb.UpdaterGPUScBFM_AB_Type().setup(system, gpu=gpu, rng=pb.Rng.Saru)
     if args.sweep_shape != -1:
         u.setSweepShape(args.sweep_shape)
     S = args.mcs_per_step
-    u.runSimulationOnGPU(args.melt_mcs)        # melt the serpentine crystal (untimed)
+    if args.melt_mcs:
+        u.runSimulationOnGPU(args.melt_mcs)    # melt the ordered start (untimed)
     launch_info = u.getLaunchInfo()
     flushbuf = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{gpu}")
     for _ in range(args.warmup):
@@ -304,23 +350,40 @@ def run_b200(args, ranks):
     value, e2e, total_attempts = aggregate(ranks, attempts, dev_ms / 1e3, e2e_s)
 
     kbar = float(system.deg.mean())
-    b_check, b_perf = algorithmic_bytes(cand, acc, kbar)
+    coord_bytes = 4 if max(system.box) <= 256 else 8
+    b_check, b_perf = algorithmic_bytes(cand, acc, kbar, coord_bytes)
     nspec = u.getNSpecies()
     hbm, hbm_kind = peaks()
     t_launch = k_ms / max(k_launches, 1) / 1e3
     bytes_launch = (b_check + b_perf) * k_attempts / max(k_launches, 1)
     achieved = bytes_launch / t_launch / 1e9
     traffic = None
+    l2 = None
     kname = "k_sweep_w" if launch_info.get("mode", 0) >= 6 else "k_sweep"
-    prof = os.path.join(HERE, "profiles", f"{kname}_melt{args.box}_traffic.json")
+    prof = os.path.join(HERE, "profiles", f"{kname}_{workload_tag(args.config, args.box)}_traffic.json")
     if os.path.exists(prof):
         try:
-            # DRAM bytes per attempted move from one ncu capture of a shorter
-            # launch, scaled to this launch's attempted moves
-            traffic = json.load(open(prof))["dram_bytes_per_attempt"] * k_attempts / max(k_launches, 1)
+            # DRAM (and L2) bytes per attempted move from one ncu capture of a
+            # shorter launch, scaled to this launch's attempted moves
+            tr = json.load(open(prof))
+            traffic = tr["dram_bytes_per_attempt"] * k_attempts / max(k_launches, 1)
+            if "l2_bytes_per_attempt" in tr:
+                l2 = {"lts_throughput_pct": tr.get("lts_throughput_pct"),
+                      "l2_bytes_per_attempt": tr["l2_bytes_per_attempt"],
+                      "algorithmic_bytes_per_attempt": b_check + b_perf,
+                      "dram_bytes_per_attempt": tr["dram_bytes_per_attempt"],
+                      "source": os.path.relpath(prof, HERE)}
         except Exception:
             traffic = None
     whole_bytes = (b_check + b_perf) * total_attempts / ranks.world
+    if cfg["resident"] == "l2":
+        bound = "l2/latency"
+        bound_note = ("the state is L2-resident: the algorithmic bytes are served by L2/L1, not DRAM; the kernel is "
+                      "bound by integer issue, L2 round trips and two grid barriers per colour substep. frac is "
+                      "against the measured HBM copy bandwidth, as the scope table's formula defines it")
+    else:
+        bound = "hbm"
+        bound_note = "the state (GB) is beyond L2: monomer streams and lattice words come from DRAM"
     line = {
         "metric": METRIC,
         "value": value,
@@ -333,18 +396,23 @@ def run_b200(args, ranks):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "u32",
-        "data": "synthetic (seeded serpentine melt of the stated shape, melted in place before warm-up)",
-        "config": {"workload": workload_name(args.box, system), "mcs_per_step": S, "monomers": system.n, "box": list(system.box),
+        "data": ("synthetic (seeded self-avoiding walks)" if args.config == "c1" else
+                 "synthetic (ordered start of the stated shape, melted in place before warm-up)"),
+        "config": {"workload": workload_name(args.config, args.box, system), "config": args.config, "mcs_per_step": S,
+                   "monomers": system.n, "box": [int(b) for b in system.box],
                    "colours": nspec, "replicas": ranks.world,
-                   "l2": "flushed before every step (256 MiB write); the 19 MiB state is L2-resident within a step",
+                   "l2": ("flushed before every step (256 MiB write); the state is L2-resident within a step"
+                          if cfg["resident"] == "l2" else
+                          "flushed before every step (256 MiB write); the state (GB) is larger than L2"),
                    "launch": "one persistent cooperative kernel per chunk of up to 4096 colour substeps",
                    "kernel_shape": launch_info},
         "e2e": {"value": e2e, "unit": UNIT,
                 "h2d_bytes_per_step": S * nspec * 16,
                 "d2h_bytes_per_step": system.n * 12},
         "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+        "roofline": {"bound": bound, "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic, "kernel": kname, "peak_source": f"{hbm_kind} hbm_gbs",
+                     "note": bound_note, "l2": l2, "coord_bytes": coord_bytes,
                      "bytes_per_attempt": {"check": b_check, "perform": b_perf},
                      "attempts_per_launch": k_attempts / max(k_launches, 1),
                      "launch_ms": t_launch * 1e3, "launches_timed": k_launches,
@@ -354,7 +422,8 @@ def run_b200(args, ranks):
         "wall_s": wall,
     }
     if ranks.rank == 0 and ranks.world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(system, pos, args.cpu_seconds)
+        what = {"c1": "128^3 dilute system", "c3": "1024^3 star-comb melt"}.get(args.config, f"{args.box}^3 melt")
+        line["cpu_baseline"] = cpu_baseline(system, pos, args.cpu_seconds, what)
     if ranks.rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -455,54 +524,81 @@ def run_batch(args, ranks):
 
 
 def run_reference(args, ranks):
+    """The reference's own updater on the same workload, from the same R250
+    state as the B200 arm (seed 1000 for rank 0), through its public API:
+    set-up, an untimed melt, warm-up, then timed runSimulationOnGPU calls
+    (value: CUDA events on the legacy stream around each call, which waits
+    for the updater's own stream; e2e: host clock around the call and the
+    read-back through its per-index position getters)."""
     if ranks.rank != 0:
         return
-    if args.box != 256:
-        print(json.dumps({"impl": "reference", "unavailable": "the reference's 8-bit device coordinates take boxes of "
-                                                               "at most 256 per axis"}), flush=True)
+    cfg = CONFIGS[args.config]
+    if cfg["ref_ctype"] is None or args.box != 256:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's device coordinates take boxes of at "
+                                                               "most 256 per axis (UpdaterGPUScBFM_AB_Type.cu:2468-2478)"}),
+              flush=True)
         return
     from oracle import oracle
-    system = make_workload()
+    system = make_workload(args.config, args.box)
     S = args.mcs_per_step
+    config = {"workload": workload_name(args.config, args.box, system), "config": args.config, "mcs_per_step": S,
+              "monomers": system.n, "box": [int(b) for b in system.box], "colours": None, "replicas": 1,
+              "l2": ("flushed before every step (256 MiB write); the state is L2-resident within a step"
+                     if cfg["resident"] == "l2" else "flushed before every step (256 MiB write)"),
+              "launch": f"the reference's UpdaterGPUScBFM_AB_Type<{cfg['ref_type']}>: check, perform and clear "
+                        f"kernels per colour substep, launched from the host"}
     if oracle.ref_gpu() is not None:
         import torch
-        ref = oracle.RefUpdater(system, rng=2, age=0, sort_every=5000, ctype=1, gpu=ranks.local)
-        st = oracle.r250_state(7)
-        ref.run(args.melt_mcs, st)
+        ref = oracle.RefUpdater(system, rng=2, age=0, sort_every=5000, ctype=cfg["ref_ctype"], gpu=ranks.local)
+        st = oracle.r250_state(1000)
+        if args.melt_mcs:
+            ref.run(args.melt_mcs, st)
         flushbuf = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{ranks.local}")
         for _ in range(args.warmup):
             flush_l2(flushbuf)
             ref.run(S, st)
             ref.positions()
+        config["colours"] = int(oracle.graph_coloring(system.deg, system.nbr)[0])
         clocks = Clocks(ranks.local)
         torch.cuda.synchronize()
         clocks.start()
-        tot = 0.0
+        dev_ms, tot = 0.0, 0.0
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
         for _ in range(args.steps):
             flush_l2(flushbuf)
             t0 = time.perf_counter()
+            e0.record()
             ref.run(S, st)            # synchronous, ends with its own copy-back
+            e1.record()
             ref.positions()
             tot += time.perf_counter() - t0
+            e1.synchronize()
+            dev_ms += e0.elapsed_time(e1)
         clk = clocks.stop()
-        value = system.n * S * args.steps / tot
+        value = system.n * S * args.steps / (dev_ms / 1e3)
+        e2e = system.n * S * args.steps / tot
         desc = {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
-                "sample": f"{args.steps} x {S} MCS of the same melt through the reference's "
-                          f"UpdaterGPUScBFM_AB_Type<uint8_t> (its own CUDA kernels, built for sm_100a), "
+                "sample": f"{args.steps} x {S} MCS of the same workload through the reference's "
+                          f"UpdaterGPUScBFM_AB_Type<{cfg['ref_type']}> (its own CUDA kernels, built for sm_100a), "
                           f"one host thread driving the B200"}
+        d2h = system.n * 16           # doCopyBack: mPolymerSystem->pop(), int4 per monomer (.cu:3468-3471)
+        ms_per_step = dev_ms / args.steps
     else:
         clk = None
-        c = cpu_baseline(system, system.pos, args.cpu_seconds)
-        value = c["value"]
+        what = {"c1": "128^3 dilute system"}.get(args.config, "256^3 melt")
+        c = cpu_baseline(system, system.pos, args.cpu_seconds, what)
+        value = e2e = c["value"]
         desc = {k: c[k] for k in ("value", "unit", "cores", "kind", "sample")}
-        tot = None
+        d2h = 0
+        ms_per_step = None
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": (tot / args.steps * 1e3) if tot else None,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "mcs_per_step": S},
-            "cpu_baseline": desc,
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "data": ("synthetic (seeded self-avoiding walks)" if args.config == "c1" else
+                     "synthetic (ordered start of the stated shape, melted in place before warm-up)"),
+            "config": config, "cpu_baseline": desc,
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h},
             "clocks": clk}
     print(json.dumps(line), flush=True)
 

@@ -306,12 +306,19 @@ int bfm_get_coloring(const bfm_handle *h, int *mode, int *on_device);
  *   lattice   device occupation bits, Z-order, 32-bit words, max(L)^3/32 words
  *   allowed512 host table, index (dx&7)|(dy&7)<<3|(dz&7)<<6, 108 entries set
  *   slot_offset, count: the colour's slab; local index = RNG subsequence
- *   seed, iteration, rng: as drawn per substep by runSimulationOnGPU
+ *   seed, iteration: as drawn per substep by runSimulationOnGPU
+ *   rng       BFM_RNG_INTHASH or BFM_RNG_SARU only; Philox (whose offset is
+ *             the full 64-bit age) is refused with BFM_EINVAL
  *   stream    cudaStream_t to enqueue on (asynchronous; NULL = legacy stream)
+ * Every axis is periodic (there are no walls in this call).
  * Limits: max(L)^3 <= 128^3 sites and count <= 262144, else BFM_ETOOLARGE.
+ * A bond table without exactly 108 allowed entries is BFM_EINVAL.  If a CUDA
+ * error from the caller's earlier work is pending, nothing runs and the call
+ * returns BFM_ECUDA, leaving that error for the caller to read.
  * The first call on a device looks up the scratch array's address (one
- * cudaGetSymbolAddress, no allocation); make that first call before any
- * stream capture.  All calls share the one scratch array, so calls that
+ * cudaGetSymbolAddress, no allocation) and loads the call's kernels; make
+ * that first call before any stream capture.  After it, no call loads or
+ * allocates anything.  All calls share the one scratch array, so calls that
  * overlap on the GPU (concurrent streams, several host threads) race. */
 int bfm_substep_noalloc(uint32_t *pos, int32_t *img, const uint32_t *nbr, const uint8_t *deg, uint32_t npad,
                         uint32_t *lattice, uint32_t box_x, uint32_t box_y, uint32_t box_z, const uint8_t *allowed512,

@@ -16,7 +16,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_HOST_SO = os.path.join(HERE, "_ref", "libref_host.so")
 REF_GPU_SO = os.path.join(HERE, "_ref", "libref_pscbfm.so")
-REF_SRC = "/root/reference/src/pscbfm"
+# the reference checkout: $PSCBFM_REFERENCE, else a sibling of the repository
+REF_ROOT = os.environ.get("PSCBFM_REFERENCE", os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
+REF_SRC = os.path.join(REF_ROOT, "src", "pscbfm")
 
 _c = ctypes
 _P = _c.c_void_p

@@ -2075,6 +2075,14 @@ int noalloc_scratch(uint32_t **out)
     if (!g_noalloc_ptr[dev]) {
         void *p = nullptr;
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return BFM_ECUDA;
+        /* With lazy module loading a kernel is loaded (which may allocate and
+         * synchronize) at its first launch.  Load all three kernels now, so
+         * that no later call, whatever its RNG, loads anything. */
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, k_check_na<RNG_SARU>) != cudaSuccess ||
+            cudaFuncGetAttributes(&fa, k_check_na<RNG_INTHASH>) != cudaSuccess ||
+            cudaFuncGetAttributes(&fa, k_perform_na) != cudaSuccess)
+            return BFM_ECUDA;
         g_noalloc_ptr[dev] = p;
     }
     *out = static_cast<uint32_t *>(g_noalloc_ptr[dev]);
@@ -2654,6 +2662,9 @@ int bfm_substep_noalloc(uint32_t *pos, int32_t *img, const uint32_t *nbr, const 
 {
     if (!pos || !nbr || !deg || !lattice || !allowed512) return BFM_EINVAL;
     if (rng != BFM_RNG_INTHASH && rng != BFM_RNG_SARU) return BFM_EINVAL;
+    /* an error left pending by the caller's own earlier work stays theirs:
+     * nothing runs, and it is not cleared */
+    if (cudaPeekAtLastError() != cudaSuccess) return BFM_ECUDA;
     const uint32_t b[3] = {box_x, box_y, box_z};
     uint32_t Lm = 0;
     for (int a = 0; a < 3; ++a) {
@@ -2675,7 +2686,7 @@ int bfm_substep_noalloc(uint32_t *pos, int32_t *img, const uint32_t *nbr, const 
                     bonds.forbidden[code >> 5] |= 1u << (code & 31);
                 }
             }
-    if (nAllowed != 108) return BFM_ERUNTIME;
+    if (nAllowed != 108) return BFM_EINVAL;
     Geometry g;
     for (int a = 0; a < 3; ++a) g.m[a] = dilate3(b[a] - 1) << a;
     uint32_t *scratch = nullptr;

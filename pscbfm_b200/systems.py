@@ -458,6 +458,123 @@ def _with_side_chains(L, path, used, idx, seqs, side_every, side_len):
     return allidx, np.array(bonds, np.int64).reshape(-1, 2)
 
 
+def star_comb_melt(L: int = 1024, arm_len: int = 64, side_every: int = 8, side_len: int = 16) -> System:
+    """Dense melt of 3-arm star-combs: a core and three arms of arm_len
+    backbone monomers, a side chain of side_len = 2 * side_every monomers on
+    every side_every-th backbone monomer (attribute 1 backbone and core,
+    2 side chains).  For L = 1024 this is 115,600 stars x 577 = 66,701,200
+    monomers at volume fraction 0.497.
+
+    Construction (every bond a vector of the 108 set, no two cubes overlap):
+    monomer cubes sit on the grid (2i, 2j, 4k) of L/2 x L/2 sites in L/4
+    layers.  A layer is cut into blocks of arm_len x 3 grid sites, one arm
+    each: the backbone runs along one row of the block from its right end
+    (index 0) to its left end, and the side chain of backbone index q (with
+    (q + 1) % side_every == 0) fills the side_every x 2 sites beside the
+    backbone indices q-side_every+1 .. q, starting next to its anchor and
+    turning back in the far row.  Blocks pair up across rows (6 rows: the
+    lower block's backbone on its top row, the upper block's on its bottom
+    row), so the first backbone monomers of both meet at the corner of a
+    grid cell at the right end of the block column.  The cores sit in the
+    empty half-layers between grid layers (z = 4g + 2), over that corner;
+    a core reaches the first backbone monomers of both blocks in the layer
+    below and in the layer above with (+-1, +-1, +-2) bonds.  Along z, the
+    blocks of a block column are taken in order (layer by layer, lower block
+    first) three at a time: star s owns blocks 3s, 3s+1, 3s+2, which lie in
+    layers g and g+1 for g = floor(3s/2), and its core sits in the half-layer
+    between them (a different one for every star).  Rows of the layer beyond
+    the last whole 6-row pair, and blocks beyond the last whole star of a
+    column, stay empty."""
+    if side_len != 2 * side_every or arm_len % side_every:
+        raise ValueError("side chains must be 2 * side_every long and side_every must divide arm_len")
+    G = L // 2
+    if L % 4 or G % arm_len:
+        raise ValueError("L / 2 must be a multiple of the arm length")
+    A, E, S = arm_len, side_every, side_len
+    ncol, npair, nz = G // A, G // 6, L // 4
+    per_col = (2 * nz) // 3
+    if npair < 1 or per_col < 1:
+        raise ValueError("box too small for one star")
+    arm_size = A + (A // E) * S
+    size = 1 + 3 * arm_size
+    # one arm in block coordinates: grid dx from the block's left column,
+    # row rel. to the backbone row (0), adjacent side row (1), far row (2)
+    q = np.arange(A)
+    a_gx = [A - 1 - q]
+    a_row = [np.zeros(A, np.int64)]
+    anchors = np.arange(E - 1, A, E)
+    t = np.arange(S)
+    for qa in anchors:
+        x0 = A - 1 - qa
+        a_gx.append(x0 + np.where(t < E, t, 2 * E - 1 - t))
+        a_row.append(np.where(t < E, 1, 2))
+    a_gx = np.concatenate(a_gx)
+    a_row = np.concatenate(a_row)
+    # local bonds of one arm (ids relative to the arm's first monomer)
+    ab = [np.stack([q[:-1], q[1:]], axis=1)]
+    for c, qa in enumerate(anchors):
+        first = A + c * S
+        ab.append(np.array([[qa, first]]))
+        ab.append(np.stack([first + t[:-1], first + t[1:]], axis=1))
+    ab = np.concatenate(ab)
+    # star template for even and odd star index: (layer offset dk, block row b) of each arm
+    arm_blocks = {0: ((0, 0), (0, 1), (1, 0)), 1: ((0, 1), (1, 0), (1, 1))}
+
+    def template(par):
+        gx = np.zeros(size, np.int64)
+        gy = np.zeros(size, np.int64)
+        dk = np.zeros(size, np.int64)
+        for a, (k, b) in enumerate(arm_blocks[par]):
+            sl = slice(1 + a * arm_size, 1 + (a + 1) * arm_size)
+            gx[sl] = a_gx
+            # lower block (b = 0): backbone on row 2 of rows 0..2, sides on 1, 0;
+            # upper block (b = 1): backbone on row 3, sides on 4, 5
+            gy[sl] = np.where(b == 0, 2 - a_row, 3 + a_row)
+            dk[sl] = k
+        return gx, gy, dk
+
+    tmpl = {par: template(par) for par in (0, 1)}
+    bonds1 = [np.array([[0, 1 + a * arm_size] for a in range(3)])]
+    for a in range(3):
+        bonds1.append(ab + 1 + a * arm_size)
+    bonds1 = np.concatenate(bonds1)          # (size - 1, 2) local bonds of one star
+    n_stars = npair * ncol * per_col
+    n = n_stars * size
+    pp, jj, ss = np.meshgrid(np.arange(npair), np.arange(ncol), np.arange(per_col), indexing="ij")
+    pp, jj, ss = pp.reshape(-1), jj.reshape(-1), ss.reshape(-1)
+    g = (3 * ss) // 2
+    pos = np.empty((n_stars, size, 3), np.int32)
+    for par in (0, 1):
+        sel = np.flatnonzero(ss % 2 == par)
+        gx, gy, dk = tmpl[par]
+        pos[sel, :, 0] = 2 * (A * jj[sel, None] + gx[None, :])
+        pos[sel, :, 1] = 2 * (6 * pp[sel, None] + gy[None, :])
+        pos[sel, :, 2] = 4 * (g[sel, None] + dk[None, :])
+    pos[:, 0, 0] = 2 * A * jj + 2 * A - 1
+    pos[:, 0, 1] = 12 * pp + 5
+    pos[:, 0, 2] = 4 * g + 2
+    pos = pos.reshape(n, 3)
+    # topology of one star, then offset per star
+    deg1 = np.zeros(size, np.uint8)
+    nbr1 = np.zeros((size, 8), np.uint32)
+    for x, y in bonds1:                      # partner slots in bond order, as _connect fills them
+        nbr1[x, deg1[x]] = y
+        deg1[x] += 1
+        nbr1[y, deg1[y]] = x
+        deg1[y] += 1
+    deg = np.tile(deg1, n_stars)
+    nbr = np.empty((n_stars, size, 8), np.uint32)
+    off = (np.arange(n_stars, dtype=np.uint64) * np.uint64(size)).astype(np.uint32)
+    valid = np.arange(8)[None, :] < deg1[:, None]
+    nbr[:] = np.where(valid[None], nbr1[None] + off[:, None, None], 0)
+    nbr = nbr.reshape(n, 8)
+    attr1 = np.ones(size, np.int32)
+    for a in range(3):
+        attr1[1 + a * arm_size + A:1 + (a + 1) * arm_size] = 2
+    return System((L, L, L), pos, deg, nbr, attributes=np.tile(attr1, n_stars),
+                  name=f"starcomb_melt_{n_stars}x{size}_L{L}")
+
+
 def ensemble_system(L: int, n_per_molecule: int, phi: float, star: bool = False, seed: int = 0, side_every: int = 0,
                     side_len: int = 0) -> System:
     """One system of a batched ensemble: linear chains of n_per_molecule

@@ -65,6 +65,25 @@ def test_cuda_sweep_statistics_match_serial_bfm():
         assert ok, f"{name}: colored {ma:.3f} vs serial {mb:.3f}, 2 sigma = {2 * se:.3f}"
 
 
+@pytest.mark.gpu
+def test_c1_statistics_match_serial_bfm():
+    """Configuration C1 itself (128 self-avoiding chains x 64 on 128^3):
+    after 10,000 MCS of equilibration, 20 blocks of 1000 MCS."""
+    s = systems.saw_chains(128, 64, box=(128, 128, 128), seed=12345)
+    pb.r250_seed(56)
+    u = pb.UpdaterGPUScBFM_AB_Type().setup(s, rng=pb.Rng.Saru)
+
+    def gpu_step(pos, nmcs):
+        u.runSimulationOnGPU(nmcs)
+        return u.getAllMonomerPositions()
+
+    col = _collect(gpu_step, s.pos, s.chains, 10000, 20, 1000)
+    ser = _collect(_serial_stepper(s, 8), s.pos, s.chains, 10000, 20, 1000)
+    for name, a, b in zip(("R_e^2", "R_g^2", "g1(1000 MCS)"), col, ser):
+        ok, ma, mb, se = _within(a, b)
+        assert ok, f"{name}: colored {ma:.3f} vs serial {mb:.3f}, 2 sigma = {2 * se:.3f}"
+
+
 def test_oracle_colored_statistics_match_serial_bfm():
     """The same check for the CPU restatement of the colored algorithm, on
     a smaller system (runs without a GPU)."""
