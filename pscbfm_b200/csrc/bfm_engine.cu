@@ -340,12 +340,13 @@ __device__ __forceinline__ void build_split_table(unsigned long long *tab)
 }
 
 /* occupied sites of a face in lattice L; which of words 1..3 it touches
- * follows from the table entry (the transverse ranges spill over into the
- * next brick when lb, lc >= 2), so the loads do not wait for the masks */
+ * follows from the face's spill flags (the transverse ranges spill over
+ * into the next brick when their first site has low coordinate bits >= 2),
+ * so the loads do not wait for the masks */
 __device__ __forceinline__ unsigned long long split_occupied(const unsigned long long *L, const FaceW &fw,
                                                              const unsigned long long *tab, uint32_t lane)
 {
-    const bool sb = ((fw.t >> 2) & 3u) >= 2u, sc = (fw.t & 3u) >= 2u;
+    const bool sb = fw.sb != 0u, sc = fw.sc != 0u;
     const unsigned long long *tp = tab + (size_t)fw.t * kTabReplicas + (lane & (kTabReplicas - 1u));
     constexpr size_t G = (size_t)192 * kTabReplicas;
     unsigned long long o = L[fw.w[0]] & tp[0];
@@ -754,6 +755,7 @@ __global__ void __launch_bounds__(1024, 1)
     __shared__ uint32_t s_after[6 * 16];
     __shared__ uint32_t s_lo[kWinMaxSpecies], s_n[kWinMaxSpecies], s_off[kWinMaxSpecies], s_base[kWinMaxSpecies];
     __shared__ unsigned int s_wcnt[2][32];
+    __shared__ DirK s_dk[6];
 
     const WinLayout lay{window, T, ptotal};
     const uint32_t seg = lay.seg();
@@ -764,6 +766,7 @@ __global__ void __launch_bounds__(1024, 1)
     uint2 *lists = reinterpret_cast<uint2 *>(s_dyn + lay.lists());
 
     build_split_table(s_tab);
+    if (threadIdx.x < 6) s_dk[threadIdx.x] = dir_consts((int)threadIdx.x, s.g);
     for (uint32_t e = threadIdx.x; e < 96; e += T) { /* the CTA may have fewer than 96 threads */
         const uint32_t dir = e >> 4, w = e & 15u, ax = dir >> 1;
         uint32_t bits = 0;
@@ -850,8 +853,7 @@ __global__ void __launch_bounds__(1024, 1)
 
         /* phase A: U items per thread at a time */
         for (uint32_t b0 = 0; b0 < n; b0 += (uint32_t)U * T) {
-            FaceW f[U];
-            uint32_t r0[U], x[U], ca[U];
+            uint32_t r0[U], x[U], ca[U], r1[U];
             unsigned long long occ[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
@@ -863,11 +865,13 @@ __global__ void __launch_bounds__(1024, 1)
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const uint32_t w = b0 + (uint32_t)u * T + threadIdx.x;
-                f[u] = face_words(r0[u], (int)(x[u] & 7u), geo);
+                const DirK dk = s_dk[x[u] & 7u];
+                const FaceW f = face_k(r0[u], dk);
+                r1[u] = step_k(r0[u], dk);
                 occ[u] = 1ull;
                 ca[u] = 0u;
                 if (w < n) {
-                    occ[u] = occupied(lat, f[u]);
+                    occ[u] = occupied(lat, f);
                     if (maxdeg > 0) ca[u] = bc_pair(bcode)[off + w];
                 }
             }
@@ -887,10 +891,7 @@ __global__ void __launch_bounds__(1024, 1)
                         if ((after[c >> 5] >> (c & 31u)) & 1u) ok = false;
                     }
                 }
-                if (ok) {
-                    const uint32_t r1 = (dir & 1) ? zinc(r0[u], f[u].ma, f[u].ua) : zdec(r0[u], f[u].ma, f[u].ua);
-                    atomicOr(tb + (r1 >> 6), 1ull << (r1 & 63u));
-                }
+                if (ok) atomicOr(tb + (r1[u] >> 6), 1ull << (r1[u] & 63u));
                 const unsigned int m = __ballot_sync(0xFFFFFFFFu, ok);
                 if (ok) wlist[wc + __popc(m & lanemask)] = make_uint2(w | ((uint32_t)dir << 28), r0[u]);
                 wc += __popc(m);
@@ -965,7 +966,7 @@ __global__ void __launch_bounds__(1024, 1)
             const unsigned long long *tr = tmp + (size_t)d.buf * words;
             if (bval) {
                 const uint32_t w = e0.x & 0x0FFFFFFFu;
-                if (!occupied(tr, face_words(e0.y, (int)(e0.x >> 28), geo))) {
+                if (!occupied(tr, face_k(e0.y, s_dk[e0.x >> 28]))) {
                     apply_move(s, lat, spos + base + w, off + w, e0.y, (int)(e0.x >> 28), geo, bdg, bq0, bv0, bc0, bq1, bv1, bc1);
                     ++nAcc;
                 }
@@ -989,7 +990,7 @@ __global__ void __launch_bounds__(1024, 1)
                     q1 = nbr[(size_t)npad + slot];
                     v1 = s.rev[(size_t)npad + slot];
                 }
-                if (occupied(tr, face_words(e.y, (int)(e.x >> 28), geo))) continue;
+                if (occupied(tr, face_k(e.y, s_dk[e.x >> 28]))) continue;
                 apply_move(s, lat, spos + base + w, slot, e.y, (int)(e.x >> 28), geo, dgm, q0, v0, c0, q1, v1, c1);
                 ++nAcc;
             }
