@@ -88,6 +88,11 @@ def parse():
                         "run one after another through the single-system updater")
     p.add_argument("--plain-sample", type=int, default=48,
                    help="systems of the ensemble timed one by one for the plain comparison")
+    p.add_argument("--schedule", type=int, default=0,
+                   help="run the learned schedule live against plain fixed budgets on an ensemble of this many "
+                        "systems (batched-ensemble ranges), recorded for --schedule-mcs MCS")
+    p.add_argument("--schedule-mcs", type=int, default=100000)
+    p.add_argument("--schedule-every", type=int, default=500)
     a = p.parse_args()
     cfg = CONFIGS[a.config]
     if a.mcs_per_step is None:
@@ -523,6 +528,31 @@ def run_batch(args, ranks):
         print(json.dumps(line), flush=True)
 
 
+def run_schedule(args, ranks):
+    """The learned run schedule, live: systems equilibrated per hour on the
+    wall clock, learned budgets (with admission order and the drift judge
+    extending runs on the GPU) against the cheapest plain fixed budget of
+    equal R_e^2 bias, batched and solo."""
+    if ranks.rank != 0:
+        return
+    import torch
+
+    from pscbfm_b200 import schedule as sch
+    torch.cuda.set_device(ranks.local)
+    clocks = Clocks(ranks.local)
+    clocks.start()
+    rep = sch.live_compare(args.schedule, args.schedule_mcs, args.schedule_every, gpu=ranks.local)
+    clk = clocks.stop()
+    line = {"metric": "systems equilibrated per hour on 1 B200, learned schedule vs plain fixed budget at equal R_e^2 bias",
+            "value": rep["systems_per_hour"]["learned"], "unit": "systems/hour", "n_gpus": 1, "higher_is_better": True,
+            "vs_baseline": None, "dtype": "u32 (sweep), bf16/fp32 (network)", "data": "synthetic (seeded ensemble generator)",
+            "config": {"workload": "learned schedule on batched ensembles", "systems": args.schedule,
+                       "recorded_mcs": args.schedule_mcs, "snapshot_every": args.schedule_every},
+            "ratio_learned_vs_plain": rep["ratio_learned_vs_plain"], "ratio_learned_vs_solo": rep["ratio_learned_vs_solo"],
+            "report": rep, "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, ranks):
     """The reference's own updater on the same workload, from the same R250
     state as the B200 arm (seed 1000 for rank 0), through its public API:
@@ -609,6 +639,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, ranks)
+        elif args.schedule:
+            run_schedule(args, ranks)
         elif args.batch:
             run_batch(args, ranks)
         else:

@@ -183,6 +183,12 @@ int bfm_batch_get_positions(bfm_batch *b, uint32_t sys, int32_t *pos3, size_t n)
 /* positions of every system at once: systems in the order added, each in
  * its original monomer order (n_total >= all monomers; 3 ints each) */
 int bfm_batch_get_all_positions(bfm_batch *b, int32_t *pos3, size_t n_total);
+/* unfolded positions of m selected monomers (3 ints each, in the order
+ * asked): ids[k] = (system index << 32) | original monomer id.  For
+ * observables of many systems between runs (molecule ends for R_e^2 and
+ * the end-to-end autocorrelation) without reading whole ensembles back.
+ * No counterpart in the reference (one system per updater there). */
+int bfm_batch_gather_positions(bfm_batch *b, const uint64_t *ids, size_t m, int32_t *pos3);
 /* age, R250 state (251 words) and counters (attempts, candidates, accepts) of system sys; any pointer may be NULL */
 int bfm_batch_get_state(bfm_batch *b, uint32_t sys, int64_t *age, uint32_t *r250_state251, uint64_t *counters3);
 /* occupation bits of system sys (Z-order of the box padded to powers of two); *needed receives the word count */

@@ -117,6 +117,7 @@ _SIGS = {
     "bfm_batch_get_positions": (_c.c_int, [_P, _c.c_uint32, _P, _c.c_size_t]),
     "bfm_batch_get_state": (_c.c_int, [_P, _c.c_uint32, _P, _P, _P]),
     "bfm_batch_get_all_positions": (_c.c_int, [_P, _P, _c.c_size_t]),
+    "bfm_batch_gather_positions": (_c.c_int, [_P, _P, _c.c_size_t, _P]),
     "bfm_batch_get_lattice": (_c.c_int, [_P, _c.c_uint32, _P, _c.c_size_t, _P]),
     "bfm_batch_info": (_c.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "bfm_mlp_create": (_c.c_int, [_c.c_int, _c.c_uint32, _c.c_uint32, _c.c_uint32, _c.c_uint64, _c.POINTER(_P)]),

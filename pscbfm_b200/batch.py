@@ -103,6 +103,19 @@ class Batch:
         cuts = np.cumsum([0] + self._sizes)
         return [out[cuts[i]:cuts[i + 1]] for i in range(len(self._sizes))]
 
+    def gather(self, systems, ids) -> np.ndarray:
+        """unfolded positions (m, 3) of the monomers ids[k] of systems[k]
+        (original monomer ids), read on the device"""
+        sy = np.asarray(systems, np.uint64).reshape(-1)
+        ii = np.asarray(ids, np.uint64).reshape(-1)
+        if sy.size != ii.size:
+            raise ValueError("one system index per monomer id")
+        g = np.ascontiguousarray((sy << np.uint64(32)) | ii, dtype=np.uint64)
+        out = np.empty((g.size, 3), np.int32)
+        if g.size:
+            self._check(self._lib.bfm_batch_gather_positions(self._h, g.ctypes.data, g.size, out.ctypes.data))
+        return out
+
     def state(self, sys: int):
         """(age, R250 state of 251 words, (attempts, candidates, accepts))"""
         age = ctypes.c_int64()

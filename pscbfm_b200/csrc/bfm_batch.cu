@@ -468,6 +468,36 @@ __global__ void k_unfold(const uint32_t *__restrict__ pos, const int32_t *__rest
     }
 }
 
+/* slot of every monomer, by global original index (system base + original id) */
+__global__ void k_slot_of(const uint32_t *__restrict__ s2o, const SysDesc *__restrict__ desc, uint32_t nsys, uint32_t T,
+                          uint32_t *__restrict__ slotOf)
+{
+    for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < T; slot += gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = nsys; /* the system whose slot range holds `slot` */
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (desc[mid].base <= slot) lo = mid;
+            else hi = mid;
+        }
+        slotOf[desc[lo].base + s2o[slot]] = slot;
+    }
+}
+
+/* unfolded positions of selected monomers: ids[k] = (system << 32) | original id */
+__global__ void k_gather(const uint32_t *__restrict__ pos, const int32_t *__restrict__ img, const uint32_t *__restrict__ slotOf,
+                         const SysDesc *__restrict__ desc, uint32_t T, const unsigned long long *__restrict__ ids, uint32_t m,
+                         int32_t *__restrict__ out)
+{
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        const unsigned long long id = ids[k];
+        const SysDesc &d = desc[id >> 32];
+        const uint32_t slot = slotOf[d.base + (uint32_t)id], c = pos[slot];
+        out[3 * (size_t)k + 0] = (int32_t)undilate3(c) + img[slot] * (int32_t)(undilate3(d.top[0]) + 1);
+        out[3 * (size_t)k + 1] = (int32_t)undilate3(c >> 1) + img[(size_t)T + slot] * (int32_t)(undilate3(d.top[1] >> 1) + 1);
+        out[3 * (size_t)k + 2] = (int32_t)undilate3(c >> 2) + img[2 * (size_t)T + slot] * (int32_t)(undilate3(d.top[2] >> 2) + 1);
+    }
+}
+
 /* ---------------------------------------------------------------- host */
 
 struct Err : std::runtime_error {
@@ -551,6 +581,13 @@ struct Batch {
     size_t cubBytes = 0;
     int32_t *d_out = nullptr;
     size_t outCap = 0;
+    /* selected-monomer read-back: slot of every global original index
+     * (rebuilt after runs, which re-sort), requested ids and their positions */
+    uint32_t *d_slotOf = nullptr;
+    bool slotOfValid = false;
+    unsigned long long *d_gids = nullptr;
+    int32_t *d_gout = nullptr;
+    size_t gCap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaStream_t stream2 = nullptr; /* the single-CTA kernel runs beside the cluster kernel */
     cudaEvent_t evFork = nullptr, evJoin = nullptr, evT0 = nullptr, evT1 = nullptr;
@@ -574,6 +611,9 @@ struct Batch {
         bfree(d_lat); bfree(d_tmp); bfree(d_r250); bfree(d_cnt);
         bfree(d_slotSeg); bfree(d_segStart); bfree(d_iota); bfree(d_perm); bfree(d_inv); bfree(d_segSort);
         bfree(d_keys); bfree(d_keys2); bfree(d_out);
+        bfree(d_slotOf); bfree(d_gids); bfree(d_gout);
+        gCap = 0;
+        slotOfValid = false;
         if (d_cub) cudaFree(d_cub);
         d_cub = nullptr;
         if (ev0) cudaEventDestroy(ev0);
@@ -897,6 +937,7 @@ struct Batch {
         const size_t S = desc.size();
         if (count != S || !mcs) throw ArgErr("one MCS count per system is needed");
         BCK(cudaSetDevice(gpu));
+        slotOfValid = false; /* re-sorts move monomers between slots */
         std::vector<uint64_t> left(mcs, mcs + S), done(S, 0);
         std::vector<Work> hw(S);
         std::vector<uint32_t> order;
@@ -1043,6 +1084,40 @@ struct Batch {
         BCK(cudaStreamSynchronize(stream));
     }
 
+    /* unfolded positions of m selected monomers, ids[k] = (system << 32) | original id */
+    void gather(const uint64_t *ids, size_t m, int32_t *out)
+    {
+        if (!initialized) throw Err("bfm_batch_initialize must be called first");
+        if (m == 0) return;
+        if (!ids || !out) throw ArgErr("ids and output are needed");
+        if (m > 0xFFFFFFFFull) throw ArgErr("too many monomers in one call");
+        for (size_t k = 0; k < m; ++k) {
+            const uint64_t s = ids[k] >> 32, o = ids[k] & 0xFFFFFFFFull;
+            if (s >= desc.size() || o >= desc[s].n) throw ArgErr("monomer id out of range at entry " + std::to_string(k));
+        }
+        BCK(cudaSetDevice(gpu));
+        if (!d_slotOf) balloc(d_slotOf, std::max<uint32_t>(T, 1));
+        if (!slotOfValid) {
+            const int blocks = (int)std::min<uint32_t>((T + 255) / 256, 148 * 8);
+            k_slot_of<<<std::max(blocks, 1), 256, 0, stream>>>(d_s2o, d_desc, (uint32_t)desc.size(), T, d_slotOf);
+            BCK(cudaGetLastError());
+            slotOfValid = true;
+        }
+        if (m > gCap) {
+            bfree(d_gids);
+            bfree(d_gout);
+            balloc(d_gids, m);
+            balloc(d_gout, 3 * m);
+            gCap = m;
+        }
+        BCK(cudaMemcpyAsync(d_gids, ids, m * sizeof(uint64_t), cudaMemcpyHostToDevice, stream));
+        const int blocks = (int)std::min<size_t>((m + 255) / 256, 148 * 8);
+        k_gather<<<blocks, 256, 0, stream>>>(d_pos, d_img, d_slotOf, d_desc, T, d_gids, (uint32_t)m, d_gout);
+        BCK(cudaGetLastError());
+        BCK(cudaMemcpyAsync(out, d_gout, 3 * m * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+        BCK(cudaStreamSynchronize(stream));
+    }
+
     /* every system's unfolded positions, systems in order, each in its original monomer order */
     void allPositions(int32_t *out, size_t n)
     {
@@ -1183,6 +1258,11 @@ int bfm_batch_run(bfm_batch *h, const uint32_t *mcs, size_t nsys) { BGUARD(h, { 
 int bfm_batch_get_positions(bfm_batch *h, uint32_t sys, int32_t *pos3, size_t n) { BGUARD(h, { h->b.positions(sys, pos3, n); }); }
 
 int bfm_batch_get_all_positions(bfm_batch *h, int32_t *pos3, size_t n_total) { BGUARD(h, { h->b.allPositions(pos3, n_total); }); }
+
+int bfm_batch_gather_positions(bfm_batch *h, const uint64_t *ids, size_t m, int32_t *pos3)
+{
+    BGUARD(h, { h->b.gather(ids, m, pos3); });
+}
 
 int bfm_batch_get_state(bfm_batch *h, uint32_t sys, int64_t *age, uint32_t *r250_state251, uint64_t *counters3)
 {

@@ -323,6 +323,299 @@ def admission_order(pred_log_teq, sizes):
     return np.argsort(-(10.0 ** np.asarray(pred_log_teq, np.float64)) * np.asarray(sizes, np.float64), kind="stable")
 
 
+# ------------------------------------------------------------ live runs
+class EndRecorder:
+    """R_e^2 and end vectors of every system of a batch from the positions
+    of the molecule ends alone (chain ends; star cores and arm tips), read
+    on the device with Batch.gather -- a few percent of the monomers, so a
+    snapshot of a whole ensemble costs milliseconds.  For stars R_e^2 is the
+    mean squared core-to-tip distance, as in `observables`."""
+
+    def __init__(self, mols, max_vectors: int = 32):
+        sel_s, sel_i, a_idx, b_idx, vsys = [], [], [], [], []
+        off = 0
+        self.keep = []
+        for si, m in enumerate(mols):
+            if m["star"]:
+                core, tips = m["ends"]
+                ids = np.concatenate([core, tips.reshape(-1)])
+                c = len(core)
+                a = np.repeat(np.arange(c), 3)                  # the core of each arm
+                b = c + np.arange(3 * c)                        # its tip
+            else:
+                first, last = m["ends"]
+                ids = np.concatenate([first, last])
+                c = len(first)
+                a, b = np.arange(c), c + np.arange(c)
+            sel_s.append(np.full(len(ids), si, np.int64))
+            sel_i.append(ids.astype(np.int64))
+            nv0 = sum(len(x) for x in a_idx)
+            a_idx.append(off + a)
+            b_idx.append(off + b)
+            vsys.append(np.full(len(a), si, np.int64))
+            self.keep.append(np.arange(nv0, nv0 + min(max_vectors, len(a))))
+            off += len(ids)
+        self.sel_s = np.concatenate(sel_s)
+        self.sel_i = np.concatenate(sel_i)
+        self.a = np.concatenate(a_idx)
+        self.b = np.concatenate(b_idx)
+        self.vsys = np.concatenate(vsys)
+        self.nsys = len(mols)
+        self.count = np.bincount(self.vsys, minlength=self.nsys).astype(np.float64)
+
+    def snapshot(self, batch, batch_index=None):
+        """(R_e^2 per system, end vectors of the first max_vectors molecules
+        of each system); batch_index[i]: the batch's index of system i when
+        the batch holds them in another order"""
+        sel = self.sel_s if batch_index is None else np.asarray(batch_index)[self.sel_s]
+        p = batch.gather(sel, self.sel_i).astype(np.float64)
+        v = p[self.b] - p[self.a]
+        re2 = np.bincount(self.vsys, weights=(v * v).sum(1), minlength=self.nsys) / np.maximum(self.count, 1)
+        return re2, [v[k].astype(np.float32) for k in self.keep]
+
+
+def round_up(x, every):
+    return int(every * math.ceil(float(x) / every))
+
+
+def live_run(systems_, r250_seeds, budgets, every: int, recorder, max_mcs: int | None = None, grow: float = 1.5,
+             judge: bool = True, order=None, gpu: int = 0):
+    """Run an ensemble live on the GPU under per-system budgets: system i
+    advances `every` MCS per batched launch until its budget is spent; its
+    R_e^2 is recorded after every launch; when the budget is spent and the
+    drift check (`drifting`, on the second half of its own series) sees the
+    run still relaxing, the budget grows by `grow` (up to max_mcs) and the
+    system goes on.  Systems are added to the batch in `order` (admission:
+    longest predicted work first).  Returns (wall seconds, per-system MCS
+    run, per-system series {t, re2}, attempted moves, device ms)."""
+    import time
+
+    from .batch import Batch
+    from .updater import Rng
+    nsys = len(systems_)
+    order = np.arange(nsys) if order is None else np.asarray(order)
+    pos_in_batch = np.empty(nsys, np.int64)
+    pos_in_batch[order] = np.arange(nsys)
+    b = Batch(gpu)
+    for i in order:
+        b.add(systems_[i], rng=Rng.Saru, r250_seed=int(r250_seeds[i]))
+    b.initialize()
+    rec = recorder
+    remaining = np.array([round_up(x, every) for x in budgets], np.int64)
+    ran = np.zeros(nsys, np.int64)
+    cap = np.full(nsys, np.iinfo(np.int64).max if max_mcs is None else int(max_mcs), np.int64)
+    remaining = np.minimum(remaining, cap)
+    series = [{"t": [0.0], "re2": []} for _ in range(nsys)]
+    re2, _ = rec.snapshot(b, pos_in_batch)
+    for i in range(nsys):
+        series[i]["re2"].append(float(re2[i]))
+    moves, dev_ms = 0, 0.0
+    t0 = time.perf_counter()
+    while (remaining > 0).any():
+        step = np.where(remaining > 0, every, 0).astype(np.uint32)
+        b.run(step[order])
+        info = b.info()
+        moves += info["last_attempts"]
+        dev_ms += info["last_ms"]
+        ran += step
+        remaining -= step
+        re2, _ = rec.snapshot(b, pos_in_batch)
+        for i in np.flatnonzero(step):
+            series[i]["t"].append(float(ran[i]))
+            series[i]["re2"].append(float(re2[i]))
+            if remaining[i] == 0 and judge and ran[i] < cap[i]:
+                s = {"t": np.asarray(series[i]["t"]), "re2": np.asarray(series[i]["re2"])}
+                if drifting(s, float(ran[i])):
+                    remaining[i] = min(round_up(ran[i] * grow, every), cap[i]) - ran[i]
+    wall = time.perf_counter() - t0
+    b.close()
+    for s in series:
+        s["t"] = np.asarray(s["t"])
+        s["re2"] = np.asarray(s["re2"])
+    return wall, ran, series, moves, dev_ms
+
+
+def record_live(params, total_mcs: int, every: int, seed: int = 0, gpu: int = 0, max_vectors: int = 32, rg2_snapshots: int = 8):
+    """Record an ensemble for total_mcs MCS with the batched simulator:
+    R_e^2 and end vectors of every system after every `every` MCS (from the
+    gathered molecule ends), R_g^2 from whole-system read-backs at
+    rg2_snapshots points of the last third.  Returns (series, systems,
+    rate in attempted moves/s, cumulative device seconds at each snapshot)."""
+    from . import systems as gen
+    from .batch import Batch
+    from .updater import Rng
+    sys_ = [gen.ensemble_system(p["L"], p["n"], p["phi"], p["star"], seed=seed + i, side_every=p.get("side_every", 0),
+                                side_len=p.get("side_len", 0)) for i, p in enumerate(params)]
+    mols = [molecules(s, p["n"], p["star"]) for s, p in zip(sys_, params)]
+    rec = EndRecorder(mols, max_vectors)
+    b = Batch(gpu)
+    for i, s in enumerate(sys_):
+        b.add(s, rng=Rng.Saru, r250_seed=seed + 7919 * i)
+    b.initialize()
+    nsnap = total_mcs // every + 1
+    re2 = np.zeros((len(sys_), nsnap))
+    rg2 = np.full((len(sys_), nsnap), np.nan)
+    ends = [np.zeros((nsnap, len(k), 3), np.float32) for k in rec.keep]
+    late = set(np.linspace(nsnap - nsnap // 3, nsnap - 1, rg2_snapshots).astype(int).tolist())
+
+    def take(k):
+        r, e = rec.snapshot(b)
+        re2[:, k] = r
+        for i in range(len(sys_)):
+            ends[i][k] = e[i]
+        if k in late:
+            for i, p in enumerate(b.all_positions()):
+                rg2[i, k] = observables(p, mols[i])[1]
+
+    take(0)
+    moves, ms = 0, 0.0
+    cum = np.zeros(nsnap)
+    for k in range(1, nsnap):
+        b.run(every)
+        info = b.info()
+        moves += info["last_attempts"]
+        ms += info["last_ms"]
+        cum[k] = ms / 1e3
+        take(k)
+    b.close()
+    t = np.arange(nsnap) * float(every)
+    series = []
+    for i in range(len(sys_)):
+        rg = rg2[i].copy()
+        fill = np.nanmean(rg) if np.isfinite(rg).any() else 0.0
+        rg[~np.isfinite(rg)] = fill
+        series.append({"t": t, "re2": re2[i], "rg2": rg, "ends": ends[i], "n": sys_[i].n, "mol": mols[i]})
+    return series, sys_, moves / (ms / 1e3), cum
+
+
+def live_compare(n_systems: int = 2048, mcs: int = 200000, every: int = 1000, test_fraction: float = 0.25, epochs: int = 300,
+                 seed: int = 3, gpu: int = 0, boxes=(32, 48, 64, 96, 128), n_range=(16, 512), phi_range=(0.1, 0.5)):
+    """The learned schedule run live against plain fixed budgets.
+
+    An ensemble of the batched configuration's ranges is recorded for `mcs`
+    MCS (the full-length runs, whose last third gives each system's plateau
+    R_e^2); the network is trained on the training part; on the held-out
+    test systems three schedules then run live on the GPU, each from the
+    systems' initial states with their own R250 seeds (so every run is a
+    prefix of the recorded trajectory):
+      learned  budgets = factor x predicted end-to-end autocorrelation time,
+               admission longest predicted work first, the drift check
+               extending under-budgeted systems by further batched launches;
+      plain    the cheapest fixed budget whose ensemble bias of R_e^2 is no
+               larger than the learned schedule's, for every system;
+      solo     that fixed budget through the single-system updater, one
+               system after another (timed on a sample, scaled).
+    Systems per hour come from the wall clock of each live run."""
+    import time
+    params = ensemble_params(n_systems, seed, boxes=boxes, n_range=n_range, phi_range=phi_range)
+    t0 = time.perf_counter()
+    series, sys_, rate, cum = record_live(params, mcs, every, seed=seed, gpu=gpu)
+    t_rec = time.perf_counter() - t0
+    x, y = dataset(params, series)
+    rng = np.random.default_rng(seed)
+    idx = rng.permutation(n_systems)
+    n_te = max(1, int(n_systems * test_fraction))
+    te, tr = idx[:n_te], idx[n_te:]
+    n_cal = max(1, len(tr) // 5)
+    cal, fit = tr[:n_cal], tr[n_cal:]
+    model = Surrogate(seed=seed, gpu=gpu)
+    hist = model.fit(x[fit], y[fit], epochs=epochs)
+    pred_te = model.predict(x[te])
+    rmse = np.sqrt(((pred_te - y[te]) ** 2).mean(0))
+    rmse_const = np.sqrt(((y[fit].mean(0) - y[te]) ** 2).mean(0))
+    assess = y[:, 0] <= math.log10(mcs / 12.0)
+    te_a, cal_a = te[assess[te]], cal[assess[cal]]
+    if len(te_a) == 0 or len(cal_a) == 0:
+        te_a, cal_a = te, cal
+    # budget factor calibrated on held-out training systems (replayed on their records)
+    cal_series = [series[i] for i in cal_a]
+    pred_cal = model.predict(x[cal_a])
+    factor, calib = 8.0, {}
+    for f in (2.0, 3.0, 4.0, 6.0, 8.0, 12.0, 16.0):
+        c = compare(cal_series, learned_budgets(pred_cal[:, 3], cal_series, factor=f))
+        calib[f] = {"ratio": c["systems_per_hour_ratio"], "ensemble_re2_vs_full": c["ensemble_re2_per_n_learned_vs_full_window"]}
+    ok = [f for f in calib if abs(calib[f]["ensemble_re2_vs_full"]) <= 0.01]
+    if ok:
+        factor = max(ok, key=lambda f: calib[f]["ratio"])
+    # live runs on the assessable test systems
+    test_sys = [sys_[i] for i in te_a]
+    seeds = [seed + 7919 * int(i) for i in te_a]
+    mols = [series[i]["mol"] for i in te_a]
+    truth = np.array([series[i]["re2"][-max(1, len(series[i]["re2"]) // 3):].mean() for i in te_a])
+    pred = model.predict(x[te_a])
+    budgets = np.maximum(200.0, factor * 10.0 ** pred[:, 3])
+    order = admission_order(pred[:, 3], [s.n for s in test_sys])
+    rec = EndRecorder(mols)
+    wall_l, ran_l, ser_l, moves_l, dev_l = live_run(test_sys, seeds, budgets, every, rec, max_mcs=mcs, order=order, gpu=gpu)
+    est_l = np.array([window_estimate(s, float(r)) for s, r in zip(ser_l, ran_l)])
+    rel_l = (est_l - truth) / truth
+    # the plain fixed budget of equal bias, from the recorded trajectories (a
+    # plain run of B MCS is their prefix), then run live
+    target = max(abs(float(rel_l.mean())), 0.005)
+    rec_series = [series[i] for i in te_a]
+    B = float(mcs)
+    for b_ in series[0]["t"][1:]:
+        rel = np.array([(window_estimate(s, float(b_)) - tv) / tv for s, tv in zip(rec_series, truth)])
+        if abs(rel.mean()) <= target:
+            B = float(b_)
+            break
+    wall_p, ran_p, ser_p, moves_p, dev_p = live_run(test_sys, seeds, np.full(len(te_a), B), every, rec, judge=False, gpu=gpu)
+    est_p = np.array([window_estimate(s, float(r)) for s, r in zip(ser_p, ran_p)])
+    rel_p = (est_p - truth) / truth
+    # ensemble R_e^2 / N over molecules against the full-length runs
+    cnt = np.array([m["count"] for m in mols], np.float64)
+    size = np.array([m["size"] for m in mols], np.float64)
+    ens = lambda e: float(np.sum(cnt / size * e) / np.sum(cnt))
+    est_full = np.array([window_estimate(s, float(mcs)) for s in rec_series])
+    solo = solo_rate([sys_[i] for i in te_a], seeds, gpu=gpu)
+    solo_wall = float(np.sum([s.n for s in test_sys])) * B / solo if solo else None
+    return {
+        "systems": n_systems, "test_systems": int(n_te), "test_systems_assessed": int(len(te_a)), "recorded_mcs": mcs,
+        "snapshot_every": every,
+        "ensemble": f"box edges {list(boxes)}, linear chains or 3-arm stars of {n_range[0]}..{n_range[1]} monomers, "
+                    f"half of them combs (side chains of 2..4 on every 4th or 8th backbone monomer), volume fraction "
+                    f"{phi_range[0]}..{phi_range[1]}, Saru",
+        "record_s": t_rec, "batch_rate_moves_per_s": rate, "train_loss_first_last": [hist[0], hist[-1]],
+        "test_rmse": dict(zip(TARGETS, map(float, rmse))),
+        "test_rmse_constant_predictor": dict(zip(TARGETS, map(float, rmse_const))),
+        "budget_factor": factor, "calibration": {str(k): v for k, v in calib.items()},
+        "learned": {"wall_s": wall_l, "device_s": dev_l / 1e3, "moves": int(moves_l), "mean_mcs": float(ran_l.mean()),
+                    "extended": int(np.sum(ran_l > np.array([round_up(v, every) for v in np.minimum(budgets, mcs)]))),
+                    "bias_re2": float(rel_l.mean()), "mean_abs_rel_err_re2": float(np.abs(rel_l).mean()),
+                    "ensemble_re2_per_n_vs_full": ens(est_l) / ens(est_full) - 1.0},
+        "plain": {"budget_mcs": B, "wall_s": wall_p, "device_s": dev_p / 1e3, "moves": int(moves_p),
+                  "bias_re2": float(rel_p.mean()), "mean_abs_rel_err_re2": float(np.abs(rel_p).mean()),
+                  "ensemble_re2_per_n_vs_full": ens(est_p) / ens(est_full) - 1.0},
+        "solo": {"moves_per_s": solo, "wall_s_estimate": solo_wall},
+        "systems_per_hour": {"learned": len(te_a) / wall_l * 3600.0, "plain": len(te_a) / wall_p * 3600.0,
+                             "solo": (len(te_a) / solo_wall * 3600.0) if solo_wall else None},
+        "ratio_learned_vs_plain": wall_p / wall_l,
+        "ratio_learned_vs_solo": (solo_wall / wall_l) if solo_wall else None,
+    }
+
+
+def solo_rate(systems_, seeds, gpu: int = 0, sample: int = 24, mcs: int = 2000):
+    """attempted moves/s of systems run one after another through the
+    single-system updater (power-of-two boxes; a sample, timed on the host
+    clock around each runSimulationOnGPU)"""
+    import time
+
+    from .updater import Rng, UpdaterGPUScBFM_AB_Type, r250_seed
+    rng = np.random.default_rng(11)
+    pick = [i for i in rng.permutation(len(systems_)) if not any(v & (v - 1) for v in systems_[i].box)][:sample]
+    moves, wall = 0, 0.0
+    for i in pick:
+        r250_seed(int(seeds[i]))
+        u = UpdaterGPUScBFM_AB_Type().setup(systems_[i], gpu=gpu, rng=Rng.Saru)
+        u.runSimulationOnGPU(1)
+        t0 = time.perf_counter()
+        u.runSimulationOnGPU(mcs)
+        wall += time.perf_counter() - t0
+        moves += systems_[i].n * mcs
+        u.cleanup()
+    return moves / wall if wall else None
+
+
 # ------------------------------------------------------------- driver
 def run(n_systems: int = 4096, mcs: int = 20000, every: int = 200, test_fraction: float = 0.25, epochs: int = 300,
         seed: int = 1, gpu: int = 0, save: str | None = None):

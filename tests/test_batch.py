@@ -188,3 +188,26 @@ def test_batch_ensemble_of_64_systems():
     for i in (0, 17, 40, 63):
         o = _run_oracle(sys_[i], pb.Rng.Saru, 0, 5000, states[i].copy(), [20])
         assert np.array_equal(b.positions(i), o.positions()), f"system {i}"
+
+
+@pytest.mark.gpu
+def test_batch_gather_selected_monomers():
+    """bfm_batch_gather_positions returns, in the order asked, the same
+    unfolded positions as the whole-system read-back, also after a run
+    whose re-sorts moved monomers between slots"""
+    sys_, _ = systems.ensemble(12, seed=33, boxes=(32, 48, 64, 128), n_range=(16, 128))
+    b = pb.Batch()
+    for i, s in enumerate(sys_):
+        b.add(s, rng=pb.Rng.Saru, sort_every=7, r250_seed=900 + i)
+    b.initialize()
+    rng = np.random.default_rng(5)
+    for mcs in (0, 23, 40):
+        if mcs:
+            b.run(mcs)
+        sel_s = rng.integers(0, len(sys_), 400)
+        sel_i = np.array([rng.integers(0, sys_[k].n) for k in sel_s])
+        got = b.gather(sel_s, sel_i)
+        want = np.stack([b.positions(int(k))[int(i)] for k, i in zip(sel_s, sel_i)])
+        assert np.array_equal(got, want)
+    with pytest.raises(Exception):
+        b.gather([0], [sys_[0].n])

@@ -131,3 +131,159 @@ def test_driver_logic_with_a_synthetic_record(monkeypatch):
     assert rep["schedule"]["learned"]["cost_moves"] > 0 and rep["schedule"]["plain"]["cost_moves"] > 0
     assert rep["budget_factor"] in (2.0, 3.0, 4.0, 6.0, 8.0, 12.0, 16.0)
     assert set(rep["test_rmse"]) == set(sch.TARGETS)
+
+
+class _FakeBatch:
+    """Stand-in for pscbfm_b200.batch.Batch on the CPU: system i's chain
+    ends separate linearly in time at rate rates[i] (drift) up to a plateau
+    at cap[i] MCS, so the drift check's verdicts are known."""
+
+    rates, caps = None, None
+
+    def __init__(self, gpu=0):
+        self.sys, self.t = [], []
+
+    def add(self, system, rng=None, r250_seed=0):
+        self.sys.append(system)
+        self.t.append(0)
+        return len(self.sys) - 1
+
+    def initialize(self):
+        pass
+
+    def run(self, mcs):
+        m = np.asarray(mcs)
+        for j in range(len(self.sys)):
+            self.t[j] += int(m[j])
+        self._last = int(np.sum(m * np.array([s.n for s in self.sys])))
+
+    def info(self):
+        return {"last_attempts": self._last, "last_ms": 1.0}
+
+    def gather(self, sel_s, sel_i):
+        out = np.zeros((len(sel_s), 3), np.int32)
+        for k, (j, i) in enumerate(zip(sel_s, sel_i)):
+            s = self.sys[int(j)]
+            key = s.name
+            t = min(self.t[int(j)], _FakeBatch.caps[key])
+            out[k] = s.pos[int(i)]
+            out[k, 0] += int(i) * int(round(_FakeBatch.rates[key] * t))   # ends drift apart along x
+        return out
+
+    def close(self):
+        pass
+
+
+def test_live_run_extends_only_drifting_systems(monkeypatch):
+    import pscbfm_b200.batch as batch_mod
+    a = systems.ensemble_system(32, 16, 0.2, False, seed=1)
+    b = systems.ensemble_system(32, 16, 0.2, False, seed=2)
+    a.name, b.name = "drifts_long", "settles_early"
+    _FakeBatch.rates = {"drifts_long": 0.002, "settles_early": 0.002}
+    _FakeBatch.caps = {"drifts_long": 40000, "settles_early": 1000}
+    monkeypatch.setattr(batch_mod, "Batch", _FakeBatch)
+    mols = [sch.molecules(s, 16, False) for s in (a, b)]
+    rec = sch.EndRecorder(mols)
+    wall, ran, series, moves, dev = sch.live_run([a, b], [1, 2], [4000, 4000], 200, rec, max_mcs=20000, order=[1, 0])
+    assert ran[1] == 4000                  # flat second half: no extension
+    assert ran[0] > 4000                   # still relaxing at its budget: extended
+    assert ran[0] <= 20000
+    assert len(series[0]["t"]) == ran[0] // 200 + 1 and series[0]["t"][-1] == ran[0]
+
+
+def test_end_recorder_matches_observables():
+    sys_ = [systems.ensemble_system(32, 24, 0.3, False, seed=3), systems.ensemble_system(32, 31, 0.3, True, seed=4)]
+    mols = [sch.molecules(sys_[0], 24, False), sch.molecules(sys_[1], 31, True)]
+    rec = sch.EndRecorder(mols, max_vectors=5)
+
+    class G:
+        def gather(self, sel_s, sel_i):
+            return np.stack([sys_[int(j)].pos[int(i)] for j, i in zip(sel_s, sel_i)]).astype(np.int32)
+
+    re2, ends = rec.snapshot(G())
+    for k, (s, m) in enumerate(zip(sys_, mols)):
+        want, _, e = sch.observables(s.pos, m)
+        assert abs(re2[k] - want) < 1e-9 * max(1.0, want)
+        assert np.allclose(ends[k], e[:5])
+
+
+class _DetBatch:
+    """Deterministic stand-in for Batch: the chain ends of system j drift
+    apart as 1 - exp(-t / tau), tau growing with its size, plus a small
+    fluctuation fixed by (seed, t) -- so a live run from the same seed
+    reproduces the recorded run, as the real bit-exact batch does."""
+
+    def __init__(self, gpu=0):
+        self.sys, self.seed, self.t = [], [], []
+
+    def add(self, system, rng=None, r250_seed=0):
+        self.sys.append(system)
+        self.seed.append(int(r250_seed))
+        self.t.append(0)
+        return len(self.sys) - 1
+
+    def initialize(self):
+        pass
+
+    def run(self, mcs):
+        m = np.broadcast_to(np.asarray(mcs), (len(self.sys),))
+        for j in range(len(self.sys)):
+            self.t[j] += int(m[j])
+        self._last = int(np.sum(m * np.array([s.n for s in self.sys])))
+
+    def info(self):
+        return {"last_attempts": self._last, "last_ms": 1e-3 * self._last / 1e7}
+
+    def _pos(self, j):
+        s = self.sys[j]
+        tau = 2.0 * s.n ** 1.2
+        t = self.t[j]
+        f = 1.0 - math.exp(-t / tau) + 0.01 * np.random.default_rng(self.seed[j] * 1000003 + t).normal()
+        p = s.pos.astype(np.int64).copy()
+        p[:, 0] += (np.arange(s.n) * 3.0 * f).astype(np.int64)
+        return p.astype(np.int32)
+
+    def gather(self, sel_s, sel_i):
+        cache = {}
+        out = np.zeros((len(sel_s), 3), np.int32)
+        for k, (j, i) in enumerate(zip(sel_s, sel_i)):
+            j = int(j)
+            if j not in cache:
+                cache[j] = self._pos(j)
+            out[k] = cache[j][int(i)]
+        return out
+
+    def all_positions(self):
+        return [self._pos(j) for j in range(len(self.sys))]
+
+    def close(self):
+        pass
+
+
+def test_live_compare_plumbing_on_the_cpu(monkeypatch):
+    """live_compare end to end with the batch, the network and the solo
+    timing replaced by CPU stand-ins: the report's structure and that the
+    learned and plain live runs, calibration and ratios come out."""
+    import pscbfm_b200.batch as batch_mod
+
+    class Stand:
+        def __init__(self, *a, **k):
+            pass
+
+        def fit(self, x, y, epochs=1, **k):
+            X = np.c_[x, np.ones(len(x))]
+            self.w, *_ = np.linalg.lstsq(X, y, rcond=None)
+            return [1.0, 0.5]
+
+        def predict(self, x):
+            return np.c_[x, np.ones(len(x))] @ self.w
+
+    monkeypatch.setattr(batch_mod, "Batch", _DetBatch)
+    monkeypatch.setattr(sch, "Surrogate", Stand)
+    monkeypatch.setattr(sch, "solo_rate", lambda *a, **k: 1e9)
+    rep = sch.live_compare(n_systems=40, mcs=6000, every=200, epochs=1, seed=5, boxes=(16, 24, 32), n_range=(8, 32))
+    assert rep["test_systems"] == 10 and rep["test_systems_assessed"] >= 1
+    assert rep["learned"]["wall_s"] > 0 and rep["plain"]["wall_s"] > 0
+    assert rep["plain"]["budget_mcs"] > 0 and rep["ratio_learned_vs_plain"] > 0
+    assert rep["budget_factor"] in (2.0, 3.0, 4.0, 6.0, 8.0, 12.0, 16.0)
+    assert rep["systems_per_hour"]["learned"] > 0
