@@ -198,15 +198,16 @@ int bfm_batch_info(const bfm_batch *b, uint32_t *nsys, uint64_t *monomers, uint3
                    uint64_t *last_launches, uint64_t *last_attempts);
 
 /* ---- the learned schedule's network (no counterpart in the reference):
- * in -> hidden -> hidden -> out with ReLU, trained and evaluated on the GPU
- * by the library's own tensor-core kernels (bf16 operands, fp32
- * accumulation; fp32 master parameters and Adam moments).  Parameters are
- * one fp32 vector [W1 (hidden x in), b1, W2 (hidden x hidden), b2,
- * W3 (out x hidden), b3], row-major (out x in); He-uniform start from seed.
- * Widths: in and out 1..64, hidden 1..512.  x: batch x in, y and targets:
- * batch x out, row-major host arrays; out_weight (NULL = all 1) weights the
- * squared error of each output; loss = sum_o w_o (y - t)^2 averaged over the
- * batch. */
+ * in -> 128 -> 128 -> out with ReLU, trained and evaluated on the GPU by the
+ * library's own kernel on the tcgen05 tensor cores (bf16 operands in shared
+ * memory, fp32 accumulators in tensor memory; fp32 master parameters and
+ * Adam moments; forward, backward and Adam of many steps in one cooperative
+ * launch).  Parameters are one fp32 vector [W1 (hidden x in), b1,
+ * W2 (hidden x hidden), b2, W3 (out x hidden), b3], row-major (out x in);
+ * He-uniform start from seed.  Widths: in and out 1..16, hidden 128.
+ * x: batch x in, y and targets: batch x out, row-major host arrays;
+ * out_weight (NULL = all 1) weights the squared error of each output;
+ * loss = sum_o w_o (y - t)^2 averaged over the batch. */
 typedef struct bfm_mlp bfm_mlp;
 int bfm_mlp_create(int gpu, uint32_t n_in, uint32_t n_hidden, uint32_t n_out, uint64_t seed, bfm_mlp **out);
 int bfm_mlp_destroy(bfm_mlp *m);
@@ -222,6 +223,14 @@ int bfm_mlp_gradients(bfm_mlp *m, const float *x, const float *y_target, const f
 /* one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the batch; *loss is the loss before the step */
 int bfm_mlp_train_step(bfm_mlp *m, const float *x, const float *y_target, const float *out_weight, uint32_t batch, float lr,
                        float *loss);
+/* n_steps Adam steps in one launch over a data set of n_rows rows: step s
+ * takes the step_rows[s] rows listed next in row_index (indices < n_rows);
+ * losses[s] (may be NULL) is the loss of step s before its update.  The
+ * same as n_steps calls of bfm_mlp_train_step on those rows, bit for bit. */
+int bfm_mlp_train_steps(bfm_mlp *m, const float *x, const float *y_target, const float *out_weight, uint32_t n_rows,
+                        const uint32_t *row_index, const uint32_t *step_rows, uint32_t n_steps, float lr, float *losses);
+/* device time of the latest forward / gradients / training launch, in ms */
+int bfm_mlp_last_ms(const bfm_mlp *m, double *ms);
 
 /* cleanup (.h:487, .cu:3486-3502): frees the set-up; setters may be used again */
 int bfm_cleanup(bfm_handle *h);

@@ -129,6 +129,8 @@ _SIGS = {
     "bfm_mlp_forward": (_c.c_int, [_P, _P, _c.c_uint32, _P]),
     "bfm_mlp_gradients": (_c.c_int, [_P, _P, _P, _P, _c.c_uint32, _P, _c.c_size_t, _P]),
     "bfm_mlp_train_step": (_c.c_int, [_P, _P, _P, _P, _c.c_uint32, _c.c_float, _P]),
+    "bfm_mlp_train_steps": (_c.c_int, [_P, _P, _P, _P, _c.c_uint32, _P, _P, _c.c_uint32, _c.c_float, _P]),
+    "bfm_mlp_last_ms": (_c.c_int, [_P, _P]),
     "bfm_get_lattice": (_c.c_int, [_P, _P, _c.c_size_t]),
     "bfm_get_lattice_words": (_c.c_int, [_P, _c.POINTER(_c.c_size_t)]),
     "bfm_get_nspecies": (_c.c_int, [_P, _c.POINTER(_c.c_uint32)]),

@@ -1,6 +1,7 @@
 """The learned schedule's network on the GPU (``bfm_mlp_*`` in
-include/pscbfm_b200.h): in -> hidden -> hidden -> out with ReLU, bf16
-tensor-core products with fp32 accumulation, fp32 masters and Adam."""
+include/pscbfm_b200.h): in -> 128 -> 128 -> out with ReLU, products on the
+tcgen05 tensor cores (bf16 operands, fp32 accumulators in tensor memory),
+fp32 masters and Adam; training runs many steps per launch."""
 from __future__ import annotations
 
 import ctypes
@@ -68,19 +69,37 @@ class MLP:
                                                  x.shape[0], float(lr), ctypes.byref(loss)))
         return loss.value
 
+    def train_steps(self, x, t, row_index, step_rows, w=None, lr: float = 1e-3) -> np.ndarray:
+        """Adam steps in one launch: step s uses the next step_rows[s] rows of
+        row_index; returns the loss of every step (before its update)"""
+        x, t = self._f32(x, self.shape[0]), self._f32(t, self.shape[2])
+        idx = np.ascontiguousarray(row_index, dtype=np.uint32)
+        rows = np.ascontiguousarray(step_rows, dtype=np.uint32)
+        if int(rows.sum()) != idx.size:
+            raise ValueError("step_rows must add up to the length of row_index")
+        wv = None if w is None else self._f32(w)
+        losses = np.empty(rows.size, np.float32)
+        self._check(self._lib.bfm_mlp_train_steps(self._h, x.ctypes.data, t.ctypes.data, None if wv is None else wv.ctypes.data,
+                                                  x.shape[0], idx.ctypes.data, rows.ctypes.data, rows.size, float(lr),
+                                                  losses.ctypes.data))
+        return losses
+
+    def last_ms(self) -> float:
+        ms = ctypes.c_double()
+        self._check(self._lib.bfm_mlp_last_ms(self._h, ctypes.byref(ms)))
+        return ms.value
+
     def fit(self, x, t, w=None, epochs: int = 200, batch: int = 256, lr: float = 1e-3, seed: int = 0):
-        """mini-batch Adam over shuffled data; returns the loss per epoch"""
+        """mini-batch Adam over shuffled data, every epoch's steps in one
+        launch; returns the loss per epoch"""
         x, t = self._f32(x, self.shape[0]), self._f32(t, self.shape[2])
         rng = np.random.default_rng(seed)
-        hist = []
-        for _ in range(epochs):
-            idx = rng.permutation(len(x))
-            tot = 0.0
-            for b0 in range(0, len(x), batch):
-                sel = idx[b0:b0 + batch]
-                tot += self.train_step(x[sel], t[sel], w, lr) * len(sel)
-            hist.append(tot / len(x))
-        return hist
+        n = len(x)
+        idx = np.concatenate([rng.permutation(n) for _ in range(epochs)]).astype(np.uint32)
+        per = [min(batch, n - b0) for b0 in range(0, n, batch)]
+        losses = self.train_steps(x, t, idx, per * epochs, w, lr)
+        wts = np.array(per * epochs, np.float64).reshape(epochs, len(per))
+        return list((losses.reshape(epochs, len(per)) * wts).sum(1) / n)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -110,9 +129,15 @@ def main(argv=None):
     for _ in range(a.steps):
         last = m.train_step(x, t, lr=1e-3)
     dt = (time.perf_counter() - t0) / a.steps
+    one_ms = m.last_ms()
+    # the same steps in one launch
+    idx = np.tile(np.arange(a.batch, dtype=np.uint32), a.steps)
+    losses = m.train_steps(x, t, idx, [a.batch] * a.steps, lr=1e-3)
+    fused_ms = m.last_ms() / a.steps
     flops = 3 * 2 * a.batch * (6 * a.hidden + a.hidden * a.hidden + a.hidden * 4)
-    print(json.dumps({"batch": a.batch, "hidden": a.hidden, "ms_per_step": dt * 1e3, "loss_first": first, "loss_last": last,
-                      "tflops_per_s_incl_host": flops / dt / 1e12}))
+    print(json.dumps({"batch": a.batch, "hidden": a.hidden, "ms_per_step_host": dt * 1e3, "ms_one_step_launch": one_ms,
+                      "ms_per_step_fused": fused_ms, "loss_first": first, "loss_last": float(losses[-1]),
+                      "tflops_per_s_fused": flops / (fused_ms / 1e3) / 1e12}))
 
 
 if __name__ == "__main__":

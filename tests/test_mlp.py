@@ -114,3 +114,35 @@ def test_adam_step_matches_oracle_and_training_learns():
     assert hist[-1] < 0.1 * first
     xv, tv = _data(1024, seed=12)
     assert float(np.mean((m2.forward(xv) - tv) ** 2).sum()) < 0.2 * first
+
+
+@pytest.mark.gpu
+def test_steps_in_one_launch_equal_single_steps():
+    """bfm_mlp_train_steps runs several Adam steps in one cooperative launch;
+    they must equal the same steps launched one by one, bit for bit (the
+    cross-CTA gradient sums run in a fixed order), including a last step of
+    fewer rows than the others."""
+    from pscbfm_b200.mlp import MLP
+    x, t = _data(700, seed=21)
+    w = np.array([1.0, 0.5, 2.0, 1.0], np.float32)
+    rng = np.random.default_rng(4)
+    idx = rng.permutation(700).astype(np.uint32)
+    rows = [256, 256, 188]
+    a = MLP(I, H, O, seed=7)
+    b = MLP(I, H, O, seed=7)
+    la = a.train_steps(x, t, idx, rows, w, lr=3e-3)
+    lb, o = [], 0
+    for r in rows:
+        sel = idx[o:o + r]
+        lb.append(b.train_step(x[sel], t[sel], w, lr=3e-3))
+        o += r
+    assert np.array_equal(a.params(), b.params())
+    assert np.array_equal(la, np.array(lb, np.float32))
+
+
+@pytest.mark.gpu
+def test_network_shapes_outside_the_kernel_are_refused():
+    from pscbfm_b200.mlp import MLP
+    for shape in ((17, 128, 4), (6, 64, 4), (6, 128, 17)):
+        with pytest.raises(ValueError):
+            MLP(*shape)
