@@ -272,6 +272,20 @@ int bfm_get_launch_info(const bfm_handle *h, int *mode, int *grid, int *threads,
  * (1024 threads x 1 item in flight, 1024 x 2, 512 x 4).
  * BFM_ERUNTIME when the shape does not fit this system. */
 int bfm_set_sweep_shape(bfm_handle *h, int shape);
+/* launch-shape autotuner (no counterpart in the reference, whose launch
+ * configuration is fixed, UpdaterGPUScBFM_AB_Type.cu:2952-2981): with `on`,
+ * the first schedule chunk of the next run is split into equal trial
+ * launches of the automatic shape, the windowed shapes 6..8, the stored and
+ * staged shapes 1, 2 and the windowed shape with one more round of items per
+ * thread (smaller CTAs), each timed with events; the trials are part of the
+ * run (every shape gives the same trajectory) and the fastest per attempted
+ * move is kept unless the automatic shape is within 3% of it.  Shapes that
+ * do not fit the system are skipped. */
+int bfm_set_sweep_autotune(bfm_handle *h, int on);
+/* the autotuner's trials (up to cap): shape, extra rounds, threads per CTA
+ * and ns per attempted move; *tuned = 1 once it has chosen */
+int bfm_get_sweep_tuning(const bfm_handle *h, int *tuned, uint32_t *count, int *shapes, int *extra_rounds, int *threads,
+                         double *ns_per_move, uint32_t cap);
 /* bound of every grid-barrier wait in the persistent kernel (default 2000 ms);
  * a wait that runs out ends the launch and bfm_run returns BFM_ETIMEOUT */
 int bfm_set_barrier_timeout_ms(bfm_handle *h, uint32_t ms);

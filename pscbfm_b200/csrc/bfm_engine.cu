@@ -1521,6 +1521,19 @@ struct Engine {
     int sweepMode = 0;
     uint32_t sweepWindow = 0;
     int forcedShape = -1; /* -1 automatic; 0..2 bond mode; +3: candidate lists in global memory; 6 windowed */
+    int extraRounds = 0;  /* windowed shapes: rounds of items per thread beyond the fewest (smaller CTAs) */
+
+    /* launch-shape autotuner: on the first chunk of the next run, each
+     * candidate shape runs a trial launch of an equal share of the chunk's
+     * substeps (part of the run: every shape gives the same trajectory),
+     * timed with events; the fastest per attempted move is kept unless the
+     * automatic shape is within 3% of it */
+    struct ShapeTrial {
+        int shape, extra, threads;
+        double nsPerMove;
+    };
+    bool autotune = false, tuned = false;
+    std::vector<ShapeTrial> trials;
     int sweepThreads = kSweepThreads;
     uint32_t sweepTotal = 0; /* windowed kernel: most items of all colours one CTA owns */
     bool sweepGlobalList = false; /* k_sweep: candidate lists in global memory */
@@ -1572,11 +1585,12 @@ struct Engine {
         const uint32_t grid = (uint32_t)smCount;
         const uint32_t per = (nmax + grid - 1) / grid + 1u;
         const uint32_t W = (per + 15u) & ~15u;
-        /* fewest rounds of U items per thread at <= 1024 threads, then the
-         * fewest warps for that many rounds (at least 2: warp 0 watches the
-         * barriers) */
+        /* fewest rounds of U items per thread at <= 1024 threads (plus
+         * `extraRounds`, which the autotuner may add for smaller CTAs), then
+         * the fewest warps for that many rounds (at least 2: warp 0 watches
+         * the barriers) */
         const uint32_t U = (uint32_t)kWinU[variant];
-        const uint32_t rounds = (per + U * 1024u - 1u) / (U * 1024u);
+        const uint32_t rounds = (per + U * 1024u - 1u) / (U * 1024u) + (uint32_t)extraRounds;
         const uint32_t threads = std::max<uint32_t>(64u, 32u * ((per + 32u * U * rounds - 1u) / (32u * U * rounds)));
         uint32_t P = 0; /* most items of all colours one CTA owns */
         for (uint32_t c = 0; c < nSpecies; ++c) P += (spec[c].n + grid - 1) / grid;
@@ -1793,6 +1807,71 @@ struct Engine {
         CK(cudaGraphDestroy(gr));
     }
 
+    /* the autotuner's trials on substeps [0, m) of the uploaded chunk, then
+     * the rest of the chunk with the chosen shape; returns the launches */
+    uint64_t tuneShapes(const Substep *sched, const Substep *hs, uint32_t m)
+    {
+        const int savedShape = forcedShape, savedExtra = extraRounds;
+        /* candidates: automatic first, then every other shape that fits */
+        std::vector<std::pair<int, int>> cand = {{-1, 0}};
+        const int autoMode = sweepMode;
+        for (int sh : {6, 7, 8, 1, 2})
+            if (sh != autoMode) cand.push_back({sh, 0});
+        cand.push_back({autoMode >= SWEEP_WINDOWED ? autoMode : 7, 1});
+        const uint32_t piece = std::max<uint32_t>(1, m / (uint32_t)(cand.size() + 1) / nSpecies) * nSpecies;
+        uint32_t k = 0;
+        uint64_t launches = 0;
+        trials.clear();
+        std::vector<cudaEvent_t> ev;
+        for (auto &c : cand) {
+            if (k + piece > m) break;
+            forcedShape = c.first;
+            extraRounds = c.second;
+            try {
+                configureSweep();
+            } catch (std::runtime_error const &) {
+                continue; /* this shape does not fit the system */
+            }
+            cudaEvent_t e0, e1;
+            CK(cudaEventCreate(&e0));
+            CK(cudaEventCreate(&e1));
+            ev.push_back(e0);
+            ev.push_back(e1);
+            CK(cudaEventRecord(e0, stream));
+            launchSweep(sched, k, k + piece);
+            CK(cudaEventRecord(e1, stream));
+            ++launches;
+            uint64_t att = 0;
+            for (uint32_t j = k; j < k + piece; ++j) att += spec[hs[j].species].n;
+            trials.push_back({c.first < 0 ? sweepMode : c.first, c.second, sweepThreads, (double)att});
+            k += piece;
+        }
+        CK(cudaStreamSynchronize(stream));
+        size_t best = 0;
+        for (size_t i = 0; i < trials.size(); ++i) {
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]));
+            trials[i].nsPerMove = ms * 1e6 / std::max(trials[i].nsPerMove, 1.0);
+            if (trials[i].nsPerMove < trials[best].nsPerMove) best = i;
+        }
+        for (auto e : ev) cudaEventDestroy(e);
+        /* keep the automatic shape unless another is more than 3% faster */
+        if (!trials.empty() && trials[best].nsPerMove < 0.97 * trials[0].nsPerMove) {
+            forcedShape = trials[best].shape;
+            extraRounds = trials[best].extra;
+        } else {
+            forcedShape = savedShape;
+            extraRounds = savedExtra;
+        }
+        configureSweep();
+        tuned = true;
+        if (k < m) {
+            launchSweep(sched, k, m);
+            ++launches;
+        }
+        return launches;
+    }
+
     /* runSimulationOnGPU (.cu:2902-3400) */
     void run(uint32_t nMCS)
     {
@@ -1848,7 +1927,9 @@ struct Engine {
             CK(cudaMemcpyAsync(d_sched[b], hs, m * sizeof(Substep), cudaMemcpyHostToDevice, stream));
             CK(cudaEventRecord(schedFree[b], stream));
             if (filterStats) CK(cudaMemsetAsync(d_fstats, 0, (size_t)m * kFilters * sizeof(unsigned long long), stream));
-            if (mode == 0) {
+            if (mode == 0 && autotune && !tuned && m >= 2 * nSpecies) {
+                launches += tuneShapes(d_sched[b], hs, m);
+            } else if (mode == 0) {
                 profMark();
                 launchSweep(d_sched[b], 0, m);
                 profMark();
@@ -2514,6 +2595,30 @@ int bfm_set_sweep_shape(bfm_handle *h, int shape)
         h->e.forcedShape = shape;
         if (h->e.initialized) h->e.configureSweep();
     });
+}
+
+int bfm_set_sweep_autotune(bfm_handle *h, int on)
+{
+    GUARD(h, {
+        h->e.autotune = on != 0;
+        h->e.tuned = false;
+    });
+}
+
+int bfm_get_sweep_tuning(const bfm_handle *h, int *tuned, uint32_t *count, int *shapes, int *extra_rounds, int *threads,
+                         double *ns_per_move, uint32_t cap)
+{
+    if (!h) return BFM_EINVAL;
+    const auto &t = h->e.trials;
+    if (tuned) *tuned = h->e.tuned ? 1 : 0;
+    if (count) *count = (uint32_t)t.size();
+    for (uint32_t i = 0; i < t.size() && i < cap; ++i) {
+        if (shapes) shapes[i] = t[i].shape;
+        if (extra_rounds) extra_rounds[i] = t[i].extra;
+        if (threads) threads[i] = t[i].threads;
+        if (ns_per_move) ns_per_move[i] = t[i].nsPerMove;
+    }
+    return BFM_OK;
 }
 
 int bfm_get_launch_info(const bfm_handle *h, int *mode, int *grid, int *threads, size_t *smem_bytes)

@@ -309,6 +309,21 @@ class UpdaterGPUScBFM_AB_Type:
         6..8 windowed (1024 threads x 1 item, 1024 x 2, 512 x 4)."""
         self._check(self._lib.bfm_set_sweep_shape(self._h, int(shape)))
 
+    def setSweepAutotune(self, on: bool = True):
+        """time the persistent-kernel shapes on the first chunk of the next run, keep the fastest"""
+        self._check(self._lib.bfm_set_sweep_autotune(self._h, int(bool(on))))
+
+    def getSweepTuning(self) -> dict:
+        tuned = ctypes.c_int()
+        n = ctypes.c_uint32()
+        cap = 16
+        sh, ex, th = (ctypes.c_int * cap)(), (ctypes.c_int * cap)(), (ctypes.c_int * cap)()
+        ns = (ctypes.c_double * cap)()
+        self._check(self._lib.bfm_get_sweep_tuning(self._h, ctypes.byref(tuned), ctypes.byref(n), sh, ex, th, ns, cap))
+        k = min(n.value, cap)
+        return {"tuned": bool(tuned.value),
+                "trials": [{"shape": sh[i], "extra_rounds": ex[i], "threads": th[i], "ns_per_move": ns[i]} for i in range(k)]}
+
     def setBarrierTimeoutMs(self, ms: int):
         self._check(self._lib.bfm_set_barrier_timeout_ms(self._h, int(ms)))
 

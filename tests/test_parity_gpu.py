@@ -236,3 +236,25 @@ def test_full_size_melt_properties():
     w = pos % 256
     codes = w[:, 0] * 65536 + w[:, 1] * 256 + w[:, 2]
     assert np.unique(codes).size == s.n
+
+
+@pytest.mark.parametrize("name", ["melt_L32", "dense_chains", "star_comb"])
+def test_shape_autotuner_keeps_the_trajectory(name):
+    """the autotuner's trial launches (every shape that fits, each on a share
+    of the first chunk) are part of the run: positions stay bit-exact
+    against the oracle, and the tuner reports its trials and a choice"""
+    s = SYSTEMS[name]
+    pb.r250_seed(99)
+    st = pb.r250_get_state()
+    u = pb.UpdaterGPUScBFM_AB_Type().setup(s, rng=pb.Rng.Saru, steps_between_sortings=40)
+    u.setSweepAutotune(True)
+    o = oracle.Sweep(s, rng=2, sort_every=40, threads=4)
+    for nmcs in (60, 25):
+        u.runSimulationOnGPU(nmcs)
+        o.run(nmcs, st)
+        assert np.array_equal(u.getAllMonomerPositions(), o.positions())
+        assert np.array_equal(u.getLattice(), oracle.lattice_words(o.positions(), s.box))
+    info = u.getSweepTuning()
+    assert info["tuned"] and len(info["trials"]) >= 3
+    assert all(t["ns_per_move"] > 0 for t in info["trials"])
+    assert u.getLaunchInfo()["mode"] in {t["shape"] for t in info["trials"]}
