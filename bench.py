@@ -77,9 +77,10 @@ def parse():
     p.add_argument("--melt-mcs", type=int, default=None, help="untimed MCS before warm-up (default per config)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
-    p.add_argument("--box", type=int, default=256,
-                   help="edge of the cubic melt (256: the 4096 x 256 benchmark melt; 512, 1024: the same density "
-                        "with chains of L monomers, states beyond L2)")
+    p.add_argument("--box", type=int, default=None,
+                   help="c2: edge of the cubic linear melt (256: the 4096 x 256 benchmark melt; 512, 1024: the same "
+                        "density with chains of L monomers, states beyond L2); c3: edge of the star-comb melt "
+                        "(1024: the benchmark; 256, 512: the same construction in a smaller box)")
     p.add_argument("--sweep-shape", type=int, default=-1,
                    help="persistent-kernel shape (-1 automatic; see bfm_set_sweep_shape)")
     p.add_argument("--batch", type=int, default=0,
@@ -99,8 +100,10 @@ def parse():
         a.mcs_per_step = cfg["mcs_per_step"]
     if a.melt_mcs is None:
         a.melt_mcs = cfg["melt_mcs"]
-    if a.config != "c2" and a.box != 256:
-        p.error("--box applies to the linear melt (c2) only")
+    if a.box is None:
+        a.box = {"c1": 128, "c2": 256, "c3": 1024}[a.config]
+    if a.config == "c1" and a.box != 128:
+        p.error("c1 is the 128^3 system")
     return a
 
 
@@ -233,11 +236,16 @@ def make_workload(config: str = "c2", box: int = 256):
     if config == "c1":
         return systems.saw_chains(128, 64, box=(128, 128, 128), seed=12345)
     if config == "c3":
-        return systems.star_comb_melt(1024)
+        return systems.star_comb_melt(box)
     return systems.ordered_melt(box)
 
 
 def workload_name(config: str, box: int, system) -> str:
+    if config == "c3" and box != 1024:
+        stars = system.n // 577
+        return (f"dense star-comb melt: {stars:,} 3-arm stars (arm 64, side chain of 16 on every 8th backbone monomer) "
+                f"x 577 = {system.n:,} monomers, {box}^3 periodic lattice, volume fraction {8 * system.n / box ** 3:.3f}, "
+                f"108-vector bond set, Saru RNG")
     if config != "c2" or box == 256:
         return CONFIGS[config]["desc"]
     chains = len(system.chains)
@@ -247,7 +255,7 @@ def workload_name(config: str, box: int, system) -> str:
 
 def workload_tag(config: str, box: int) -> str:
     """file tag of the committed ncu summaries for this workload"""
-    return {"c1": "c1_128", "c3": "starcomb1024"}.get(config, f"melt{box}")
+    return {"c1": "c1_128", "c3": f"starcomb{box}"}.get(config, f"melt{box}")
 
 
 def algorithmic_bytes(c: float, a: float, kbar: float, C: int = 4):
@@ -381,7 +389,8 @@ def run_b200(args, ranks):
         except Exception:
             traffic = None
     whole_bytes = (b_check + b_perf) * total_attempts / ranks.world
-    if cfg["resident"] == "l2":
+    resident = "l2" if max(system.box) <= 256 else "hbm"
+    if resident == "l2":
         bound = "l2/latency"
         bound_note = ("the state is L2-resident: the algorithmic bytes are served by L2/L1, not DRAM; the kernel is "
                       "bound by integer issue, L2 round trips and two grid barriers per colour substep. frac is "
@@ -407,8 +416,8 @@ def run_b200(args, ranks):
                    "monomers": system.n, "box": [int(b) for b in system.box],
                    "colours": nspec, "replicas": ranks.world,
                    "l2": ("flushed before every step (256 MiB write); the state is L2-resident within a step"
-                          if cfg["resident"] == "l2" else
-                          "flushed before every step (256 MiB write); the state (GB) is larger than L2"),
+                          if resident == "l2" else
+                          "flushed before every step (256 MiB write); the state is larger than L2"),
                    "launch": "one persistent cooperative kernel per chunk of up to 4096 colour substeps",
                    "kernel_shape": launch_info},
         "e2e": {"value": e2e, "unit": UNIT,
@@ -427,7 +436,7 @@ def run_b200(args, ranks):
         "wall_s": wall,
     }
     if ranks.rank == 0 and ranks.world == 1 and not args.no_cpu_baseline:
-        what = {"c1": "128^3 dilute system", "c3": "1024^3 star-comb melt"}.get(args.config, f"{args.box}^3 melt")
+        what = {"c1": "128^3 dilute system", "c3": f"{args.box}^3 star-comb melt"}.get(args.config, f"{args.box}^3 melt")
         line["cpu_baseline"] = cpu_baseline(system, pos, args.cpu_seconds, what)
     if ranks.rank == 0:
         print(json.dumps(line), flush=True)
@@ -563,7 +572,7 @@ def run_reference(args, ranks):
     if ranks.rank != 0:
         return
     cfg = CONFIGS[args.config]
-    if cfg["ref_ctype"] is None or args.box != 256:
+    if cfg["ref_ctype"] is None or args.box > 256:
         print(json.dumps({"impl": "reference", "unavailable": "the reference's device coordinates take boxes of at "
                                                                "most 256 per axis (UpdaterGPUScBFM_AB_Type.cu:2468-2478)"}),
               flush=True)

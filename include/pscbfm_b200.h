@@ -306,17 +306,21 @@ int bfm_barrier_selftest_variant(int gpu, uint32_t timeout_ms, uint32_t extra_ar
  * colors[n] receives the colours, *ncolors their number. */
 int bfm_color_graph(uint32_t n, const uint8_t *deg, const uint32_t *nbr8, int uniform, uint32_t *colors,
                     uint32_t *ncolors);
-/* The same colours for a forest (linear chains, stars, combs), with the
- * reference's depth-first walk (graphColoring.tpp:176-351) replaced by a
- * parity union-find on GPU `gpu`: on a forest the walk gives every node the
- * parity of its distance to the lowest id of its component; the uniform
- * rebalancing pass then runs on the host as in bfm_color_graph.  A graph
- * that is not a forest is coloured on the host; *on_device tells which. */
+/* The same colours as bfm_color_graph, with the reference's depth-first
+ * walk (graphColoring.tpp:176-351) replaced on every tree component (linear
+ * chains, stars, combs) by a parity union-find on GPU `gpu`: on a tree the
+ * walk gives every node the parity of its distance to the lowest id of its
+ * component.  Components with a cycle (crosslinks) are walked on the host
+ * -- the walk colours each component from its own nodes, so the result is
+ * the walk's over the whole graph -- and the uniform rebalancing pass runs
+ * on the host.  *on_device: 1 every component on the device, 2 the tree
+ * components on the device and the others on the host, 0 all on the host. */
 int bfm_color_graph_device(int gpu, uint32_t n, const uint8_t *deg, const uint32_t *nbr8, int uniform, uint32_t *colors,
                            uint32_t *ncolors, int *on_device);
-/* colouring at initialize: 0 the host walk (default), 1 the device for
- * forests (same colours, see bfm_color_graph_device); bfm_get_coloring
- * reports the mode and whether the last initialize coloured on the device */
+/* colouring at initialize: 0 the host walk (default), 1 the device path of
+ * bfm_color_graph_device (same colours); bfm_get_coloring reports the mode
+ * and, as bfm_color_graph_device's *on_device, how the last initialize
+ * coloured */
 int bfm_set_coloring(bfm_handle *h, int mode);
 int bfm_get_coloring(const bfm_handle *h, int *mode, int *on_device);
 

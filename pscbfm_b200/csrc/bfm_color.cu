@@ -11,8 +11,11 @@
  * its component.  That parity is computed here with a parity union-find on
  * the GPU (hooking the larger root under the smaller by 64-bit CAS, pointer
  * jumping), and the host rebalancing pass of the reference runs on it, so
- * the colours are the reference's.  A graph that is not a forest is left to
- * the host walk.
+ * the colours are the reference's.  The union-find also yields every node's
+ * component; the walk colours a component from its own nodes only, so a
+ * component with a cycle (bonds >= nodes) is left to the host walk while the
+ * tree components keep their device colours -- the same colours as the
+ * walk over the whole graph.
  *
  * Parent words: parent id << 1 | parity of the path to that parent.
  */
@@ -95,11 +98,9 @@ void ck(cudaError_t e, const char *what)
 
 } // namespace
 
-bool color_forest_device(uint32_t n, const uint8_t *deg, const uint32_t *nbr8, bool uniform, std::vector<uint32_t> &color)
+int color_graph_device(uint32_t n, const uint8_t *deg, const uint32_t *nbr8, bool uniform, std::vector<uint32_t> &color)
 {
-    if (n == 0) return false;
-    uint64_t bonds2 = 0;
-    for (uint32_t i = 0; i < n; ++i) bonds2 += deg[i];
+    if (n == 0) return 0;
     Dev d;
     unsigned long long *P = nullptr;
     uint8_t *ddeg = nullptr;
@@ -132,25 +133,31 @@ bool color_forest_device(uint32_t n, const uint8_t *deg, const uint32_t *nbr8, b
             ck(cudaMemcpy(&changed, cnt + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost), "cudaMemcpy");
             flat = changed == 0;
         }
-        if (!flat) return false;
+        if (!flat) return 0;
         converged = hooks == 0;
     }
-    if (!converged) return false;
+    if (!converged) return 0;
     std::vector<unsigned long long> words(n);
     ck(cudaMemcpy(words.data(), P, (size_t)n * 8, cudaMemcpyDeviceToHost), "cudaMemcpy");
-    uint64_t roots = 0;
-    for (uint32_t i = 0; i < n; ++i) roots += (words[i] >> 1) == i;
-    if (bonds2 / 2 != (uint64_t)n - roots) return false; /* a cycle: not a forest */
-    color.assign(n, 0);
-    std::vector<size_t> count(1, 0);
+    /* nodes and bond ends per component (indexed by its root, the lowest id) */
+    std::vector<uint32_t> nodes(n, 0);
+    std::vector<uint64_t> ends(n, 0);
     for (uint32_t i = 0; i < n; ++i) {
-        const uint32_t c = (uint32_t)(words[i] & 1ull);
-        color[i] = c;
-        if (c >= count.size()) count.resize(c + 1, 0);
-        ++count[c];
+        const uint32_t r = (uint32_t)(words[i] >> 1);
+        ++nodes[r];
+        ends[r] += deg[i];
     }
+    color.assign(n, kNoColor);
+    bool cyclic = false;
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t r = (uint32_t)(words[i] >> 1);
+        if (ends[r] / 2 == (uint64_t)nodes[r] - 1) color[i] = (uint32_t)(words[i] & 1ull); /* a tree */
+        else cyclic = true;
+    }
+    std::vector<size_t> count;
+    dfs_colors_rest(n, deg, nbr8, color, count); /* components with a cycle */
     if (uniform) rebalance_colors(n, deg, nbr8, color, count);
-    return true;
+    return cyclic ? 2 : 1;
 }
 
 } // namespace bfm

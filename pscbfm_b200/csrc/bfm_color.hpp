@@ -1,5 +1,5 @@
 /*
- * bfm_color.hpp -- species colouring of forests on the device (bfm_color.cu).
+ * bfm_color.hpp -- species colouring on the device (bfm_color.cu).
  */
 #pragma once
 #include <cstdint>
@@ -8,10 +8,12 @@
 namespace bfm {
 
 /* The reference's colouring (graphColoring with uniform rebalancing) of a
- * bond graph that is a forest, with its depth-first walk replaced by a
- * parity union-find on the current GPU.  nbr8 holds 8 slots per node.
- * Returns false, leaving `color` untouched, when the graph is not a forest
- * (the caller then colours on the host). */
-bool color_forest_device(uint32_t n, const uint8_t *deg, const uint32_t *nbr8, bool uniform, std::vector<uint32_t> &color);
+ * bond graph, with its depth-first walk replaced on every tree component by
+ * a parity union-find on the current GPU; components with a cycle are
+ * walked on the host.  nbr8 holds 8 slots per node.  Returns 1 when every
+ * component was coloured on the device, 2 when components with a cycle went
+ * to the host walk, 0 (leaving `color` untouched) when the union-find did
+ * not converge and the caller must colour on the host. */
+int color_graph_device(uint32_t n, const uint8_t *deg, const uint32_t *nbr8, bool uniform, std::vector<uint32_t> &color);
 
 } // namespace bfm

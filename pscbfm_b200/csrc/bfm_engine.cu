@@ -1162,7 +1162,7 @@ struct Engine {
     int filterStats = 0; /* the reference's "Stats" filter analysis: 0 off, 1 counted as the reference, 2 the moves made */
 
     /* ---- derived at initialize */
-    bool colorOnDevice = false;
+    int colorOnDevice = 0; /* last initialize: 0 host walk, 1 device, 2 device for the tree components */
     bool initialized = false;
     Geometry g{};
     Bondset bonds{};
@@ -1335,10 +1335,10 @@ struct Engine {
             for (uint32_t j = 0; j < deg[i]; ++j)
                 if (nbr[(size_t)i * 8 + j] >= n)
                     throw InvalidArgument("bond partner id out of range for monomer " + std::to_string(i));
-        colorOnDevice = false;
+        colorOnDevice = 0;
         if (coloringMode == 1) {
             CK(cudaSetDevice(gpu));
-            colorOnDevice = color_forest_device(n, deg.data(), nbr.data(), true, color);
+            colorOnDevice = color_graph_device(n, deg.data(), nbr.data(), true, color);
         }
         if (!colorOnDevice) color = color_graph(n, deg.data(), nbr.data(), true);
         nSpecies = 0;
@@ -2700,7 +2700,7 @@ int bfm_set_launch_mode(bfm_handle *h, int mode)
 int bfm_set_coloring(bfm_handle *h, int mode)
 {
     GUARD(h, {
-        if (mode != 0 && mode != 1) throw InvalidArgument("colouring mode must be 0 (host) or 1 (device for forests)");
+        if (mode != 0 && mode != 1) throw InvalidArgument("colouring mode must be 0 (host) or 1 (device)");
         h->e.coloringMode = mode;
     });
 }
@@ -2709,7 +2709,7 @@ int bfm_get_coloring(const bfm_handle *h, int *mode, int *on_device)
 {
     if (!h) return BFM_EINVAL;
     if (mode) *mode = h->e.coloringMode;
-    if (on_device) *on_device = h->e.colorOnDevice ? 1 : 0;
+    if (on_device) *on_device = h->e.colorOnDevice;
     return BFM_OK;
 }
 
@@ -2725,7 +2725,7 @@ int bfm_color_graph_device(int gpu, uint32_t n, const uint8_t *deg, const uint32
         }
         if (cudaSetDevice(gpu) != cudaSuccess) return BFM_ECUDA;
         std::vector<uint32_t> c;
-        const bool dev = color_forest_device(n, deg, nbr8, uniform != 0, c);
+        const int dev = color_graph_device(n, deg, nbr8, uniform != 0, c);
         if (!dev) c = color_graph(n, deg, nbr8, uniform != 0);
         uint32_t k = 0;
         for (uint32_t i = 0; i < n; ++i) {
@@ -2733,7 +2733,7 @@ int bfm_color_graph_device(int gpu, uint32_t n, const uint8_t *deg, const uint32
             k = std::max(k, c[i] + 1);
         }
         *ncolors = k;
-        if (on_device) *on_device = dev ? 1 : 0;
+        if (on_device) *on_device = dev;
         return BFM_OK;
     } catch (std::exception const &) {
         return BFM_ECUDA;

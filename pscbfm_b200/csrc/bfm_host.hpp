@@ -66,12 +66,21 @@ struct R250 {
  *     do not use, scanning the colours rarest-first (the scan goes on after a
  *     move, as in the reference).
  * nbr holds 8 slots per node.  Throws std::runtime_error past 255 colours. */
-inline std::vector<uint32_t> dfs_colors(uint32_t n, const uint8_t *deg, const uint32_t *nbr, std::vector<size_t> &count)
+/* The walk of step 1 over the nodes whose colour is still kNoColor (whole
+ * components: a component is either coloured already or not at all), in
+ * the reference's order; count receives every colour's node count. */
+constexpr uint32_t kNoColor = 0xFFFFFFFFu;
+inline void dfs_colors_rest(uint32_t n, const uint8_t *deg, const uint32_t *nbr, std::vector<uint32_t> &color,
+                            std::vector<size_t> &count)
 {
-    const uint32_t kNone = 0xFFFFFFFFu;
+    const uint32_t kNone = kNoColor;
     const int64_t kNoNode = -1;
-    std::vector<uint32_t> color(n, kNone);
     count.clear();
+    for (uint32_t i = 0; i < n; ++i)
+        if (color[i] != kNone) {
+            if (color[i] >= count.size()) count.resize(color[i] + 1, 0);
+            ++count[color[i]];
+        }
     std::vector<uint8_t> taken(256);
     for (uint32_t root = 0; root < n; ++root) {
         if (color[root] != kNone) continue;
@@ -116,6 +125,12 @@ inline std::vector<uint32_t> dfs_colors(uint32_t n, const uint8_t *deg, const ui
             }
         }
     }
+}
+
+inline std::vector<uint32_t> dfs_colors(uint32_t n, const uint8_t *deg, const uint32_t *nbr, std::vector<size_t> &count)
+{
+    std::vector<uint32_t> color(n, kNoColor);
+    dfs_colors_rest(n, deg, nbr, color, count);
     return color;
 }
 

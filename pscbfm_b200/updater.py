@@ -351,8 +351,9 @@ class UpdaterGPUScBFM_AB_Type:
 def color_graph(deg, nbr, uniform: bool = True, device: bool = False, gpu: int = 0):
     """The species colouring initialize() uses (the reference's
     graphColoring with uniform rebalancing).  device=True computes the same
-    colours of a forest on the GPU (see bfm_color_graph_device).  Returns
-    (colours, number of colours, coloured on the device)."""
+    colours with the tree components on the GPU (see bfm_color_graph_device).
+    Returns (colours, number of colours, how: 0 host, 1 device, 2 the tree
+    components on the device and the cyclic ones on the host)."""
     d = np.ascontiguousarray(deg, dtype=np.uint8)
     b = np.ascontiguousarray(nbr, dtype=np.uint32)
     n = d.size
@@ -363,10 +364,10 @@ def color_graph(deg, nbr, uniform: bool = True, device: bool = False, gpu: int =
         dev = ctypes.c_int()
         st = lib.bfm_color_graph_device(int(gpu), n, d.ctypes.data, b.ctypes.data, int(uniform), col.ctypes.data,
                                         ctypes.byref(nc), ctypes.byref(dev))
-        on_dev = bool(dev.value)
+        on_dev = int(dev.value)
     else:
         st = lib.bfm_color_graph(n, d.ctypes.data, b.ctypes.data, int(uniform), col.ctypes.data, ctypes.byref(nc))
-        on_dev = False
+        on_dev = 0
     if st != _native.BFM_OK:
         _raise(st, f"colouring failed (status {st})")
     return col, nc.value, on_dev

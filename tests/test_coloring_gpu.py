@@ -1,8 +1,8 @@
-"""Species colouring of forests on the device (bfm_color_graph_device)
-against the host walk that restates the reference's graphColoring: the same
-colours, node for node, on linear chains, shuffled ids, branched trees
-(stars, combs) and isolated monomers; graphs with cycles fall back to the
-host.  A sweep set up with device colouring is bit-exact against the oracle
+"""Species colouring on the device (bfm_color_graph_device) against the
+host walk that restates the reference's graphColoring: the same colours,
+node for node, on linear chains, shuffled ids, branched trees (stars,
+combs), isolated monomers, and crosslinked graphs whose cyclic components
+go to the host walk.  A sweep set up with device colouring is bit-exact against the oracle
 (which colours on the host)."""
 import numpy as np
 import pytest
@@ -57,16 +57,22 @@ def test_device_colouring_equals_host_walk(name):
     s = CASES[name]()
     host, kh, _ = pb.color_graph(s.deg, s.nbr)
     dev, kd, on_dev = pb.color_graph(s.deg, s.nbr, device=True)
-    assert on_dev
+    assert on_dev == 1
     assert kd == kh and np.array_equal(dev, host)
     assert np.array_equal(oracle.graph_coloring(s.deg, s.nbr)[1], host)
 
 
-def test_graph_with_cycles_is_coloured_on_the_host():
-    s = systems.add_crosslinks(systems.saw_chains(40, 20, box=(32, 32, 32), seed=95), 30)
+@pytest.mark.parametrize("links", [3, 30, 400])
+def test_graph_with_cycles_keeps_the_host_colours(links):
+    """crosslinks close cycles in a few components (3 links: 3 of 40), in
+    many (30: 14 of 34) or join everything into cyclic networks (400: 5 of
+    5): tree components are coloured on the device, cyclic ones by the host
+    walk, and the result equals the walk over the whole graph"""
+    s = systems.add_crosslinks(systems.saw_chains(40, 20, box=(32, 32, 32), seed=95), links)
     host, kh, _ = pb.color_graph(s.deg, s.nbr)
     dev, kd, on_dev = pb.color_graph(s.deg, s.nbr, device=True)
-    assert not on_dev and np.array_equal(dev, host)
+    assert on_dev == 2 and kd == kh and np.array_equal(dev, host)
+    assert np.array_equal(oracle.graph_coloring(s.deg, s.nbr)[1], host)
 
 
 def test_sweep_with_device_colouring_matches_oracle():
