@@ -743,9 +743,34 @@ __device__ __forceinline__ void apply_move(const Sys &s, unsigned long long *lat
     }
 }
 
+/* The two synchronisations of a substep, split into arrival and wait: the
+ * counting grid barrier over all CTAs of the cooperative launch, or -- when
+ * the whole launch is one thread-block cluster (CL, small systems) -- the
+ * hardware cluster barrier, where every thread arrives with release and
+ * waits with acquire semantics at cluster scope (which orders the global
+ * lattice, target and bond-code updates between the cluster's CTAs) and a
+ * CTA barrier then ends the window work. */
+template <bool CL>
+__device__ __forceinline__ void win_arrive(GridBarrier *bar, unsigned int &target)
+{
+    if (CL) asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+    else grid_arrive(bar, target, gridDim.x);
+}
+template <bool CL>
+__device__ __forceinline__ bool win_wait(GridBarrier *bar, unsigned int target, unsigned long long timeoutNs)
+{
+    if (CL) {
+        asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+        __syncthreads();
+        return true;
+    }
+    return grid_wait(bar, target, timeoutNs);
+}
+
 /* one shape of the windowed kernel: U items per thread in flight in the
- * check phase; blockDim.x threads (a multiple of 32, 64 to 1024) */
-template <int RNG, int U>
+ * check phase; blockDim.x threads (a multiple of 32, 64 to 1024); CL: the
+ * grid is one cluster (cluster barriers instead of grid barriers) */
+template <int RNG, int U, bool CL = false>
 __global__ void __launch_bounds__(1024, 1)
     k_sweep_w(Sys s, const Substep *__restrict__ sched, uint32_t k0, uint32_t k1, GridBarrier *bar,
               unsigned long long timeoutNs, uint32_t maxdeg, uint32_t window, uint32_t nspec, uint32_t ptotal)
@@ -902,7 +927,7 @@ __global__ void __launch_bounds__(1024, 1)
 
         /* check -> perform barrier */
         __syncthreads();
-        grid_arrive(bar, target, gridDim.x);
+        win_arrive<CL>(bar, target);
         /* the previous substep's targets (nobody reads or writes that buffer
          * until every CTA has passed the next barrier); warp 1 also takes
          * warp 0's */
@@ -956,7 +981,7 @@ __global__ void __launch_bounds__(1024, 1)
                 }
             }
         }
-        if (!grid_wait(bar, target, timeoutNs)) {
+        if (!win_wait<CL>(bar, target, timeoutNs)) {
             alive = false;
             break;
         }
@@ -998,9 +1023,9 @@ __global__ void __launch_bounds__(1024, 1)
 
         /* perform -> next check barrier */
         __syncthreads();
-        grid_arrive(bar, target, gridDim.x);
+        win_arrive<CL>(bar, target);
         if (k + 1u < k1 && threadIdx.x >= 32) prep(dnext);
-        if (!grid_wait(bar, target, timeoutNs)) {
+        if (!win_wait<CL>(bar, target, timeoutNs)) {
             alive = false;
             break;
         }
@@ -1023,12 +1048,18 @@ __global__ void __launch_bounds__(1024, 1)
 
 /* the windowed shapes: items in flight per thread in the check phase; the
  * CTA size is chosen at configuration to pack the CTA's items tightly */
-constexpr int kWinU[3] = {1, 2, 4};
+constexpr int kWinU[5] = {1, 2, 4, 2, 2};
+/* windowed variants 3 and 4 (shapes 9, 10): the launch is one cluster of
+ * 8 or 16 CTAs, for systems small enough that each CTA holds few monomers */
+constexpr int kWinCluster[5] = {0, 0, 0, 8, 16};
 
 template <int RNG>
 const void *win_kernel(int i)
 {
-    return i == 0 ? (const void *)k_sweep_w<RNG, 1> : i == 1 ? (const void *)k_sweep_w<RNG, 2> : (const void *)k_sweep_w<RNG, 4>;
+    return i == 0   ? (const void *)k_sweep_w<RNG, 1>
+           : i == 1 ? (const void *)k_sweep_w<RNG, 2>
+           : i == 2 ? (const void *)k_sweep_w<RNG, 4>
+                    : (const void *)k_sweep_w<RNG, 2, true>;
 }
 
 /* rounds grid barriers expecting `expected` CTAs; with expected > gridDim.x
@@ -1576,13 +1607,15 @@ struct Engine {
         return true;
     }
 
-    /* the windowed kernel (shape 6 + variant): one CTA per SM; positions,
-     * directions and both candidate lists in shared memory */
+    /* the windowed kernel (shape 6 + variant): one CTA per SM (variants
+     * 0..2) or one cluster of 8 or 16 CTAs (3, 4); positions, directions and
+     * both candidate lists in shared memory */
     template <int RNG>
     bool configureWindowed(int smCount, size_t smemLimit, int variant)
     {
         if (nSpecies > kWinMaxSpecies) return false;
-        const uint32_t grid = (uint32_t)smCount;
+        const uint32_t cluster = (uint32_t)kWinCluster[variant];
+        const uint32_t grid = cluster ? cluster : (uint32_t)smCount;
         const uint32_t per = (nmax + grid - 1) / grid + 1u;
         const uint32_t W = (per + 15u) & ~15u;
         /* fewest rounds of U items per thread at <= 1024 threads (plus
@@ -1602,6 +1635,26 @@ struct Engine {
         int fit = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, fn, (int)threads, smem));
         if (fit < 1) return false;
+        if (cluster) {
+            if (cluster > 8) CK(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(cluster);
+            cfg.blockDim = dim3(threads);
+            cfg.dynamicSmemBytes = smem;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = cluster;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            int clusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&clusters, fn, &cfg) != cudaSuccess) {
+                (void)cudaGetLastError();
+                return false;
+            }
+            if (clusters < 1) return false;
+        }
         sweepGrid = (int)grid;
         sweepCap = W;
         sweepSmem = smem;
@@ -1675,6 +1728,22 @@ struct Engine {
             const void *wf = rng == BFM_RNG_SARU     ? win_kernel<RNG_SARU>(v)
                              : rng == BFM_RNG_PHILOX ? win_kernel<RNG_PHILOX>(v)
                                                      : win_kernel<RNG_INTHASH>(v);
+            if (kWinCluster[v]) { /* one cluster: hardware cluster barriers */
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3((unsigned)sweepGrid);
+                cfg.blockDim = dim3((unsigned)sweepThreads);
+                cfg.dynamicSmemBytes = sweepSmem;
+                cfg.stream = stream;
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeClusterDimension;
+                at[0].val.clusterDim.x = (unsigned)sweepGrid;
+                at[0].val.clusterDim.y = 1;
+                at[0].val.clusterDim.z = 1;
+                cfg.attrs = at;
+                cfg.numAttrs = 1;
+                CK(cudaLaunchKernelExC(&cfg, wf, wargs));
+                return;
+            }
             CK(cudaLaunchCooperativeKernel(wf, dim3(sweepGrid), dim3(sweepThreads), wargs, sweepSmem, stream));
             return;
         }
@@ -1815,7 +1884,7 @@ struct Engine {
         /* candidates: automatic first, then every other shape that fits */
         std::vector<std::pair<int, int>> cand = {{-1, 0}};
         const int autoMode = sweepMode;
-        for (int sh : {6, 7, 8, 1, 2})
+        for (int sh : {6, 7, 8, 9, 10, 1, 2})
             if (sh != autoMode) cand.push_back({sh, 0});
         cand.push_back({autoMode >= SWEEP_WINDOWED ? autoMode : 7, 1});
         const uint32_t piece = std::max<uint32_t>(1, m / (uint32_t)(cand.size() + 1) / nSpecies) * nSpecies;
@@ -2591,7 +2660,7 @@ int bfm_time_kernels(bfm_handle *h, uint32_t nmcs, double *ms, uint64_t *launche
 int bfm_set_sweep_shape(bfm_handle *h, int shape)
 {
     GUARD(h, {
-        if (shape < -1 || shape > 8) throw InvalidArgument("sweep shape must be -1 (automatic) or 0..8");
+        if (shape < -1 || shape > 10) throw InvalidArgument("sweep shape must be -1 (automatic) or 0..10");
         h->e.forcedShape = shape;
         if (h->e.initialized) h->e.configureSweep();
     });
