@@ -549,6 +549,10 @@ def live_compare(n_systems: int = 2048, mcs: int = 200000, every: int = 1000, te
     wall_l, ran_l, ser_l, moves_l, dev_l = live_run(test_sys, seeds, budgets, every, rec, max_mcs=mcs, order=order, gpu=gpu)
     est_l = np.array([window_estimate(s, float(r)) for s, r in zip(ser_l, ran_l)])
     rel_l = (est_l - truth) / truth
+    # the live runs start from the recorded systems' initial states with the
+    # same seeds, so (bit-exact simulation) their R_e^2 series are prefixes of
+    # the recorded ones
+    prefix = all(np.array_equal(sl["re2"], series[i]["re2"][:len(sl["re2"])]) for sl, i in zip(ser_l, te_a))
     # the plain fixed budget of equal bias, from the recorded trajectories (a
     # plain run of B MCS is their prefix), then run live
     target = max(abs(float(rel_l.mean())), 0.005)
@@ -589,6 +593,7 @@ def live_compare(n_systems: int = 2048, mcs: int = 200000, every: int = 1000, te
         "solo": {"moves_per_s": solo, "wall_s_estimate": solo_wall},
         "systems_per_hour": {"learned": len(te_a) / wall_l * 3600.0, "plain": len(te_a) / wall_p * 3600.0,
                              "solo": (len(te_a) / solo_wall * 3600.0) if solo_wall else None},
+        "live_runs_reproduce_the_record": bool(prefix),
         "ratio_learned_vs_plain": wall_p / wall_l,
         "ratio_learned_vs_solo": (solo_wall / wall_l) if solo_wall else None,
     }

@@ -92,6 +92,23 @@ def test_pipeline_and_what_the_network_adds():
     assert rep["test_rmse"][key] < rep["test_rmse_constant_predictor"][key]
 
 
+@pytest.mark.gpu
+def test_live_schedule_on_the_gpu():
+    """The live learned schedule on a small ensemble (384 systems of edges
+    32..64, molecules of 16..96 monomers, 40,000 MCS recorded): the live
+    runs reproduce the recorded trajectories exactly (bit-exact batched
+    simulation from the same seeds), the drift judge ran, and the learned
+    schedule's ensemble R_e^2/N stays within 2% of the full-length runs.
+    The measured systems-per-hour ratio is reported by bench.py --schedule
+    on the full ensemble; here it only has to be positive."""
+    rep = sch.live_compare(n_systems=384, mcs=40000, every=500, epochs=200, seed=4, boxes=(32, 48, 64), n_range=(16, 96))
+    assert rep["live_runs_reproduce_the_record"]
+    assert rep["test_systems_assessed"] >= 20
+    assert abs(rep["learned"]["ensemble_re2_per_n_vs_full"]) <= 0.02
+    assert rep["learned"]["wall_s"] > 0 and rep["plain"]["wall_s"] > 0 and rep["ratio_learned_vs_plain"] > 0
+    assert rep["learned"]["mean_mcs"] <= 40000
+
+
 def test_driver_logic_with_a_synthetic_record(monkeypatch):
     """schedule.run end to end on the CPU: the batched recorder is replaced by
     synthetic series whose relaxation grows with N, the network by a
