@@ -167,11 +167,22 @@ int bfm_batch_initialize(bfm_batch *b);
  * `size` CTAs: 2, 4 (default; 1 also selects it) or 8; 0 runs every system
  * on one CTA.  Every size gives the same trajectories. */
 int bfm_batch_set_clusters(bfm_batch *b, int size);
-/* autotuner: the next bfm_batch_run times cluster sizes 4, 2, 8 and off on
- * four trial launches (each an eighth of the longest pending work, 2 .. 50
- * MCS; part of the run, same trajectories) and keeps the fastest per
- * attempted move; the default 4 stays unless another is more than 3% faster */
+/* autotuner: the next bfm_batch_run times, on trial launches (each an
+ * eighth of the longest pending work, 2 .. 50 MCS; part of the run, same
+ * trajectories), first the cluster sizes 4, 2, 8 and off, then 1 and 4
+ * monomers per thread in flight against the default 2, then the cluster
+ * kernel also for systems of 48^3..64^3 sites (whose lattices otherwise sit
+ * in one CTA's shared memory); at every stage the default stays unless a
+ * candidate is more than 3% faster per attempted move.  Trials that affect
+ * no system of the batch are skipped. */
 int bfm_batch_set_autotune(bfm_batch *b, int on);
+/* fix the tile shape by hand: monomers in flight per thread (1, 2, 4) and
+ * whether systems above 32^3 sites also go to the cluster kernel */
+int bfm_batch_set_shape(bfm_batch *b, int in_flight, int clusters_from_48);
+/* the shape in use and the autotuner's seven trials (ns per attempted move,
+ * 0 = skipped; order as in bfm_batch_set_autotune); any pointer may be NULL */
+int bfm_batch_get_tuning(const bfm_batch *b, int *cluster_size, int *in_flight, uint32_t *cluster_above_words, int *tuned,
+                         double *trial_ns_per_move7);
 /* the cluster size in use, whether the autotuner has chosen it, and its four
  * trial times (ns per attempted move, sizes 4, 2, 8, off; any pointer may be NULL) */
 int bfm_batch_get_clusters(const bfm_batch *b, int *size, int *tuned, double *trial_ns_per_move4);

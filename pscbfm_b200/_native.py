@@ -122,6 +122,8 @@ _SIGS = {
     "bfm_batch_info": (_c.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "bfm_set_sweep_autotune": (_c.c_int, [_P, _c.c_int]),
     "bfm_get_sweep_tuning": (_c.c_int, [_P, _P, _P, _P, _P, _P, _P, _c.c_uint32]),
+    "bfm_batch_set_shape": (_c.c_int, [_P, _c.c_int, _c.c_int]),
+    "bfm_batch_get_tuning": (_c.c_int, [_P, _P, _P, _P, _P, _P]),
     "bfm_mlp_create": (_c.c_int, [_c.c_int, _c.c_uint32, _c.c_uint32, _c.c_uint32, _c.c_uint64, _c.POINTER(_P)]),
     "bfm_mlp_destroy": (_c.c_int, [_P]),
     "bfm_mlp_last_error": (_c.c_char_p, [_P]),

@@ -78,6 +78,21 @@ class Batch:
         self._check(self._lib.bfm_batch_get_clusters(self._h, ctypes.byref(size), ctypes.byref(tuned), ns.ctypes.data))
         return {"size": size.value, "tuned": bool(tuned.value), "trial_ns_per_move": dict(zip((4, 2, 8, 0), ns.tolist()))}
 
+    def set_shape(self, in_flight: int = 2, clusters_from_48: bool = False):
+        """monomers per thread in flight (1, 2, 4); systems of 48^3..64^3 on clusters too"""
+        self._check(self._lib.bfm_batch_set_shape(self._h, int(in_flight), int(bool(clusters_from_48))))
+
+    def tuning(self) -> dict:
+        cs, f, tuned = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        above = ctypes.c_uint32()
+        ns = (ctypes.c_double * 7)()
+        self._check(self._lib.bfm_batch_get_tuning(self._h, ctypes.byref(cs), ctypes.byref(f), ctypes.byref(above),
+                                                   ctypes.byref(tuned), ns))
+        names = ("clusters 4", "clusters 2", "clusters 8", "clusters off", "1 in flight", "4 in flight",
+                 "clusters from 48^3")
+        return {"cluster_size": cs.value, "in_flight": f.value, "cluster_above_words": above.value,
+                "tuned": bool(tuned.value), "trial_ns_per_move": dict(zip(names, list(ns)))}
+
     def initialize(self):
         self._check(self._lib.bfm_batch_initialize(self._h))
         return self

@@ -47,7 +47,7 @@ namespace ens {
 
 constexpr int kThreads = 512;
 constexpr uint32_t kMaxSpecies = 16;
-constexpr int kInFlight = 2; /* monomers per thread in flight in the check phase (4: 1.5% slower) */
+constexpr int kInFlight = 2; /* default monomers per thread in flight in the check phase (1 and 4: autotuner candidates) */
 constexpr uint32_t kSmemLatWords = 8192; /* 64^3 sites: lattice and targets of smaller systems in shared memory */
 
 /* one system, read-only during a launch */
@@ -169,7 +169,7 @@ __device__ __forceinline__ void group_sync()
  * stride, ... of every species slab (stride = threads sharing the system);
  * the leader thread of each CTA draws the colour / seed sequence into its
  * CTA's shared copy (every CTA of a cluster draws the same sequence) */
-template <bool CL>
+template <bool CL, int IF>
 __device__ __forceinline__ void advance(const SysDesc &s, uint32_t *st, const Work wk, uint32_t *lat, uint32_t *tmp, bool inSmem,
                                         uint32_t lw, uint32_t first, uint32_t stride, const Arrays &A, uint32_t &s_sp,
                                         uint32_t &s_seed, unsigned long long &s_att, bool leader, unsigned int &myCand,
@@ -193,13 +193,13 @@ __device__ __forceinline__ void advance(const SysDesc &s, uint32_t *st, const Wo
                 const uint32_t off = base + s.spOff[sp], cnt = s.spOff[sp + 1] - s.spOff[sp];
                 if (leader && countAtt) s_att += cnt;
 
-                /* check (.cu:930-1028), kInFlight monomers in flight per thread */
-                for (uint32_t i0 = first; i0 < cnt; i0 += (uint32_t)kInFlight * stride) {
-                    uint32_t slot[kInFlight], r0[kInFlight], r1[kInFlight], dg[kInFlight];
-                    int dir[kInFlight];
-                    bool live[kInFlight], ok[kInFlight];
+                /* check (.cu:930-1028), IF monomers in flight per thread */
+                for (uint32_t i0 = first; i0 < cnt; i0 += (uint32_t)IF * stride) {
+                    uint32_t slot[IF], r0[IF], r1[IF], dg[IF];
+                    int dir[IF];
+                    bool live[IF], ok[IF];
 #pragma unroll
-                    for (int u = 0; u < kInFlight; ++u) {
+                    for (int u = 0; u < IF; ++u) {
                         const uint32_t i = i0 + (uint32_t)u * stride;
                         live[u] = i < cnt;
                         slot[u] = off + (live[u] ? i : 0u);
@@ -208,27 +208,27 @@ __device__ __forceinline__ void advance(const SysDesc &s, uint32_t *st, const Wo
                         ok[u] = live[u];
                     }
 #pragma unroll
-                    for (int u = 0; u < kInFlight; ++u) {
+                    for (int u = 0; u < IF; ++u) {
                         dir[u] = direction(draw_any(s.rng, seed, iter, i0 + (uint32_t)u * stride, iterHi));
                         bool w;
                         r1[u] = wmove(r0[u], dir[u], s, w);
                     }
                     uint32_t dmax = 0;
 #pragma unroll
-                    for (int u = 0; u < kInFlight; ++u) dmax = dg[u] > dmax ? dg[u] : dmax;
+                    for (int u = 0; u < IF; ++u) dmax = dg[u] > dmax ? dg[u] : dmax;
                     for (uint32_t j = 0; j < dmax; ++j) {
 #pragma unroll
-                        for (int u = 0; u < kInFlight; ++u)
+                        for (int u = 0; u < IF; ++u)
                             if (ok[u] && j < dg[u]) {
                                 const uint32_t code = zbond(A.pos[A.nbr[(size_t)j * A.T + slot[u]]], r1[u]);
                                 if ((s.forbidden[code >> 5] >> (code & 31u)) & 1u) ok[u] = false;
                             }
                     }
 #pragma unroll
-                    for (int u = 0; u < kInFlight; ++u)
+                    for (int u = 0; u < IF; ++u)
                         if (ok[u]) ok[u] = !face9(lat, r0[u], dir[u], s);
 #pragma unroll
-                    for (int u = 0; u < kInFlight; ++u)
+                    for (int u = 0; u < IF; ++u)
                         if (live[u]) {
                             if (ok[u]) {
                                 atomicOr(tmp + (r1[u] >> 5), 1u << (r1[u] & 31u));
@@ -289,6 +289,7 @@ __device__ __forceinline__ void advance(const SysDesc &s, uint32_t *st, const Wo
 
 }
 
+template <int IF>
 __global__ void __launch_bounds__(kThreads, 2)
     k_batch(const SysDesc *__restrict__ desc, const Work *__restrict__ work, const uint32_t *__restrict__ order,
             uint32_t nOrder, unsigned int *next, Arrays A)
@@ -327,7 +328,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 
         const Work wk = work[sid];
         unsigned int myCand = 0, myAcc = 0;
-        advance<false>(s, st, wk, lat, tmp, inSmem, lw, tid, blockDim.x, A, s_sp, s_seed, s_att, tid == 0, myCand, myAcc);
+        advance<false, IF>(s, st, wk, lat, tmp, inSmem, lw, tid, blockDim.x, A, s_sp, s_seed, s_att, tid == 0, myCand, myAcc);
 
         /* write back */
         atomicAdd(&s_cand, (unsigned long long)myCand);
@@ -370,6 +371,7 @@ __device__ __forceinline__ uint32_t cluster_index()
     return r;
 }
 
+template <int IF>
 __global__ void __launch_bounds__(kThreads, 2)
     k_batch_cl(const SysDesc *__restrict__ desc, const Work *__restrict__ work, const uint32_t *__restrict__ order,
                uint32_t nOrder, unsigned int *next, uint32_t *clusterItem, Arrays A)
@@ -404,8 +406,8 @@ __global__ void __launch_bounds__(kThreads, 2)
         cluster_barrier();
         const Work wk = work[sid];
         unsigned int myCand = 0, myAcc = 0;
-        advance<true>(s, st, wk, lat, tmp, false, lw, first, stride, A, s_sp, s_seed, s_att, tid == 0, myCand, myAcc,
-                      rank == 0);
+        advance<true, IF>(s, st, wk, lat, tmp, false, lw, first, stride, A, s_sp, s_seed, s_att, tid == 0, myCand, myAcc,
+                          rank == 0);
         atomicAdd(&s_cand, (unsigned long long)myCand);
         atomicAdd(&s_acc, (unsigned long long)myAcc);
         if (rank == 0)
@@ -549,6 +551,22 @@ struct Pending {
     std::vector<uint32_t> r250; /* 251 words */
 };
 
+/* the kernels of one monomers-in-flight count */
+inline const void *batchKernel(int f)
+{
+    return f == 1 ? (const void *)k_batch<1> : f == 4 ? (const void *)k_batch<4> : (const void *)k_batch<2>;
+}
+inline const void *clusterKernel(int f)
+{
+    return f == 1 ? (const void *)k_batch_cl<1> : f == 4 ? (const void *)k_batch_cl<4> : (const void *)k_batch_cl<2>;
+}
+
+/* the autotuner's trials, in order: cluster sizes 4, 2, 8, off (2 in
+ * flight); then 1 and 4 monomers in flight with the chosen size; then the
+ * cluster kernel also for systems above 32^3 sites */
+constexpr int kTrials = 7;
+constexpr uint32_t kClusterAboveLow = 1024;
+
 struct Batch {
     int gpu = 0;
     cudaStream_t stream = nullptr;
@@ -593,7 +611,10 @@ struct Batch {
     cudaEvent_t evFork = nullptr, evJoin = nullptr, evT0 = nullptr, evT1 = nullptr;
     uint32_t *d_clItem = nullptr;
     int clusterSize = 4;     /* CTAs per system with a global-memory lattice; 0: one CTA */
-    bool autotune = false;   /* time each cluster size on the first launches of a run, keep the fastest */
+    int inFlight = kInFlight; /* monomers per thread in flight in the check phase: 1, 2 or 4 */
+    uint32_t clusterAbove = kSmemLatWords; /* systems with more lattice words go to the cluster kernel */
+    bool autotune = false;   /* time the launch shapes on the first launches of a run, keep the fastest */
+    double tunedNs = 0;      /* ns per attempted move of the configuration chosen so far */
     bool tuned = false;
     std::vector<double> trialNsPerMove; /* per candidate of the autotuner */
 
@@ -846,12 +867,15 @@ struct Batch {
         balloc(d_iota, T); balloc(d_perm, T); balloc(d_inv, T);
         balloc(d_keys, T); balloc(d_keys2, T);
         int perSm = 0;
-        BCK(cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * kSmemLatWords * 4)));
-        BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_batch, kThreads, 2 * kSmemLatWords * 4));
+        for (int f : {1, 2, 4})
+            BCK(cudaFuncSetAttribute(batchKernel(f), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * kSmemLatWords * 4)));
+        BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_batch<kInFlight>, kThreads, 2 * kSmemLatWords * 4));
         int sms = 0;
         BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, gpu));
         grid = std::max(1, perSm) * sms;
-        if (maxLatWords > kSmemLatWords) balloc(d_tmp, (size_t)grid * maxLatWords);
+        /* target scratch of the systems the cluster kernel may take (those
+         * above 32^3 sites when the autotuner lowers the threshold) */
+        if (maxLatWords > kClusterAboveLow) balloc(d_tmp, (size_t)grid * maxLatWords);
         balloc(d_clItem, (size_t)grid / 2 + 1);
         size_t bytes = 0;
         BCK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, d_keys, d_keys2, d_iota, d_perm, (int)T, 0, 64, stream));
@@ -923,11 +947,41 @@ struct Batch {
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         int n = 0;
-        if (cudaOccupancyMaxActiveClusters(&n, k_batch_cl, &cfg) != cudaSuccess) {
+        if (cudaOccupancyMaxActiveClusters(&n, clusterKernel(inFlight), &cfg) != cudaSuccess) {
             (void)cudaGetLastError();
             return 0;
         }
         return n;
+    }
+
+    /* after trial t: at the end of a stage, keep the stage's default unless
+     * a candidate is more than 3% faster per attempted move (skipped trials
+     * are recorded as 0 and not candidates) */
+    void finishTrial(size_t t)
+    {
+        const std::vector<double> &ns = trialNsPerMove;
+        static const int kCand[4] = {4, 2, 8, 0};
+        if (t == 3) {
+            size_t best = 0;
+            for (size_t c = 1; c < 4; ++c)
+                if (ns[c] > 0 && ns[c] < 0.97 * ns[best]) best = c;
+            clusterSize = kCand[best];
+            tunedNs = ns[best];
+        } else if (t == 5) {
+            int f = kInFlight;
+            double b = tunedNs;
+            if (ns[4] > 0 && ns[4] < 0.97 * b) { f = 1; b = ns[4]; }
+            if (ns[5] > 0 && ns[5] < 0.97 * b) { f = 4; b = ns[5]; }
+            inFlight = f;
+            tunedNs = b;
+        } else if (t == 6) {
+            if (ns[6] > 0 && ns[6] < 0.97 * tunedNs) {
+                clusterAbove = kClusterAboveLow;
+                if (clusterSize == 0) clusterSize = 4;
+                tunedNs = ns[6];
+            }
+            tuned = true;
+        }
     }
 
     /* every system advances by mcs[s] MCS */
@@ -943,17 +997,39 @@ struct Batch {
         std::vector<uint32_t> order;
         lastLaunches = 0;
         lastAttempts = 0;
-        /* the autotuner's candidates; only systems with a global-memory
-         * lattice are affected, and every choice gives the same trajectory */
+        /* the autotuner's candidates (every choice gives the same
+         * trajectories); a cluster-size trial only matters with systems
+         * above 64^3 sites, the threshold trial with systems of 48^3..64^3 */
         static const int kCand[4] = {4, 2, 8, 0};
-        bool anyBig = false;
-        for (const SysDesc &d : desc) anyBig |= d.latWords > kSmemLatWords;
-        if (autotune && !tuned && !anyBig) tuned = true;
-        size_t trial = autotune && !tuned ? trialNsPerMove.size() : 4;
+        bool anyBig = false, anyMid = false;
+        for (const SysDesc &d : desc) {
+            anyBig |= d.latWords > kSmemLatWords;
+            anyMid |= d.latWords > kClusterAboveLow && d.latWords <= kSmemLatWords;
+        }
+        size_t trial = autotune && !tuned ? trialNsPerMove.size() : (size_t)kTrials;
+        auto applies = [&](size_t t) { return t == 0 || (t < 4 ? anyBig : t < 6 ? true : anyMid); };
         BCK(cudaEventRecord(ev0, stream));
         for (;;) {
-            const bool trying = trial < 4;
-            int cs = trying ? kCand[trial] : clusterSize;
+            while (trial < (size_t)kTrials && !applies(trial)) {
+                trialNsPerMove.push_back(0.0); /* skipped: affects no system of this batch */
+                finishTrial(trial++);
+            }
+            const bool trying = trial < (size_t)kTrials;
+            int cs = clusterSize, IF = inFlight;
+            uint32_t above = clusterAbove;
+            if (trying) {
+                if (trial < 4) {
+                    cs = kCand[trial];
+                    IF = kInFlight;
+                } else if (trial < 6) {
+                    IF = trial == 4 ? 1 : 4;
+                } else {
+                    above = kClusterAboveLow;
+                    if (cs == 0) cs = 4;
+                }
+            }
+            const int savedIF = inFlight;
+            inFlight = IF; /* activeClusters() asks for this count's kernel */
             bool unlaunchable = false;
             if (cs > 0 && activeClusters(cs) == 0) {
                 if (!trying) throw Err("clusters of " + std::to_string(cs) + " CTAs cannot be launched on this GPU");
@@ -992,7 +1068,7 @@ struct Batch {
             /* systems with a global-memory lattice go to the cluster kernel
              * (first part of the order), the others to the single-CTA kernel */
             std::vector<uint32_t> big, small;
-            for (uint32_t sI : order) ((cs > 0 && desc[sI].latWords > kSmemLatWords) ? big : small).push_back(sI);
+            for (uint32_t sI : order) ((cs > 0 && desc[sI].latWords > above) ? big : small).push_back(sI);
             order = big;
             order.insert(order.end(), small.begin(), small.end());
             BCK(cudaMemcpyAsync(d_work, hw.data(), S * sizeof(Work), cudaMemcpyHostToDevice, stream));
@@ -1018,17 +1094,28 @@ struct Batch {
                 attr[0].val.clusterDim.z = 1;
                 cfg.attrs = attr;
                 cfg.numAttrs = 1;
-                BCK(cudaLaunchKernelEx(&cfg, k_batch_cl, (const SysDesc *)d_desc, (const Work *)d_work, (const uint32_t *)d_order,
-                                       (uint32_t)big.size(), d_next, d_clItem, A));
+                const SysDesc *a0 = d_desc;
+                const Work *a1 = d_work;
+                const uint32_t *a2 = d_order;
+                uint32_t a3 = (uint32_t)big.size();
+                unsigned int *a4 = d_next;
+                uint32_t *a5 = d_clItem;
+                void *args[] = {&a0, &a1, &a2, &a3, &a4, &a5, &A};
+                BCK(cudaLaunchKernelExC(&cfg, clusterKernel(IF), args));
                 ++lastLaunches;
             }
             if (!small.empty()) {
                 const int g = (int)std::min<size_t>((size_t)grid, small.size());
-                k_batch<<<g, kThreads, 2 * kSmemLatWords * 4, stream2>>>(d_desc, d_work, d_order + big.size(),
-                                                                          (uint32_t)small.size(), d_next + 1, A);
-                BCK(cudaGetLastError());
+                const SysDesc *a0 = d_desc;
+                const Work *a1 = d_work;
+                const uint32_t *a2 = d_order + big.size();
+                uint32_t a3 = (uint32_t)small.size();
+                unsigned int *a4 = d_next + 1;
+                void *args[] = {&a0, &a1, &a2, &a3, &a4, &A};
+                BCK(cudaLaunchKernel(batchKernel(IF), dim3((unsigned)g), dim3(kThreads), args, 2 * kSmemLatWords * 4, stream2));
                 ++lastLaunches;
             }
+            inFlight = savedIF;
             BCK(cudaEventRecord(evJoin, stream2));
             BCK(cudaStreamWaitEvent(stream, evJoin, 0));
             BCK(cudaEventRecord(evT1, stream));
@@ -1039,15 +1126,8 @@ struct Batch {
             if (trying) {
                 float tms = 0;
                 BCK(cudaEventElapsedTime(&tms, evT0, evT1));
-                trialNsPerMove.push_back(unlaunchable ? 1e30 : (moves ? tms * 1e6 / (double)moves : 0.0));
-                if (++trial == 4) {
-                    /* the default (4) stays unless another size is more than 3% faster */
-                    size_t best = 0;
-                    for (size_t c = 1; c < 4; ++c)
-                        if (trialNsPerMove[c] < 0.97 * trialNsPerMove[best]) best = c;
-                    clusterSize = kCand[best];
-                    tuned = true;
-                }
+                trialNsPerMove.push_back(unlaunchable ? 1e30 : (moves ? tms * 1e6 / (double)moves : 1e30));
+                finishTrial(trial++);
             }
             for (uint32_t sI : order) {
                 lastAttempts += (uint64_t)hw[sI].steps * desc[sI].n;
@@ -1240,6 +1320,18 @@ int bfm_batch_set_autotune(bfm_batch *h, int on)
         h->b.autotune = on != 0;
         h->b.tuned = false;
         h->b.trialNsPerMove.clear();
+        h->b.inFlight = bfm::ens::kInFlight;
+        h->b.clusterAbove = bfm::ens::kSmemLatWords;
+    });
+}
+
+int bfm_batch_set_shape(bfm_batch *h, int in_flight, int clusters_from_48)
+{
+    BGUARD(h, {
+        if (in_flight != 1 && in_flight != 2 && in_flight != 4) throw bfm::ens::ArgErr("monomers in flight must be 1, 2 or 4");
+        h->b.inFlight = in_flight;
+        h->b.clusterAbove = clusters_from_48 ? bfm::ens::kClusterAboveLow : bfm::ens::kSmemLatWords;
+        h->b.autotune = false;
     });
 }
 
@@ -1250,6 +1342,21 @@ int bfm_batch_get_clusters(const bfm_batch *h, int *size, int *tuned, double *tr
     if (tuned) *tuned = h->b.tuned ? 1 : 0;
     if (trial_ns_per_move4)
         for (size_t c = 0; c < 4; ++c) trial_ns_per_move4[c] = c < h->b.trialNsPerMove.size() ? h->b.trialNsPerMove[c] : 0.0;
+    return BFM_OK;
+}
+
+int bfm_batch_get_tuning(const bfm_batch *h, int *cluster_size, int *in_flight, uint32_t *cluster_above_words, int *tuned,
+                         double *trial_ns_per_move7)
+{
+    if (!h) return BFM_EINVAL;
+    const auto &b = h->b;
+    if (cluster_size) *cluster_size = b.clusterSize;
+    if (in_flight) *in_flight = b.inFlight;
+    if (cluster_above_words) *cluster_above_words = b.clusterAbove;
+    if (tuned) *tuned = b.tuned ? 1 : 0;
+    if (trial_ns_per_move7)
+        for (size_t c = 0; c < (size_t)bfm::ens::kTrials; ++c)
+            trial_ns_per_move7[c] = c < b.trialNsPerMove.size() ? b.trialNsPerMove[c] : 0.0;
     return BFM_OK;
 }
 

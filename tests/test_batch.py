@@ -143,10 +143,38 @@ def test_batch_matches_oracle_and_single_runs(clusters):
         assert np.array_equal(u.getAllMonomerPositions(), b.positions(i)), f"system {i}"
     info = b.clusters()
     if clusters == "auto":
-        assert info["tuned"] and info["size"] in (0, 2, 4, 8)
+        assert info["size"] in (0, 2, 4, 8)
         assert all(v > 0 for v in info["trial_ns_per_move"].values())
+        t = b.tuning()
+        assert t["tuned"] and t["in_flight"] in (1, 2, 4) and t["cluster_above_words"] in (1024, 8192)
+        # every stage ran: the 64^3 system makes the threshold trial count too
+        assert all(v > 0 for v in t["trial_ns_per_move"].values())
     else:
         assert info["size"] == clusters
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("in_flight,from48", [(1, False), (4, False), (2, True), (4, True)])
+def test_batch_tile_shapes_match_oracle(in_flight, from48):
+    """every tile shape the autotuner may choose -- 1, 2 or 4 monomers in
+    flight per thread; systems of 48^3..64^3 sites on the cluster kernel
+    with a global-memory lattice instead of one CTA's shared memory -- gives
+    the oracle's trajectories"""
+    made = [(make(), rng, age, se) for make, rng, age, se in CASES]
+    b = pb.Batch()
+    b.set_shape(in_flight, from48)
+    states = [oracle.r250_state(300 + i) for i in range(len(made))]
+    for (s, rng, age, se), st in zip(made, states):
+        b.add(s, rng=rng, age=age, sort_every=se, r250_state=st)
+    b.initialize()
+    budgets = [np.array([7, 0, 11, 5, 23, 9, 14], np.uint32), np.full(len(made), 10, np.uint32)]
+    for m in budgets:
+        b.run(m)
+    for i, ((s, rng, age, se), st0) in enumerate(zip(made, states)):
+        o = _run_oracle(s, rng, age, se, st0.copy(), [budgets[0][i], budgets[1][i]])
+        assert np.array_equal(b.positions(i), o.positions()), f"system {i}"
+    t = b.tuning()
+    assert t["in_flight"] == in_flight and t["cluster_above_words"] == (1024 if from48 else 8192)
 
 
 @pytest.mark.gpu
