@@ -383,6 +383,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
     constexpr bool STAGE = MODE == SWEEP_STAGED;
     extern __shared__ __align__(16) unsigned char s_dyn[];
     __shared__ __align__(16) DirConst s_dir[6];
+    __shared__ __align__(16) DirK s_dk[6];
     __shared__ uint32_t s_forbid[16];
     __shared__ uint32_t s_after[6 * 16]; /* forbidden after a move in dir: bit (code) of row dir */
     __shared__ unsigned int s_cnt[2];     /* candidate count of the even / odd substep */
@@ -398,6 +399,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
 
     build_split_table(s_tab);
     build_dir_table(s_dir, s.g);
+    if (threadIdx.x < 6) s_dk[threadIdx.x] = dir_consts((int)threadIdx.x, s.g);
     if (threadIdx.x < 16) s_forbid[threadIdx.x] = s.bonds.forbidden[threadIdx.x];
     if (threadIdx.x < 96) {
         const uint32_t dir = threadIdx.x >> 4, w = threadIdx.x & 15u, ax = dir >> 1;
@@ -527,7 +529,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
             if (valid) {
                 if (!STAGE) dir = direction(draw<RNG>(d.seed, d.iter, i, d.iterHi));
                 const DirConst dc = s_dir[dir];
-                const FaceW fw = face_words(r0, dir, s.g);
+                const FaceW fw = face_k(r0, s_dk[dir]);
                 const uint32_t r1 = dstep(r0, dir, dc);
                 if (STORED) {
                     const uint32_t *after = s_after + dir * 16;
@@ -582,7 +584,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
                 const uint32_t slot = e.x & 0x0FFFFFFFu;
                 const uint32_t r0 = e.y;
                 const DirConst dc = s_dir[dir];
-                const FaceW fw = face_words(r0, dir, s.g);
+                const FaceW fw = face_k(r0, s_dk[dir]);
                 /* bond data of a possible move, loaded together with the probe */
                 uint32_t dgm = 0, q0 = 0, q1 = 0, v0 = 0, v1 = 0, c0 = 0, c1 = 0;
                 if (STORED) {
