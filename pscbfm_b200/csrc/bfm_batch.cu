@@ -49,6 +49,7 @@ constexpr int kThreads = 512;
 constexpr uint32_t kMaxSpecies = 16;
 constexpr int kInFlight = 2; /* default monomers per thread in flight in the check phase (1 and 4: autotuner candidates) */
 constexpr uint32_t kSmemLatWords = 8192; /* 64^3 sites: lattice and targets of smaller systems in shared memory */
+constexpr uint32_t kMaxCluster = 16;     /* CTAs of a cluster, at most */
 
 /* one system, read-only during a launch */
 struct SysDesc {
@@ -99,11 +100,28 @@ __device__ __forceinline__ uint32_t wmove(uint32_t a, int dir, const SysDesc &s,
     return wstep(a, dir >> 1, dir & 1, s, wrapped);
 }
 
-__device__ __forceinline__ bool bit(const uint32_t *lat, uint32_t c) { return (lat[c >> 5] >> (c & 31u)) & 1u; }
+/* Where a system's bit lattice lives: one array (global memory, or the
+ * CTA's own shared memory) ... */
+struct FlatLat {
+    uint32_t *p;
+    __device__ __forceinline__ uint32_t *at(uint32_t w) const { return p + w; }
+};
+/* ... or spread over the shared memory of the cluster's CTAs: word w in the
+ * CTA of rank w >> shift at index w & mask, reached through the generic
+ * address of that CTA's slice (distributed shared memory) */
+struct DistLat {
+    uint32_t *const *rank; /* per rank: generic address of its slice */
+    uint32_t shift, mask;
+    __device__ __forceinline__ uint32_t *at(uint32_t w) const { return rank[w >> shift] + (w & mask); }
+};
+
+template <class LAT>
+__device__ __forceinline__ bool bit(const LAT &lat, uint32_t c) { return (*lat.at(c >> 5) >> (c & 31u)) & 1u; }
 
 /* checkFront (.cu:420-869): any of the nine sites at r0 + 2*D[dir], -1..+1
  * along the two other axes */
-__device__ __forceinline__ bool face9(const uint32_t *lat, uint32_t r0, int dir, const SysDesc &s)
+template <class LAT>
+__device__ __forceinline__ bool face9(const LAT &lat, uint32_t r0, int dir, const SysDesc &s)
 {
     bool w;
     const uint32_t c = wmove(wmove(r0, dir, s, w), dir, s, w);
@@ -169,9 +187,10 @@ __device__ __forceinline__ void group_sync()
  * stride, ... of every species slab (stride = threads sharing the system);
  * the leader thread of each CTA draws the colour / seed sequence into its
  * CTA's shared copy (every CTA of a cluster draws the same sequence) */
-template <bool CL, int IF>
-__device__ __forceinline__ void advance(const SysDesc &s, uint32_t *st, const Work wk, uint32_t *lat, uint32_t *tmp, bool inSmem,
-                                        uint32_t lw, uint32_t first, uint32_t stride, const Arrays &A, uint32_t &s_sp,
+template <bool CL, int IF, class LAT>
+__device__ __forceinline__ void advance(const SysDesc &s, uint32_t *st, const Work wk, const LAT lat, const LAT tmp,
+                                        uint32_t *clearLocal, uint32_t clearWords, uint32_t clearFirst, uint32_t clearStride,
+                                        uint32_t first, uint32_t stride, const Arrays &A, uint32_t &s_sp,
                                         uint32_t &s_seed, unsigned long long &s_att, bool leader, unsigned int &myCand,
                                         unsigned int &myAcc, bool countAtt = true)
 {
@@ -231,7 +250,7 @@ __device__ __forceinline__ void advance(const SysDesc &s, uint32_t *st, const Wo
                     for (int u = 0; u < IF; ++u)
                         if (live[u]) {
                             if (ok[u]) {
-                                atomicOr(tmp + (r1[u] >> 5), 1u << (r1[u] & 31u));
+                                atomicOr(tmp.at(r1[u] >> 5), 1u << (r1[u] & 31u));
                                 ++myCand;
                             }
                             A.flags[slot[u]] = ok[u] ? (uint8_t)(dir[u] | 8) : (uint8_t)0;
@@ -252,10 +271,10 @@ __device__ __forceinline__ void advance(const SysDesc &s, uint32_t *st, const Wo
                     const uint32_t w0 = r0 >> 5, w1 = r1 >> 5;
                     const uint32_t b0 = 1u << (r0 & 31u), b1 = 1u << (r1 & 31u);
                     if (w0 == w1) {
-                        atomicXor(lat + w0, b0 | b1);
+                        atomicXor(lat.at(w0), b0 | b1);
                     } else {
-                        atomicXor(lat + w0, b0);
-                        atomicXor(lat + w1, b1);
+                        atomicXor(lat.at(w0), b0);
+                        atomicXor(lat.at(w1), b1);
                     }
                     A.pos[slot] = r1;
                     if (wrapped) A.img[(size_t)(dir >> 1) * A.T + slot] += (dir & 1) ? 1 : -1;
@@ -264,15 +283,16 @@ __device__ __forceinline__ void advance(const SysDesc &s, uint32_t *st, const Wo
                 }
                 group_sync<CL>();
 
-                /* clear this substep's targets: the whole buffer when it is in
-                 * shared memory, the candidates' words otherwise */
+                /* clear this substep's targets: this CTA's shared-memory part
+                 * of the buffer when it is in shared memory, the candidates'
+                 * words otherwise */
                 if (leader && !(iStep + 1 == wk.steps && sub + 1 == nSp)) {
                     s_sp = r250_next(st) % nSp;
                     s_seed = r250_next(st);
                 }
-                if (inSmem) {
-                    uint4 *t4 = reinterpret_cast<uint4 *>(tmp);
-                    for (uint32_t w = first; w < lw / 4; w += stride) t4[w] = make_uint4(0u, 0u, 0u, 0u);
+                if (clearLocal) {
+                    uint4 *t4 = reinterpret_cast<uint4 *>(clearLocal);
+                    for (uint32_t w = clearFirst; w < clearWords / 4; w += clearStride) t4[w] = make_uint4(0u, 0u, 0u, 0u);
                 } else {
                     for (uint32_t i = first; i < cnt; i += stride) {
                         const uint32_t slot = off + i;
@@ -280,7 +300,7 @@ __device__ __forceinline__ void advance(const SysDesc &s, uint32_t *st, const Wo
                         if (!(f & 8)) continue;
                         bool w;
                         const uint32_t r1 = (f & 16) ? A.pos[slot] : wmove(A.pos[slot], f & 7, s, w);
-                        tmp[r1 >> 5] = 0u;
+                        *tmp.at(r1 >> 5) = 0u;
                     }
                 }
                 group_sync<CL>();
@@ -328,7 +348,8 @@ __global__ void __launch_bounds__(kThreads, 2)
 
         const Work wk = work[sid];
         unsigned int myCand = 0, myAcc = 0;
-        advance<false, IF>(s, st, wk, lat, tmp, inSmem, lw, tid, blockDim.x, A, s_sp, s_seed, s_att, tid == 0, myCand, myAcc);
+        advance<false, IF>(s, st, wk, FlatLat{lat}, FlatLat{tmp}, inSmem ? tmp : nullptr, lw, tid, blockDim.x, tid, blockDim.x, A,
+                           s_sp, s_seed, s_att, tid == 0, myCand, myAcc);
 
         /* write back */
         atomicAdd(&s_cand, (unsigned long long)myCand);
@@ -371,17 +392,31 @@ __device__ __forceinline__ uint32_t cluster_index()
     return r;
 }
 
+/* generic address of the same shared-memory location in CTA `r` of the cluster */
+__device__ __forceinline__ uint32_t *cluster_map(uint32_t *p, uint32_t r)
+{
+    uint64_t q;
+    asm volatile("mapa.u64 %0, %1, %2;" : "=l"(q) : "l"(p), "r"(r));
+    return reinterpret_cast<uint32_t *>(q);
+}
+
 template <int IF>
 __global__ void __launch_bounds__(kThreads, 2)
     k_batch_cl(const SysDesc *__restrict__ desc, const Work *__restrict__ work, const uint32_t *__restrict__ order,
                uint32_t nOrder, unsigned int *next, uint32_t *clusterItem, Arrays A)
 {
+    extern __shared__ uint32_t dyn[]; /* this CTA's slices: kSmemLatWords occupation + kSmemLatWords targets */
     __shared__ SysDesc s;
     __shared__ uint32_t st[251];
     __shared__ uint32_t s_sp, s_seed;
     __shared__ unsigned long long s_cand, s_acc, s_att;
-    const uint32_t tid = threadIdx.x, rank = cluster_rank(), cid = cluster_index();
-    const uint32_t first = rank * blockDim.x + tid, stride = cluster_size() * blockDim.x;
+    __shared__ uint32_t *s_latRank[kMaxCluster], *s_tmpRank[kMaxCluster];
+    const uint32_t tid = threadIdx.x, rank = cluster_rank(), cid = cluster_index(), cs = cluster_size();
+    const uint32_t first = rank * blockDim.x + tid, stride = cs * blockDim.x;
+    if (tid < cs) {
+        s_latRank[tid] = cluster_map(dyn, tid);
+        s_tmpRank[tid] = cluster_map(dyn + kSmemLatWords, tid);
+    }
 
     for (;;) {
         if (rank == 0 && tid == 0) clusterItem[cid] = atomicAdd(next, 1u);
@@ -400,14 +435,32 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
         __syncthreads();
         const uint32_t lw = s.latWords;
-        uint32_t *lat = A.latPool + s.latOff;
-        uint32_t *tmp = A.tmpScratch + (size_t)cid * A.maxLatWords;
-        for (uint32_t w = first; w < lw; w += stride) tmp[w] = 0u;
-        cluster_barrier();
         const Work wk = work[sid];
         unsigned int myCand = 0, myAcc = 0;
-        advance<true, IF>(s, st, wk, lat, tmp, false, lw, first, stride, A, s_sp, s_seed, s_att, tid == 0, myCand, myAcc,
-                          rank == 0);
+        /* the lattices in the cluster's distributed shared memory when each
+         * CTA's share fits its slices, else in global memory */
+        const uint32_t slice = lw / cs;
+        if (slice * cs == lw && slice <= kSmemLatWords && (slice & (slice - 1)) == 0 && slice >= 4) {
+            const uint32_t *g = A.latPool + s.latOff + (size_t)rank * slice;
+            for (uint32_t w = tid; w < slice; w += blockDim.x) {
+                dyn[w] = g[w];
+                dyn[kSmemLatWords + w] = 0u;
+            }
+            cluster_barrier();
+            const uint32_t sh = 31u - __clz(slice);
+            advance<true, IF>(s, st, wk, DistLat{s_latRank, sh, slice - 1u}, DistLat{s_tmpRank, sh, slice - 1u},
+                              dyn + kSmemLatWords, slice, tid, blockDim.x, first, stride, A, s_sp, s_seed, s_att, tid == 0,
+                              myCand, myAcc, rank == 0);
+            uint32_t *gw = A.latPool + s.latOff + (size_t)rank * slice;
+            for (uint32_t w = tid; w < slice; w += blockDim.x) gw[w] = dyn[w];
+        } else {
+            uint32_t *lat = A.latPool + s.latOff;
+            uint32_t *tmp = A.tmpScratch + (size_t)cid * A.maxLatWords;
+            for (uint32_t w = first; w < lw; w += stride) tmp[w] = 0u;
+            cluster_barrier();
+            advance<true, IF>(s, st, wk, FlatLat{lat}, FlatLat{tmp}, nullptr, 0u, 0u, 1u, first, stride, A, s_sp, s_seed, s_att,
+                              tid == 0, myCand, myAcc, rank == 0);
+        }
         atomicAdd(&s_cand, (unsigned long long)myCand);
         atomicAdd(&s_acc, (unsigned long long)myAcc);
         if (rank == 0)
@@ -867,8 +920,10 @@ struct Batch {
         balloc(d_iota, T); balloc(d_perm, T); balloc(d_inv, T);
         balloc(d_keys, T); balloc(d_keys2, T);
         int perSm = 0;
-        for (int f : {1, 2, 4})
+        for (int f : {1, 2, 4}) {
             BCK(cudaFuncSetAttribute(batchKernel(f), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * kSmemLatWords * 4)));
+            BCK(cudaFuncSetAttribute(clusterKernel(f), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * kSmemLatWords * 4)));
+        }
         BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_batch<kInFlight>, kThreads, 2 * kSmemLatWords * 4));
         int sms = 0;
         BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, gpu));
@@ -939,6 +994,7 @@ struct Batch {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)cs);
         cfg.blockDim = dim3(kThreads);
+        cfg.dynamicSmemBytes = 2 * kSmemLatWords * 4;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
         attr[0].val.clusterDim.x = (unsigned)cs;
@@ -1085,7 +1141,7 @@ struct Batch {
                 cudaLaunchConfig_t cfg = {};
                 cfg.gridDim = dim3((unsigned)(clusters * (size_t)cs));
                 cfg.blockDim = dim3(kThreads);
-                cfg.dynamicSmemBytes = 0;
+                cfg.dynamicSmemBytes = 2 * kSmemLatWords * 4; /* distributed lattice slices */
                 cfg.stream = stream;
                 cudaLaunchAttribute attr[1];
                 attr[0].id = cudaLaunchAttributeClusterDimension;
