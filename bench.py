@@ -623,6 +623,9 @@ def run_reference(args, ranks):
                           f"one host thread driving the B200"}
         d2h = system.n * 16           # doCopyBack: mPolymerSystem->pop(), int4 per monomer (.cu:3468-3471)
         ms_per_step = dev_ms / args.steps
+        del ref                       # its destructor logs to stdout: before the JSON line, not after
+        import gc
+        gc.collect()
     else:
         clk = None
         what = {"c1": "128^3 dilute system"}.get(args.config, "256^3 melt")
