@@ -89,7 +89,9 @@ int bfm_initialize(bfm_handle *h);
 int bfm_run(bfm_handle *h, uint32_t nmcs);
 /* getMonomerPositionInX/Y/Z (.h:501-503) */
 int bfm_get_monomer_position(bfm_handle *h, uint32_t i, int32_t *x, int32_t *y, int32_t *z);
-/* all positions (unfolded, as doCopyBack .cu:3402-3484 returns them), 3*n int32 */
+/* all positions (unfolded, as doCopyBack .cu:3402-3484 returns them), 3*n
+ * int32; a page-locked buffer (cudaHostAlloc'd or registered) is filled by
+ * one device-to-host copy, any other through the engine's staging buffer */
 int bfm_get_positions(bfm_handle *h, int32_t *xyz, size_t n);
 
 /* ---- chain analysis on the device (the reference's AnalyzerMsd,

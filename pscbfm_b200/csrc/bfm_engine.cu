@@ -100,7 +100,6 @@ __host__ __device__ __forceinline__ size_t bc_index(uint32_t j, uint32_t slot, u
     return j < 2u ? 2u * (size_t)slot + j : (size_t)j * npad + slot;
 }
 __device__ __forceinline__ uint32_t *bc_pair(uint16_t *bcode) { return reinterpret_cast<uint32_t *>(bcode); }
-__device__ __forceinline__ const uint32_t *bc_pair(const uint16_t *bcode) { return reinterpret_cast<const uint32_t *>(bcode); }
 
 /* Filter statistics of the reference's "Stats" mode
  * (UpdaterGPUScBFM_AB_Type.cu:1033-1097, :1192-1216, :2917-2936): moves of a
@@ -985,7 +984,6 @@ __global__ void __launch_bounds__(1024, 1)
         for (uint32_t w = threadIdx.x - 32u; w < n; w += T - 32u)
             px[w] = (uint8_t)((uint32_t)direction(draw<RNG>(dn.seed, dn.iter, plo + w, dn.iterHi)) | ((uint32_t)sdeg[base + w] << 3));
     };
-    /* zero the target words of warp wi's candidates of the substep using buffer buf, list set p */
     /* the target lattice of buffer `buf` (0 or 1) */
     auto tgt = [&](uint32_t buf) -> LatAcc<DSM> {
         LatAcc<DSM> t = TA;
@@ -993,6 +991,7 @@ __global__ void __launch_bounds__(1024, 1)
         else t.p = TA.p + (size_t)buf * words;
         return t;
     };
+    /* zero the target words of warp wi's candidates of the substep using buffer buf, list set p */
     auto clear_targets = [&](uint32_t buf, uint32_t p, uint32_t wi) {
         const LatAcc<DSM> tp = tgt(buf);
         const uint2 *pl = lists + ((size_t)p * NW + wi) * seg;
@@ -2309,7 +2308,31 @@ struct Engine {
         CK(cudaStreamSynchronize(stream));
         hostPosValid = true;
     }
+
+    /* the unfolded positions straight into a caller's page-locked buffer:
+     * one unpack kernel and one device-to-host copy, no pass through the
+     * engine's own staging buffer (which stays as it was) */
+    void readbackTo(int32_t *dst)
+    {
+        if (!initialized) throw std::runtime_error("initialize must be called first");
+        const int blocks = (int)std::min<uint32_t>((npad + kThreads - 1) / kThreads, 148 * 16);
+        k_unpack<<<blocks, kThreads, 0, stream>>>(d_pos, d_img, d_s2o, npad, (int32_t)L[0], (int32_t)L[1], (int32_t)L[2], d_out);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(dst, d_out, 3 * (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+    }
 };
+
+/* whether host memory at p is page-locked (cudaHostAlloc'd or registered) */
+static bool host_pinned(const void *p)
+{
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
 
 /* ------------------------------------------- no-allocation colour substep
  *
@@ -2646,8 +2669,12 @@ int bfm_get_positions(bfm_handle *h, int32_t *xyz, size_t n)
     }
     GUARD(h, {
         if (!xyz || n != h->e.n) throw InvalidArgument("position buffer does not match the number of monomers");
-        h->e.readback();
-        std::memcpy(xyz, h->e.h_out, 3 * n * sizeof(int32_t));
+        if (!h->e.hostPosValid && host_pinned(xyz)) {
+            h->e.readbackTo(xyz);
+        } else {
+            h->e.readback();
+            std::memcpy(xyz, h->e.h_out, 3 * n * sizeof(int32_t));
+        }
     });
 }
 

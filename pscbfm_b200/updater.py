@@ -179,8 +179,13 @@ class UpdaterGPUScBFM_AB_Type:
                 for dz in range(-4, 4):
                     self.copyBondSet(dx, dy, dz, not allowed[(dx & 7) | ((dy & 7) << 3) | ((dz & 7) << 6)])
 
-    def getAllMonomerPositions(self) -> np.ndarray:
-        out = np.empty((self._n, 3), dtype=np.int32)
+    def getAllMonomerPositions(self, out: np.ndarray = None) -> np.ndarray:
+        """unfolded positions, (n, 3) int32; `out` (optional) is filled and
+        returned -- page-locked memory there takes one device-to-host copy"""
+        if out is None:
+            out = np.empty((self._n, 3), dtype=np.int32)
+        elif out.shape != (self._n, 3) or out.dtype != np.int32 or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous ({self._n}, 3) int32 array")
         self._check(self._lib.bfm_get_positions(self._h, out.ctypes.data, self._n))
         return out
 

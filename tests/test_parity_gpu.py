@@ -259,3 +259,25 @@ def test_shape_autotuner_keeps_the_trajectory(name):
     assert info["tuned"] and len(info["trials"]) >= 3
     assert all(t["ns_per_move"] > 0 for t in info["trials"])
     assert u.getLaunchInfo()["mode"] in {t["shape"] for t in info["trials"]}
+
+
+def test_positions_into_page_locked_buffer():
+    """a page-locked output buffer is filled by one device-to-host copy;
+    the positions equal those of the staging path and of the per-index
+    getters, before and after further runs"""
+    import torch
+    s = SYSTEMS["dense_chains"]
+    pb.r250_seed(77)
+    u = pb.UpdaterGPUScBFM_AB_Type().setup(s, rng=pb.Rng.Saru)
+    pinned_t = torch.empty((s.n, 3), dtype=torch.int32, pin_memory=True)
+    pinned = pinned_t.numpy()
+    for nmcs in (10, 25):
+        u.runSimulationOnGPU(nmcs)
+        pinned[:] = -1
+        got = u.getAllMonomerPositions(out=pinned)
+        assert got is pinned
+        want = u.getAllMonomerPositions()
+        assert np.array_equal(pinned, want)
+        assert [u.getMonomerPositionInX(7), u.getMonomerPositionInY(7), u.getMonomerPositionInZ(7)] == list(want[7])
+    with pytest.raises(ValueError):
+        u.getAllMonomerPositions(out=np.empty((s.n, 2), np.int32))
