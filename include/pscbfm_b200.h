@@ -276,10 +276,8 @@ int bfm_set_launch_mode(bfm_handle *h, int mode);
  * from the partners' positions, 1 = from stored bond codes, 2 = stored codes
  * with the CTA's slab segments staged in shared memory by bulk copies, 6..8 =
  * stored codes with the independent work of each substep done inside the
- * grid-barrier waits, 9, 10 the same on one cluster of 8 or 16 CTAs, 11,
- * 12 the same with the lattices and bond codes held in the cluster's
- * distributed shared memory (negative: -launch path of the per-substep
- * kernels);
+ * grid-barrier waits, 9, 10 the same on one cluster of 8 or 16 CTAs
+ * (negative: -launch path of the per-substep kernels);
  * CTAs, threads per CTA and dynamic shared memory per CTA */
 int bfm_get_launch_info(const bfm_handle *h, int *mode, int *grid, int *threads, size_t *smem_bytes);
 /* force a shape of the persistent kernel (tests, tuning): -1 automatic
@@ -287,16 +285,13 @@ int bfm_get_launch_info(const bfm_handle *h, int *mode, int *grid, int *threads,
  * candidate lists in global instead of shared memory; 6..8 windowed with
  * 1, 2, 4 items per thread in flight (one CTA per SM, grid barriers);
  * 9, 10 windowed with 2 in flight on one thread-block cluster of 8 or 16
- * CTAs (hardware cluster barriers; small systems); 11, 12 the same with the
- * occupation lattice, both target lattices and the bond codes sliced across
- * the shared memory of the cluster's CTAs for the whole launch (loaded at
- * its start, written back at its end; systems whose lattice fits on chip).
+ * CTAs (hardware cluster barriers; small systems).
  * BFM_ERUNTIME when the shape does not fit this system. */
 int bfm_set_sweep_shape(bfm_handle *h, int shape);
 /* launch-shape autotuner (no counterpart in the reference, whose launch
  * configuration is fixed, UpdaterGPUScBFM_AB_Type.cu:2952-2981): with `on`,
  * the first schedule chunk of the next run is split into equal trial
- * launches of the automatic shape, the windowed shapes 6..12, the stored and
+ * launches of the automatic shape, the windowed shapes 6..10, the stored and
  * staged shapes 1, 2 and the windowed shape with one more round of items per
  * thread (smaller CTAs), each timed with events; the trials are part of the
  * run (every shape gives the same trajectory) and the fastest per attempted

@@ -100,6 +100,7 @@ __host__ __device__ __forceinline__ size_t bc_index(uint32_t j, uint32_t slot, u
     return j < 2u ? 2u * (size_t)slot + j : (size_t)j * npad + slot;
 }
 __device__ __forceinline__ uint32_t *bc_pair(uint16_t *bcode) { return reinterpret_cast<uint32_t *>(bcode); }
+__device__ __forceinline__ const uint32_t *bc_pair(const uint16_t *bcode) { return reinterpret_cast<const uint32_t *>(bcode); }
 
 /* Filter statistics of the reference's "Stats" mode
  * (UpdaterGPUScBFM_AB_Type.cu:1033-1097, :1192-1216, :2917-2936): moves of a
@@ -706,95 +707,10 @@ struct WinLayout {
     __host__ __device__ size_t bytes() const { return lists() + (size_t)2 * (T / 32u) * seg() * 8u; }
 };
 
-/* Where the windowed kernel finds the occupation lattice, the target
- * lattices and the bond codes: global memory (DSM false), or -- for a
- * system that one cluster holds on chip -- slices in the distributed shared
- * memory of the cluster's CTAs, reached through the generic address of each
- * CTA's slice (DSM true).  64-bit lattice words: word w in rank w >> sh at
- * index w & mask. */
-template <bool DSM>
-struct LatAcc {
-    unsigned long long *p;                 /* global */
-    unsigned long long *const *rank;       /* distributed: per rank */
-    uint32_t sh, mask;
-    __device__ __forceinline__ unsigned long long *at(uint32_t w) const
-    {
-        if (DSM) return rank[w >> sh] + (w & mask);
-        return p + w;
-    }
-};
-/* bond codes: rows 0 and 1 of a slot in one 32-bit word, rows >= 2 as 16-bit
- * rows; distributed: slot s in rank s >> sh (per = 2^sh slots each), the
- * pair words first, then the rows >= 2 of per entries */
-template <bool DSM>
-struct BondAcc {
-    uint16_t *p;
-    uint32_t npad;
-    uint32_t *const *rank;
-    uint32_t sh, per;
-    __device__ __forceinline__ uint32_t *pair(uint32_t slot) const
-    {
-        if (DSM) return rank[slot >> sh] + (slot & (per - 1u));
-        return bc_pair(p) + slot;
-    }
-    __device__ __forceinline__ uint16_t *at(uint32_t j, uint32_t slot) const
-    {
-        if (DSM) {
-            uint32_t *b = rank[slot >> sh];
-            const uint32_t ls = slot & (per - 1u);
-            return j < 2u ? reinterpret_cast<uint16_t *>(b + ls) + j : reinterpret_cast<uint16_t *>(b + per) + (size_t)(j - 2u) * per + ls;
-        }
-        return p + bc_index(j, slot, npad);
-    }
-};
-
-/* occupied sites of a face in a lattice reached through an accessor */
-template <class LA>
-__device__ __forceinline__ unsigned long long split_occupied_a(const LA &L, const FaceW &fw, const unsigned long long *tab,
-                                                               uint32_t lane)
-{
-    const bool sb = fw.sb != 0u, sc = fw.sc != 0u;
-    const unsigned long long *tp = tab + (size_t)fw.t * kTabReplicas + (lane & (kTabReplicas - 1u));
-    constexpr size_t G = (size_t)192 * kTabReplicas;
-    unsigned long long o = *L.at(fw.w[0]) & tp[0];
-    if (sb) o |= *L.at(fw.w[1]) & tp[G];
-    if (sc) o |= *L.at(fw.w[2]) & tp[2 * G];
-    if (sb && sc) o |= *L.at(fw.w[3]) & tp[3 * G];
-    return o;
-}
-
-/* generic address of the same shared-memory location in CTA `r` of the cluster */
-template <typename T>
-__device__ __forceinline__ T *cluster_map(T *p, uint32_t r)
-{
-    uint64_t q;
-    asm volatile("mapa.u64 %0, %1, %2;" : "=l"(q) : "l"(p), "r"(r));
-    return reinterpret_cast<T *>(q);
-}
-
-/* shared-memory bytes of one CTA's slices of a cluster-resident system
- * (lattice, two target lattices, bond codes), and the slice sizes */
-struct DsmPlan {
-    uint32_t latSlice, bcPer;
-    size_t bytes;
-};
-__host__ __device__ inline DsmPlan dsm_plan(uint32_t latWords64, uint32_t npad, uint32_t maxdeg, uint32_t cs)
-{
-    DsmPlan d;
-    d.latSlice = latWords64 / cs;
-    uint32_t per = 1;
-    while (per * cs < npad) per <<= 1;
-    d.bcPer = per;
-    const uint32_t extraRows = maxdeg > 2 ? maxdeg - 2 : 0;
-    d.bytes = (size_t)3 * d.latSlice * 8 + (((size_t)per * 4 + (size_t)extraRows * per * 2 + 15) & ~(size_t)15);
-    return d;
-}
-
 /* apply an accepted move: lattice bits, position (shared memory), image
  * counter, own bond codes and the partners' codes of the bonds back
  * (per-axis negation) */
-template <class LA, class BA>
-__device__ __forceinline__ void apply_move(const Sys &s, const LA &lat, const BA &bc, uint32_t *spos, uint32_t slot, uint32_t r0,
+__device__ __forceinline__ void apply_move(const Sys &s, unsigned long long *lat, uint32_t *spos, uint32_t slot, uint32_t r0,
                                            int dir, const Geometry &geo, uint32_t dgm, uint32_t q0, uint32_t v0, uint32_t c0,
                                            uint32_t q1, uint32_t v1, uint32_t c1)
 {
@@ -805,27 +721,27 @@ __device__ __forceinline__ void apply_move(const Sys &s, const LA &lat, const BA
     const uint32_t w0 = r0 >> 6, w1 = r1 >> 6;
     const unsigned long long b0 = 1ull << (r0 & 63u), b1 = 1ull << (r1 & 63u);
     if (w0 == w1) {
-        atomicXor(lat.at(w0), b0 | b1);
+        atomicXor(lat + w0, b0 | b1);
     } else {
-        atomicXor(lat.at(w0), b0);
-        atomicXor(lat.at(w1), b1);
+        atomicXor(lat + w0, b0);
+        atomicXor(lat + w1, b1);
     }
     *spos = r1;
     const bool wrapped = (dir & 1) ? ((r1 & ma) == 0) : ((r0 & ma) == 0);
     if (wrapped) s.img[(size_t)ax * npad + slot] += (dir & 1) ? 1 : -1;
+    uint16_t *bcode = s.bcode;
     if (dgm > 0) {
         const uint32_t n0 = (dir & 1) ? bcode_dec(c0, ax) : bcode_inc(c0, ax);
         const uint32_t n1 = dgm > 1 ? ((dir & 1) ? bcode_dec(c1, ax) : bcode_inc(c1, ax)) : c1;
-        *bc.pair(slot) = n0 | (n1 << 16);
-        *bc.at(v0, q0) = (uint16_t)bcode_neg(n0);
-        if (dgm > 1) *bc.at(v1, q1) = (uint16_t)bcode_neg(n1);
+        bc_pair(bcode)[slot] = n0 | (n1 << 16);
+        bcode[bc_index(v0, q0, npad)] = (uint16_t)bcode_neg(n0);
+        if (dgm > 1) bcode[bc_index(v1, q1, npad)] = (uint16_t)bcode_neg(n1);
     }
     for (uint32_t b = 2; b < dgm; ++b) {
         const size_t own = (size_t)b * npad + slot;
-        uint16_t *mine = bc.at(b, slot);
-        const uint32_t nc = (dir & 1) ? bcode_dec(*mine, ax) : bcode_inc(*mine, ax);
-        *mine = (uint16_t)nc;
-        *bc.at(s.rev[own], s.nbr[own]) = (uint16_t)bcode_neg(nc);
+        const uint32_t nc = (dir & 1) ? bcode_dec(bcode[own], ax) : bcode_inc(bcode[own], ax);
+        bcode[own] = (uint16_t)nc;
+        bcode[bc_index(s.rev[own], s.nbr[own], npad)] = (uint16_t)bcode_neg(nc);
     }
 }
 
@@ -854,24 +770,18 @@ __device__ __forceinline__ bool win_wait(GridBarrier *bar, unsigned int target, 
 }
 
 /* one shape of the windowed kernel: U items per thread in flight in the
- * check phase; blockDim.x threads (a multiple of 32, 64 to 1024); CLM 0:
- * one CTA per SM, grid barriers; 1: the grid is one cluster (cluster
- * barriers); 2: one cluster that also holds the lattices and bond codes in
- * its distributed shared memory for the whole launch */
-template <int RNG, int U, int CLM = 0>
+ * check phase; blockDim.x threads (a multiple of 32, 64 to 1024); CL: the
+ * grid is one cluster (cluster barriers instead of grid barriers) */
+template <int RNG, int U, bool CL = false>
 __global__ void __launch_bounds__(1024, 1)
     k_sweep_w(Sys s, const Substep *__restrict__ sched, uint32_t k0, uint32_t k1, GridBarrier *bar,
               unsigned long long timeoutNs, uint32_t maxdeg, uint32_t window, uint32_t nspec, uint32_t ptotal)
 {
-    constexpr bool CL = CLM > 0;
-    constexpr bool DSM = CLM == 2;
     const uint32_t T = blockDim.x, NW = T >> 5;
     extern __shared__ __align__(16) unsigned char s_dyn[];
     __shared__ uint32_t s_after[6 * 16];
     __shared__ uint32_t s_lo[kWinMaxSpecies], s_n[kWinMaxSpecies], s_off[kWinMaxSpecies], s_base[kWinMaxSpecies];
     __shared__ unsigned int s_wcnt[2][32];
-    __shared__ unsigned long long *s_latR[DSM ? 16 : 1], *s_tmpR[2][DSM ? 16 : 1];
-    __shared__ uint32_t *s_bcR[DSM ? 16 : 1];
 
     const WinLayout lay{window, T, ptotal};
     const uint32_t seg = lay.seg();
@@ -919,60 +829,15 @@ __global__ void __launch_bounds__(1024, 1)
         }
     __syncthreads();
 
+    unsigned long long *lat = reinterpret_cast<unsigned long long *>(s.lat);
+    unsigned long long *tmp = reinterpret_cast<unsigned long long *>(s.tmp);
     const Geometry geo = s.g;
     const uint32_t words = s.latWords >> 1;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t lanemask = (1u << lane) - 1u;
     const uint32_t npad = s.npad;
     const uint32_t *__restrict__ nbr = s.nbr;
-    LatAcc<DSM> LA, TA;
-    BondAcc<DSM> BA;
-    LA.p = reinterpret_cast<unsigned long long *>(s.lat);
-    TA.p = reinterpret_cast<unsigned long long *>(s.tmp);
-    BA.p = s.bcode;
-    BA.npad = npad;
-    DsmPlan plan{};
-    unsigned long long *myLat = nullptr;
-    uint32_t *myBc = nullptr;
-    if (DSM) {
-        /* this CTA's slices after the windowed layout; load the lattice and
-         * bond-code slices, zero the target slices */
-        const uint32_t cs = gridDim.x, rank = blockIdx.x; /* the grid is one cluster */
-        plan = dsm_plan(words, npad, maxdeg, cs);
-        myLat = reinterpret_cast<unsigned long long *>(s_dyn + lay.bytes());
-        unsigned long long *myT0 = myLat + plan.latSlice, *myT1 = myT0 + plan.latSlice;
-        myBc = reinterpret_cast<uint32_t *>(myT1 + plan.latSlice);
-        if (threadIdx.x < cs) {
-            s_latR[threadIdx.x] = cluster_map(myLat, threadIdx.x);
-            s_tmpR[0][threadIdx.x] = cluster_map(myT0, threadIdx.x);
-            s_tmpR[1][threadIdx.x] = cluster_map(myT1, threadIdx.x);
-            s_bcR[threadIdx.x] = cluster_map(myBc, threadIdx.x);
-        }
-        const unsigned long long *gl = reinterpret_cast<const unsigned long long *>(s.lat) + (size_t)rank * plan.latSlice;
-        for (uint32_t w = threadIdx.x; w < plan.latSlice; w += T) {
-            myLat[w] = gl[w];
-            myT0[w] = 0ull;
-            myT1[w] = 0ull;
-        }
-        const uint32_t per = plan.bcPer, rows = maxdeg > 2 ? maxdeg : 2;
-        uint16_t *myRows = reinterpret_cast<uint16_t *>(myBc + per);
-        for (uint32_t ls = threadIdx.x; ls < per; ls += T) {
-            const uint32_t slot = rank * per + ls;
-            myBc[ls] = slot < npad ? bc_pair(s.bcode)[slot] : 0u;
-            for (uint32_t j = 2; j < rows; ++j) myRows[(size_t)(j - 2) * per + ls] = slot < npad ? s.bcode[(size_t)j * npad + slot] : 0;
-        }
-        const uint32_t sh = 31u - __clz(plan.latSlice), bsh = 31u - __clz(per);
-        LA.rank = s_latR;
-        LA.sh = sh;
-        LA.mask = plan.latSlice - 1u;
-        TA.rank = s_tmpR[0];
-        TA.sh = sh;
-        TA.mask = plan.latSlice - 1u;
-        BA.rank = s_bcR;
-        BA.sh = bsh;
-        BA.per = per;
-        asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-    }
+    const uint16_t *bcode = s.bcode;
     unsigned int nCand = 0, nAcc = 0;
     unsigned int target = 0;
     bool alive = true;
@@ -984,25 +849,18 @@ __global__ void __launch_bounds__(1024, 1)
         for (uint32_t w = threadIdx.x - 32u; w < n; w += T - 32u)
             px[w] = (uint8_t)((uint32_t)direction(draw<RNG>(dn.seed, dn.iter, plo + w, dn.iterHi)) | ((uint32_t)sdeg[base + w] << 3));
     };
-    /* the target lattice of buffer `buf` (0 or 1) */
-    auto tgt = [&](uint32_t buf) -> LatAcc<DSM> {
-        LatAcc<DSM> t = TA;
-        if (DSM) t.rank = buf ? s_tmpR[1] : s_tmpR[0];
-        else t.p = TA.p + (size_t)buf * words;
-        return t;
-    };
     /* zero the target words of warp wi's candidates of the substep using buffer buf, list set p */
     auto clear_targets = [&](uint32_t buf, uint32_t p, uint32_t wi) {
-        const LatAcc<DSM> tp = tgt(buf);
+        unsigned long long *tp = tmp + (size_t)buf * words;
         const uint2 *pl = lists + ((size_t)p * NW + wi) * seg;
         const unsigned int pc = s_wcnt[p][wi];
         for (uint32_t j = lane; j < pc; j += 32u) {
             const uint2 e = pl[j];
-            *tp.at(zstep(e.y, (int)(e.x >> 28), geo) >> 6) = 0ull;
+            tp[zstep(e.y, (int)(e.x >> 28), geo) >> 6] = 0ull;
         }
     };
-    auto occupied = [&](const LatAcc<DSM> &L, const FaceW &fw) -> unsigned long long {
-        return split_occupied_a(L, fw, s_tab, lane);
+    auto occupied = [&](const unsigned long long *L, const FaceW &fw) -> unsigned long long {
+        return split_occupied(L, fw, s_tab, lane);
     };
 
     Substep d = sched[k0];
@@ -1015,7 +873,7 @@ __global__ void __launch_bounds__(1024, 1)
         const uint32_t n = s_n[d.species], off = s_off[d.species], base = s_base[d.species];
         const uint32_t p = k & 1u;
         uint2 *wlist = lists + ((size_t)p * NW + warp) * seg;
-        const LatAcc<DSM> tb = tgt(d.buf);
+        unsigned long long *tb = tmp + (size_t)d.buf * words;
         unsigned int wc = 0; /* this warp's candidates (warp-uniform) */
 
         /* phase A: U items per thread at a time */
@@ -1037,8 +895,8 @@ __global__ void __launch_bounds__(1024, 1)
                 occ[u] = 1ull;
                 ca[u] = 0u;
                 if (w < n) {
-                    occ[u] = occupied(LA, f[u]);
-                    if (maxdeg > 0) ca[u] = *BA.pair(off + w);
+                    occ[u] = occupied(lat, f[u]);
+                    if (maxdeg > 0) ca[u] = bc_pair(bcode)[off + w];
                 }
             }
 #pragma unroll
@@ -1053,13 +911,13 @@ __global__ void __launch_bounds__(1024, 1)
                     if (dg > 0) ok = !((after[a0 >> 5] >> (a0 & 31u)) & 1u);
                     if (dg > 1) ok = ok && !((after[a1 >> 5] >> (a1 & 31u)) & 1u);
                     for (uint32_t j = 2; ok && j < dg; ++j) {
-                        const uint32_t c = *BA.at(j, off + w);
+                        const uint32_t c = bcode[(size_t)j * npad + off + w];
                         if ((after[c >> 5] >> (c & 31u)) & 1u) ok = false;
                     }
                 }
                 if (ok) {
                     const uint32_t r1 = (dir & 1) ? zinc(r0[u], f[u].ma, f[u].ua) : zdec(r0[u], f[u].ma, f[u].ua);
-                    atomicOr(tb.at(r1 >> 6), 1ull << (r1 & 63u));
+                    atomicOr(tb + (r1 >> 6), 1ull << (r1 & 63u));
                 }
                 const unsigned int m = __ballot_sync(0xFFFFFFFFu, ok);
                 if (ok) wlist[wc + __popc(m & lanemask)] = make_uint2(w | ((uint32_t)dir << 28), r0[u]);
@@ -1115,7 +973,7 @@ __global__ void __launch_bounds__(1024, 1)
                 if (maxdeg > 0) {
                     bq0 = nbr[slot];
                     bv0 = s.rev[slot];
-                    const uint32_t pr = *BA.pair(slot);
+                    const uint32_t pr = bc_pair(bcode)[slot];
                     bc0 = pr & 0xFFFFu;
                     bc1 = pr >> 16;
                 }
@@ -1132,11 +990,11 @@ __global__ void __launch_bounds__(1024, 1)
 
         /* phase B: perform the candidates */
         {
-            const LatAcc<DSM> tr = tgt(d.buf);
+            const unsigned long long *tr = tmp + (size_t)d.buf * words;
             if (bval) {
                 const uint32_t w = e0.x & 0x0FFFFFFFu;
                 if (!occupied(tr, face_words(e0.y, (int)(e0.x >> 28), geo))) {
-                    apply_move(s, LA, BA, spos + base + w, off + w, e0.y, (int)(e0.x >> 28), geo, bdg, bq0, bv0, bc0, bq1, bv1, bc1);
+                    apply_move(s, lat, spos + base + w, off + w, e0.y, (int)(e0.x >> 28), geo, bdg, bq0, bv0, bc0, bq1, bv1, bc1);
                     ++nAcc;
                 }
             }
@@ -1151,7 +1009,7 @@ __global__ void __launch_bounds__(1024, 1)
                 if (maxdeg > 0) {
                     q0 = nbr[slot];
                     v0 = s.rev[slot];
-                    const uint32_t pr = *BA.pair(slot);
+                    const uint32_t pr = bc_pair(bcode)[slot];
                     c0 = pr & 0xFFFFu;
                     c1 = pr >> 16;
                 }
@@ -1160,7 +1018,7 @@ __global__ void __launch_bounds__(1024, 1)
                     v1 = s.rev[(size_t)npad + slot];
                 }
                 if (occupied(tr, face_words(e.y, (int)(e.x >> 28), geo))) continue;
-                apply_move(s, LA, BA, spos + base + w, slot, e.y, (int)(e.x >> 28), geo, dgm, q0, v0, c0, q1, v1, c1);
+                apply_move(s, lat, spos + base + w, slot, e.y, (int)(e.x >> 28), geo, dgm, q0, v0, c0, q1, v1, c1);
                 ++nAcc;
             }
         }
@@ -1183,21 +1041,6 @@ __global__ void __launch_bounds__(1024, 1)
     __syncthreads();
     for (uint32_t c = 0; c < nspec; ++c)
         for (uint32_t w = threadIdx.x; w < s_n[c]; w += T) s.pos[s_off[c] + w] = spos[s_base[c] + w];
-    if (DSM) {
-        /* every CTA is done with the slices: the lattice and bond codes back
-         * to global memory (the target slices are all zero and stay here) */
-        asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-        const uint32_t rank = blockIdx.x, per = plan.bcPer, rows = maxdeg > 2 ? maxdeg : 2;
-        unsigned long long *gl = reinterpret_cast<unsigned long long *>(s.lat) + (size_t)rank * plan.latSlice;
-        for (uint32_t w = threadIdx.x; w < plan.latSlice; w += T) gl[w] = myLat[w];
-        const uint16_t *myRows = reinterpret_cast<const uint16_t *>(myBc + per);
-        for (uint32_t ls = threadIdx.x; ls < per; ls += T) {
-            const uint32_t slot = rank * per + ls;
-            if (slot >= npad) break;
-            bc_pair(s.bcode)[slot] = myBc[ls];
-            for (uint32_t j = 2; j < rows; ++j) s.bcode[(size_t)j * npad + slot] = myRows[(size_t)(j - 2) * per + ls];
-        }
-    }
     for (int o = 16; o > 0; o >>= 1) nAcc += __shfl_down_sync(0xFFFFFFFFu, nAcc, o);
     if (lane == 0 && s.counters) {
         if (nCand) atomicAdd(s.counters + 0, (unsigned long long)nCand);
@@ -1207,13 +1050,10 @@ __global__ void __launch_bounds__(1024, 1)
 
 /* the windowed shapes: items in flight per thread in the check phase; the
  * CTA size is chosen at configuration to pack the CTA's items tightly */
-constexpr int kWinU[7] = {1, 2, 4, 2, 2, 2, 2};
-/* windowed variants 3, 4 (shapes 9, 10): the launch is one cluster of 8 or
- * 16 CTAs, for systems small enough that each CTA holds few monomers;
- * variants 5, 6 (shapes 11, 12): the same with the lattices and bond codes
- * in the cluster's distributed shared memory */
-constexpr int kWinCluster[7] = {0, 0, 0, 8, 16, 8, 16};
-constexpr bool kWinDsm[7] = {false, false, false, false, false, true, true};
+constexpr int kWinU[5] = {1, 2, 4, 2, 2};
+/* windowed variants 3 and 4 (shapes 9, 10): the launch is one cluster of
+ * 8 or 16 CTAs, for systems small enough that each CTA holds few monomers */
+constexpr int kWinCluster[5] = {0, 0, 0, 8, 16};
 
 template <int RNG>
 const void *win_kernel(int i)
@@ -1221,8 +1061,7 @@ const void *win_kernel(int i)
     return i == 0   ? (const void *)k_sweep_w<RNG, 1>
            : i == 1 ? (const void *)k_sweep_w<RNG, 2>
            : i == 2 ? (const void *)k_sweep_w<RNG, 4>
-           : i <= 4 ? (const void *)k_sweep_w<RNG, 2, 1>
-                    : (const void *)k_sweep_w<RNG, 2, 2>;
+                    : (const void *)k_sweep_w<RNG, 2, true>;
 }
 
 /* rounds grid barriers expecting `expected` CTAs; with expected > gridDim.x
@@ -1771,9 +1610,8 @@ struct Engine {
     }
 
     /* the windowed kernel (shape 6 + variant): one CTA per SM (variants
-     * 0..2) or one cluster of 8 or 16 CTAs (3, 4; 5, 6 with the lattices
-     * and bond codes in the cluster's distributed shared memory);
-     * positions, directions and both candidate lists in shared memory */
+     * 0..2) or one cluster of 8 or 16 CTAs (3, 4); positions, directions and
+     * both candidate lists in shared memory */
     template <int RNG>
     bool configureWindowed(int smCount, size_t smemLimit, int variant)
     {
@@ -1792,13 +1630,7 @@ struct Engine {
         uint32_t P = 0; /* most items of all colours one CTA owns */
         for (uint32_t c = 0; c < nSpecies; ++c) P += (spec[c].n + grid - 1) / grid;
         P = (P + 15u) & ~15u;
-        size_t smem = WinLayout{W, threads, P}.bytes();
-        if (kWinDsm[variant]) {
-            const uint32_t words64 = (uint32_t)(latWords / 2);
-            /* power-of-two slices of at least four words per CTA */
-            if (words64 < cluster * 4u || (words64 & (words64 - 1u)) != 0u) return false;
-            smem += dsm_plan(words64, npad, maxdeg, cluster).bytes;
-        }
+        const size_t smem = WinLayout{W, threads, P}.bytes();
         if (smem > smemLimit) return false;
         const void *fn = win_kernel<RNG>(variant);
         CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -2054,7 +1886,7 @@ struct Engine {
         /* candidates: automatic first, then every other shape that fits */
         std::vector<std::pair<int, int>> cand = {{-1, 0}};
         const int autoMode = sweepMode;
-        for (int sh : {6, 7, 8, 9, 10, 11, 12, 1, 2})
+        for (int sh : {6, 7, 8, 9, 10, 1, 2})
             if (sh != autoMode) cand.push_back({sh, 0});
         cand.push_back({autoMode >= SWEEP_WINDOWED ? autoMode : 7, 1});
         const uint32_t piece = std::max<uint32_t>(1, m / (uint32_t)(cand.size() + 1) / nSpecies) * nSpecies;
@@ -2858,7 +2690,7 @@ int bfm_time_kernels(bfm_handle *h, uint32_t nmcs, double *ms, uint64_t *launche
 int bfm_set_sweep_shape(bfm_handle *h, int shape)
 {
     GUARD(h, {
-        if (shape < -1 || shape > 12) throw InvalidArgument("sweep shape must be -1 (automatic) or 0..12");
+        if (shape < -1 || shape > 10) throw InvalidArgument("sweep shape must be -1 (automatic) or 0..10");
         h->e.forcedShape = shape;
         if (h->e.initialized) h->e.configureSweep();
     });

@@ -103,17 +103,16 @@ def test_c1_dilute_chains_1000_mcs():
     three_way(s, [1, 499, 500], age=0, sort_every=5000, ctype=0)
 
 
-@pytest.mark.parametrize("shape", [9, 10, 11, 12])
+@pytest.mark.parametrize("shape", [9, 10])
 def test_c1_on_one_cluster(shape):
     """C1 on the windowed kernel confined to one cluster of 8 or 16 CTAs
-    (cluster barriers instead of grid barriers; 11, 12 with the 128^3
-    lattices and the bond codes in the cluster's shared memory)"""
+    (cluster barriers instead of grid barriers)"""
     s = systems.saw_chains(128, 64, box=(128, 128, 128), seed=12345)
     pb.r250_seed(4242)
     st = pb.r250_get_state()
     u = pb.UpdaterGPUScBFM_AB_Type().setup(s, rng=pb.Rng.Saru)
     u.setSweepShape(shape)
-    assert u.getLaunchInfo()["mode"] == shape and u.getLaunchInfo()["ctas"] == (8 if shape in (9, 11) else 16)
+    assert u.getLaunchInfo()["mode"] == shape and u.getLaunchInfo()["ctas"] == (8 if shape == 9 else 16)
     o = oracle.Sweep(s, rng=2, threads=THREADS)
     for nmcs in (1, 299):
         u.runSimulationOnGPU(nmcs)

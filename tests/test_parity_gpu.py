@@ -83,12 +83,12 @@ def test_split_kernel_paths_match_oracle(name, mode):
     run_pair(SYSTEMS[name], pb.Rng.Saru, 0, 50, [70, 130], mode=mode)
 
 
-@pytest.mark.parametrize("shape", [0, 1, 2, 3, 4, 6, 7, 8, 9, 10, 11, 12])
+@pytest.mark.parametrize("shape", [0, 1, 2, 3, 4, 6, 7, 8, 9, 10])
 @pytest.mark.parametrize("name", ["dense_chains", "crosslinked", "star_comb", "melt_L32"])
 def test_every_persistent_kernel_shape_matches_oracle(name, shape):
     """gather / stored / staged / windowed bond handling, candidate lists in
-    shared or global memory, grid or cluster barriers, lattices in global or
-    distributed shared memory: all bit-exact against the oracle."""
+    shared or global memory, grid or cluster barriers: all bit-exact
+    against the oracle."""
     s = SYSTEMS[name]
     pb.r250_seed(4321)
     st = pb.r250_get_state()
