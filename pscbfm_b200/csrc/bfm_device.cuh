@@ -218,23 +218,16 @@ __host__ __device__ __forceinline__ FaceM face_alu(uint32_t r0, int dir, const G
     return f;
 }
 
-/* Entry e = 64 * ax + zl of the face-mask table: for a move along axis ax
- * whose first face site (the plane two steps ahead, coordinate -1 along
- * both transverse axes) has the low six Z-order bits zl -- the position of
- * that site inside its 4x4x4 brick, i.e. the low two coordinate bits la
- * (move axis), lb, lc (transverse axes b, c), bit k and bit k + 3 of zl for
- * axis k -- the masks of the nine face sites in the (up to) four bricks it
- * touches, m[gb | gc << 1] (gb, gc: the range spills into the next brick
- * along b, c). */
+/* Entry e = ((ax * 4 + la) * 4 + lb) * 4 + lc of the face-mask table: for a
+ * move along axis ax whose leading face lies in the plane with low
+ * coordinate bits la, and whose transverse ranges start at low bits lb, lc,
+ * the masks of the nine face sites in the (up to) four bricks it touches,
+ * m[gb | gc << 1] (gb, gc: the range spills into the next brick along b, c). */
 __host__ __device__ inline void face_table_entry(int e, unsigned long long *m)
 {
-    const int a = e >> 6;
-    const uint32_t zl = (uint32_t)e & 63u;
+    const int a = e >> 6, la = (e >> 4) & 3, lb = (e >> 2) & 3, lc = e & 3;
     const int bx = (a == 0) ? 1 : 0;
     const int cx = (a == 2) ? 1 : 2;
-    const int la = (int)(((zl >> a) & 1u) | (((zl >> (a + 3)) & 1u) << 1));
-    const int lb = (int)(((zl >> bx) & 1u) | (((zl >> (bx + 3)) & 1u) << 1));
-    const int lc = (int)(((zl >> cx) & 1u) | (((zl >> (cx + 3)) & 1u) << 1));
     const uint32_t abit = (((uint32_t)la & 1u) | (((uint32_t)la & 2u) << 2)) << a;
     unsigned long long m0 = 0, m1 = 0, m2 = 0, m3 = 0;
     for (int ib = 0; ib < 3; ++ib)
@@ -255,15 +248,13 @@ __host__ __device__ inline void face_table_entry(int e, unsigned long long *m)
     m[3] = m3;
 }
 
-/* The four brick words of the face, its face-table entry 64 * ax + zl, and
- * whether the transverse ranges spill into the next brick along b (sb) and
- * c (sc): bit 1 of the first site's low coordinate along that axis, i.e.
- * Z-order bit 3 + axis (non-zero = spills); with the direction constants
- * of the step. */
+/* The four brick words of the face and the index of its masks in the face
+ * table ((ax * 4 + la) * 4 + lb) * 4 + lc (la, lb, lc: the low coordinate
+ * bits of the plane and of the first transverse values), with the
+ * direction constants computed in registers. */
 struct FaceW {
     uint32_t w[4];
     uint32_t t;
-    uint32_t sb, sc;
     uint32_t ma, ua;
 };
 
@@ -279,76 +270,21 @@ __host__ __device__ __forceinline__ FaceW face_words(uint32_t r0, int dir, const
     const uint32_t b2 = ((r0 | ~mb) + ub) & mb;
     const uint32_t c0 = ((r0 & mc) - uc) & mc;
     const uint32_t c2 = ((r0 | ~mc) + uc) & mc;
-    const uint32_t z0 = pa | b0 | c0;
+    const uint32_t la = ((pa >> ax) & 1u) | ((pa >> (ax + 2u)) & 2u);
+    const uint32_t lb = ((b0 >> bx) & 1u) | ((b0 >> (bx + 2u)) & 2u);
+    const uint32_t lc = ((c0 >> cx) & 1u) | ((c0 >> (cx + 2u)) & 2u);
+    const uint32_t ha = pa >> 6, hb0 = b0 >> 6, hb2 = b2 >> 6, hc0 = c0 >> 6, hc2 = c2 >> 6;
     FaceW f;
-    f.w[0] = z0 >> 6;
-    f.w[1] = (pa | b2 | c0) >> 6;
-    f.w[2] = (pa | b0 | c2) >> 6;
-    f.w[3] = (pa | b2 | c2) >> 6;
-    f.t = ax * 64u + (z0 & 63u);
-    f.sb = (z0 >> 3) & ub;
-    f.sc = (z0 >> 3) & uc;
+    f.w[0] = ha | hb0 | hc0;
+    f.w[1] = ha | hb2 | hc0;
+    f.w[2] = ha | hb0 | hc2;
+    f.w[3] = ha | hb2 | hc2;
+    f.t = ((ax * 4u + la) * 4u + lb) * 4u + lc;
     f.ma = ma;
     f.ua = ua;
     return f;
 }
 
-/* Constants of one move direction, for kernels that keep the six of them
- * in shared memory and index them by the drawn direction instead of
- * selecting axes and masks per move.  Steps use dilated addition only:
- * a (+) d = ((a | ~m) + d) & m, with d the dilated form of the step modulo
- * the box edge (L - 1 = all payload bits of the axis stands for -1). */
-struct DirK {
-    uint32_t ma, mb, mc; /* payload masks: move axis a, transverse axes b, c */
-    uint32_t d2;         /* dilated +-2 (mod L_a) along a: the face plane */
-    uint32_t d1;         /* dilated +-1 (mod L_a) along a: the move */
-    uint32_t ub, uc;     /* unit bits of b and c */
-    uint32_t t0;         /* 64 * a: the axis' first face-table entry */
-};
-
-__host__ __device__ inline DirK dir_consts(int dir, const Geometry &g)
-{
-    const uint32_t ax = (uint32_t)dir >> 1;
-    const uint32_t bx = ax == 0u ? 1u : 0u, cx = ax == 2u ? 1u : 2u;
-    DirK k;
-    k.ma = axis_mask(g, (int)ax);
-    k.mb = axis_mask(g, (int)bx);
-    k.mc = axis_mask(g, (int)cx);
-    const uint32_t ua = 1u << ax;
-    k.d1 = (dir & 1) ? ua : k.ma;                              /* +1, or L_a - 1 */
-    k.d2 = (dir & 1) ? (ua << 3) & k.ma : ((0u - (ua << 3)) & k.ma); /* +2, or L_a - 2 */
-    k.ub = 1u << bx;
-    k.uc = 1u << cx;
-    k.t0 = ax * 64u;
-    return k;
-}
-
-/* face_words from the direction constants (same words, entry and spills) */
-__host__ __device__ __forceinline__ FaceW face_k(uint32_t r0, const DirK &k)
-{
-    const uint32_t pa = ((r0 | ~k.ma) + k.d2) & k.ma;
-    const uint32_t rb = r0 | ~k.mb, rc = r0 | ~k.mc;
-    const uint32_t b0 = (rb + k.mb) & k.mb, b2 = (rb + k.ub) & k.mb;
-    const uint32_t c0 = (rc + k.mc) & k.mc, c2 = (rc + k.uc) & k.mc;
-    const uint32_t z0 = pa | b0 | c0;
-    FaceW f;
-    f.w[0] = z0 >> 6;
-    f.w[1] = (pa | b2 | c0) >> 6;
-    f.w[2] = (pa | b0 | c2) >> 6;
-    f.w[3] = (pa | b2 | c2) >> 6;
-    f.t = k.t0 + (z0 & 63u);
-    f.sb = (z0 >> 3) & k.ub;
-    f.sc = (z0 >> 3) & k.uc;
-    f.ma = k.ma;
-    f.ua = 0u;
-    return f;
-}
-
-/* the unit step of r0 along the direction of k */
-__host__ __device__ __forceinline__ uint32_t step_k(uint32_t r0, const DirK &k)
-{
-    return (r0 & ~k.ma) | (((r0 | ~k.ma) + k.d1) & k.ma);
-}
 
 __host__ __device__ __forceinline__ unsigned long long face_mask(const FaceM &f, int g)
 {

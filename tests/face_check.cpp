@@ -47,16 +47,12 @@ int main()
                     if (face_mask(fm, q)) alu[fm.w[q]] |= face_mask(fm, q);
                 const uint32_t r1 = zstep(r0, dir, g);
                 const uint32_t r1w = (dir & 1) ? zinc(r0, fw.ma, fw.ua) : zdec(r0, fw.ma, fw.ua);
-                /* the direction-constant form gives the same words, entry, spills and step */
-                const DirK k = dir_consts(dir, g);
-                const FaceW fk = face_k(r0, k);
-                bool same = fk.t == fw.t && (fk.sb != 0) == (fw.sb != 0) && (fk.sc != 0) == (fw.sc != 0) &&
-                            step_k(r0, k) == r1;
-                for (int q = 0; q < 4; ++q)
-                    if (table[fw.t * 4 + q]) same = same && fk.w[q] == fw.w[q];
-                /* the spill flags name exactly the words the table uses */
-                same = same && ((fw.sb != 0) == (table[fw.t * 4 + 1] != 0)) && ((fw.sc != 0) == (table[fw.t * 4 + 2] != 0)) &&
-                       ((fw.sb != 0 && fw.sc != 0) == (table[fw.t * 4 + 3] != 0));
+                /* the spill rule of the kernels' lookups (words 1..3 are read when
+                 * the transverse start bits lb, lc are >= 2) names exactly the words
+                 * the table uses */
+                const bool sb = ((fw.t >> 2) & 3u) >= 2u, sc = (fw.t & 3u) >= 2u;
+                const bool same = (sb == (table[fw.t * 4 + 1] != 0)) && (sc == (table[fw.t * 4 + 2] != 0)) &&
+                                  ((sb && sc) == (table[fw.t * 4 + 3] != 0));
                 if (tab != want || alu != want || r1 != r1w || !same) {
                     if (bad < 5) printf("mismatch L=%dx%dx%d x=%u y=%u z=%u dir=%d\n", L[0], L[1], L[2], x, y, z, dir);
                     ++bad;
