@@ -288,12 +288,6 @@ int bfm_get_launch_info(const bfm_handle *h, int *mode, int *grid, int *threads,
  * CTAs (hardware cluster barriers; small systems).
  * BFM_ERUNTIME when the shape does not fit this system. */
 int bfm_set_sweep_shape(bfm_handle *h, int shape);
-/* windowed shapes: keep rows 0 and 1 of the bond codes of bonds whose both
- * ends a CTA owns in that CTA's shared memory for the launch (on, default,
- * when they fit) or every bond code in global memory (off); same
- * trajectory either way.  get: whether the configured kernel does. */
-int bfm_set_sweep_shared_codes(bfm_handle *h, int on);
-int bfm_get_sweep_shared_codes(const bfm_handle *h, int *on);
 /* launch-shape autotuner (no counterpart in the reference, whose launch
  * configuration is fixed, UpdaterGPUScBFM_AB_Type.cu:2952-2981): with `on`,
  * the first schedule chunk of the next run is split into equal trial

@@ -121,8 +121,6 @@ _SIGS = {
     "bfm_batch_get_lattice": (_c.c_int, [_P, _c.c_uint32, _P, _c.c_size_t, _P]),
     "bfm_batch_info": (_c.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "bfm_set_sweep_autotune": (_c.c_int, [_P, _c.c_int]),
-    "bfm_set_sweep_shared_codes": (_c.c_int, [_P, _c.c_int]),
-    "bfm_get_sweep_shared_codes": (_c.c_int, [_P, _P]),
     "bfm_get_sweep_tuning": (_c.c_int, [_P, _P, _P, _P, _P, _P, _P, _c.c_uint32]),
     "bfm_batch_set_shape": (_c.c_int, [_P, _c.c_int, _c.c_int]),
     "bfm_batch_get_tuning": (_c.c_int, [_P, _P, _P, _P, _P, _P]),

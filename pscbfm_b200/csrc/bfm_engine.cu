@@ -705,67 +705,12 @@ struct WinLayout {
     __host__ __device__ size_t bytes() const { return lists() + (size_t)2 * (T / 32u) * seg() * 8u; }
 };
 
-/* Where the windowed kernel keeps bond codes.  GlobalCodes: every row in
- * global memory.  SharedCodes: rows 0 and 1 of a monomer whose partner on
- * that row belongs to the same CTA live in the CTA's shared memory for the
- * whole launch (one 32-bit word per monomer, indexed like the positions);
- * rows of bonds that cross to another CTA, and rows >= 2, stay in global
- * memory.  Both ends of a bond decide alike, so each row has one home. */
-struct GlobalCodes {
-    uint16_t *g;
-    uint32_t npad;
-    __device__ __forceinline__ void own_pair(uint32_t slot, uint32_t, uint32_t, uint32_t n0, uint32_t n1) const
-    {
-        bc_pair(g)[slot] = n0 | (n1 << 16);
-    }
-    __device__ __forceinline__ void partner(uint32_t q, uint32_t v, uint32_t code) const
-    {
-        g[bc_index(v, q, npad)] = (uint16_t)code;
-    }
-};
-struct SharedCodes {
-    uint16_t *g;
-    uint32_t npad;
-    uint32_t *sbc;                             /* rows 0, 1 of the CTA's monomers */
-    const uint32_t *off, *n, *base;            /* the CTA's colour ranges */
-    uint32_t nspec;
-    /* shared-memory index of slot q, or ~0 when another CTA owns it */
-    __device__ __forceinline__ uint32_t local(uint32_t q) const
-    {
-        for (uint32_t c = 0; c < nspec; ++c) {
-            const uint32_t d = q - off[c];
-            if (d < n[c]) return base[c] + d;
-        }
-        return ~0u;
-    }
-    /* fl: bit 4 / 5 = row 0 / 1 crosses to another CTA */
-    __device__ __forceinline__ void own_pair(uint32_t slot, uint32_t li, uint32_t fl, uint32_t n0, uint32_t n1) const
-    {
-        sbc[li] = n0 | (n1 << 16);
-        if (fl & 16u) g[2 * (size_t)slot] = (uint16_t)n0;
-        if (fl & 32u) g[2 * (size_t)slot + 1] = (uint16_t)n1;
-    }
-    __device__ __forceinline__ void partner(uint32_t q, uint32_t v, uint32_t code) const
-    {
-        if (v < 2u) {
-            const uint32_t l = local(q);
-            if (l != ~0u) {
-                reinterpret_cast<uint16_t *>(sbc + l)[v] = (uint16_t)code;
-                return;
-            }
-        }
-        g[bc_index(v, q, npad)] = (uint16_t)code;
-    }
-};
-
 /* apply an accepted move: lattice bits, position (shared memory), image
  * counter, own bond codes and the partners' codes of the bonds back
- * (per-axis negation); li: the monomer's shared-memory index, fl its
- * crossing-row flags (SharedCodes) */
-template <class Codes>
-__device__ __forceinline__ void apply_move(const Sys &s, unsigned long long *lat, uint32_t *spos, uint32_t slot, uint32_t li,
-                                           uint32_t fl, uint32_t r0, int dir, const Geometry &geo, uint32_t dgm, uint32_t q0,
-                                           uint32_t v0, uint32_t c0, uint32_t q1, uint32_t v1, uint32_t c1, const Codes &cd)
+ * (per-axis negation) */
+__device__ __forceinline__ void apply_move(const Sys &s, unsigned long long *lat, uint32_t *spos, uint32_t slot, uint32_t r0,
+                                           int dir, const Geometry &geo, uint32_t dgm, uint32_t q0, uint32_t v0, uint32_t c0,
+                                           uint32_t q1, uint32_t v1, uint32_t c1)
 {
     const uint32_t npad = s.npad;
     const uint32_t ax = (uint32_t)(dir >> 1);
@@ -786,15 +731,15 @@ __device__ __forceinline__ void apply_move(const Sys &s, unsigned long long *lat
     if (dgm > 0) {
         const uint32_t n0 = (dir & 1) ? bcode_dec(c0, ax) : bcode_inc(c0, ax);
         const uint32_t n1 = dgm > 1 ? ((dir & 1) ? bcode_dec(c1, ax) : bcode_inc(c1, ax)) : c1;
-        cd.own_pair(slot, li, fl, n0, n1);
-        cd.partner(q0, v0, bcode_neg(n0));
-        if (dgm > 1) cd.partner(q1, v1, bcode_neg(n1));
+        bc_pair(bcode)[slot] = n0 | (n1 << 16);
+        bcode[bc_index(v0, q0, npad)] = (uint16_t)bcode_neg(n0);
+        if (dgm > 1) bcode[bc_index(v1, q1, npad)] = (uint16_t)bcode_neg(n1);
     }
     for (uint32_t b = 2; b < dgm; ++b) {
         const size_t own = (size_t)b * npad + slot;
         const uint32_t nc = (dir & 1) ? bcode_dec(bcode[own], ax) : bcode_inc(bcode[own], ax);
         bcode[own] = (uint16_t)nc;
-        cd.partner(s.nbr[own], s.rev[own], bcode_neg(nc));
+        bcode[bc_index(s.rev[own], s.nbr[own], npad)] = (uint16_t)bcode_neg(nc);
     }
 }
 
@@ -825,7 +770,7 @@ __device__ __forceinline__ bool win_wait(GridBarrier *bar, unsigned int target, 
 /* one shape of the windowed kernel: U items per thread in flight in the
  * check phase; blockDim.x threads (a multiple of 32, 64 to 1024); CL: the
  * grid is one cluster (cluster barriers instead of grid barriers) */
-template <int RNG, int U, bool CL = false, bool SBC = false>
+template <int RNG, int U, bool CL = false>
 __global__ void __launch_bounds__(1024, 1)
     k_sweep_w(Sys s, const Substep *__restrict__ sched, uint32_t k0, uint32_t k1, GridBarrier *bar,
               unsigned long long timeoutNs, uint32_t maxdeg, uint32_t window, uint32_t nspec, uint32_t ptotal)
@@ -881,25 +826,6 @@ __global__ void __launch_bounds__(1024, 1)
             sdeg[s_base[c] + w] = s.deg[s_off[c] + w];
         }
     __syncthreads();
-    /* SBC: bond-code rows 0 and 1 of the CTA's monomers in shared memory;
-     * bit 4 / 5 of the bond count marks a row whose partner another CTA
-     * owns (that row stays in global memory) */
-    uint32_t *sbc = SBC ? reinterpret_cast<uint32_t *>(s_dyn + lay.bytes()) : nullptr;
-    SharedCodes scd{s.bcode, s.npad, sbc, s_off, s_n, s_base, nspec};
-    if (SBC) {
-        for (uint32_t c = 0; c < nspec; ++c)
-            for (uint32_t w = threadIdx.x; w < s_n[c]; w += T) {
-                const uint32_t li = s_base[c] + w, slot = s_off[c] + w;
-                const uint32_t dg = sdeg[li];
-                uint32_t fl = 0;
-                if (dg > 0 && scd.local(s.nbr[slot]) == ~0u) fl |= 16u;
-                if (dg > 1 && scd.local(s.nbr[(size_t)s.npad + slot]) == ~0u) fl |= 32u;
-                sdeg[li] = (uint8_t)(dg | fl);
-                sbc[li] = dg > 0 ? bc_pair(s.bcode)[slot] : 0u;
-            }
-        __syncthreads();
-    }
-    const GlobalCodes gcd{s.bcode, s.npad};
 
     unsigned long long *lat = reinterpret_cast<unsigned long long *>(s.lat);
     unsigned long long *tmp = reinterpret_cast<unsigned long long *>(s.tmp);
@@ -914,28 +840,12 @@ __global__ void __launch_bounds__(1024, 1)
     unsigned int target = 0;
     bool alive = true;
 
-    /* direction | bonds << 3 (| 128: a bond-code row in global memory) */
-    auto xbits = [&](uint32_t sd) -> uint32_t {
-        if (!SBC) return sd << 3;
-        return ((sd & 15u) << 3) | ((sd & 48u) ? 128u : 0u);
-    };
-    /* rows 0 and 1 of the bond codes of the CTA's item li (slot `slot`) */
-    auto pair_of = [&](uint32_t li, uint32_t slot, uint32_t fl) -> uint32_t {
-        if (!SBC) return bc_pair(bcode)[slot];
-        uint32_t v = sbc[li];
-        if (fl & 48u) {
-            const uint32_t g = bc_pair(bcode)[slot];
-            if (fl & 16u) v = (v & 0xFFFF0000u) | (g & 0xFFFFu);
-            if (fl & 32u) v = (v & 0x0000FFFFu) | (g & 0xFFFF0000u);
-        }
-        return v;
-    };
     /* directions of the items of substep dn, by warps 1.. */
     auto prep = [&](const Substep &dn) {
         const uint32_t plo = s_lo[dn.species], n = s_n[dn.species], base = s_base[dn.species];
 #pragma unroll 2
         for (uint32_t w = threadIdx.x - 32u; w < n; w += T - 32u)
-            px[w] = (uint8_t)((uint32_t)direction(draw<RNG>(dn.seed, dn.iter, plo + w, dn.iterHi)) | xbits(sdeg[base + w]));
+            px[w] = (uint8_t)((uint32_t)direction(draw<RNG>(dn.seed, dn.iter, plo + w, dn.iterHi)) | ((uint32_t)sdeg[base + w] << 3));
     };
     /* zero the target words of warp wi's candidates of the substep using buffer buf, list set p */
     auto clear_targets = [&](uint32_t buf, uint32_t p, uint32_t wi) {
@@ -984,14 +894,14 @@ __global__ void __launch_bounds__(1024, 1)
                 ca[u] = 0u;
                 if (w < n) {
                     occ[u] = occupied(lat, f[u]);
-                    if (maxdeg > 0) ca[u] = pair_of(base + w, off + w, (x[u] & 128u) ? (uint32_t)sdeg[base + w] : 0u);
+                    if (maxdeg > 0) ca[u] = bc_pair(bcode)[off + w];
                 }
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const uint32_t w = b0 + (uint32_t)u * T + threadIdx.x;
                 const int dir = (int)(x[u] & 7u);
-                const uint32_t dg = SBC ? (x[u] >> 3) & 15u : x[u] >> 3;
+                const uint32_t dg = x[u] >> 3;
                 bool ok = occ[u] == 0ull && !leaves_box(r0[u], dir, geo);
                 if (ok) {
                     const uint32_t *after = s_after + dir * 16;
@@ -1052,18 +962,16 @@ __global__ void __launch_bounds__(1024, 1)
         const uint32_t jb = threadIdx.x - 32u;
         const bool bval = threadIdx.x >= 32 && jb < total;
         uint2 e0 = make_uint2(0u, 0u);
-        uint32_t bdg = 0, bfl = 0, bq0 = 0, bv0 = 0, bc0 = 0, bq1 = 0, bv1 = 0, bc1 = 0;
+        uint32_t bdg = 0, bq0 = 0, bv0 = 0, bc0 = 0, bq1 = 0, bv1 = 0, bc1 = 0;
         if (warp > 0 && 32u * (warp - 1u) < total) { /* warp-uniform */
             e0 = entry(bval ? jb : 0u);
             if (bval) {
                 const uint32_t w = e0.x & 0x0FFFFFFFu, slot = off + w;
                 bdg = sdeg[base + w];
-                bfl = bdg & 48u;
-                bdg &= 15u;
                 if (maxdeg > 0) {
                     bq0 = nbr[slot];
                     bv0 = s.rev[slot];
-                    const uint32_t pr = pair_of(base + w, slot, bfl);
+                    const uint32_t pr = bc_pair(bcode)[slot];
                     bc0 = pr & 0xFFFFu;
                     bc1 = pr >> 16;
                 }
@@ -1084,12 +992,7 @@ __global__ void __launch_bounds__(1024, 1)
             if (bval) {
                 const uint32_t w = e0.x & 0x0FFFFFFFu;
                 if (!occupied(tr, face_words(e0.y, (int)(e0.x >> 28), geo))) {
-                    if (SBC)
-                        apply_move(s, lat, spos + base + w, off + w, base + w, bfl, e0.y, (int)(e0.x >> 28), geo, bdg, bq0, bv0, bc0, bq1,
-                                   bv1, bc1, scd);
-                    else
-                        apply_move(s, lat, spos + base + w, off + w, base + w, bfl, e0.y, (int)(e0.x >> 28), geo, bdg, bq0, bv0, bc0, bq1,
-                                   bv1, bc1, gcd);
+                    apply_move(s, lat, spos + base + w, off + w, e0.y, (int)(e0.x >> 28), geo, bdg, bq0, bv0, bc0, bq1, bv1, bc1);
                     ++nAcc;
                 }
             }
@@ -1099,12 +1002,12 @@ __global__ void __launch_bounds__(1024, 1)
                 const uint2 e = entry(j < total ? j : 0u);
                 if (j >= total) continue;
                 const uint32_t w = e.x & 0x0FFFFFFFu, slot = off + w;
-                const uint32_t sd = sdeg[base + w], dgm = sd & 15u, fl = sd & 48u;
+                const uint32_t dgm = sdeg[base + w];
                 uint32_t q0 = 0, v0 = 0, c0 = 0, q1 = 0, v1 = 0, c1 = 0;
                 if (maxdeg > 0) {
                     q0 = nbr[slot];
                     v0 = s.rev[slot];
-                    const uint32_t pr = pair_of(base + w, slot, fl);
+                    const uint32_t pr = bc_pair(bcode)[slot];
                     c0 = pr & 0xFFFFu;
                     c1 = pr >> 16;
                 }
@@ -1113,10 +1016,7 @@ __global__ void __launch_bounds__(1024, 1)
                     v1 = s.rev[(size_t)npad + slot];
                 }
                 if (occupied(tr, face_words(e.y, (int)(e.x >> 28), geo))) continue;
-                if (SBC)
-                    apply_move(s, lat, spos + base + w, slot, base + w, fl, e.y, (int)(e.x >> 28), geo, dgm, q0, v0, c0, q1, v1, c1, scd);
-                else
-                    apply_move(s, lat, spos + base + w, slot, base + w, fl, e.y, (int)(e.x >> 28), geo, dgm, q0, v0, c0, q1, v1, c1, gcd);
+                apply_move(s, lat, spos + base + w, slot, e.y, (int)(e.x >> 28), geo, dgm, q0, v0, c0, q1, v1, c1);
                 ++nAcc;
             }
         }
@@ -1135,18 +1035,10 @@ __global__ void __launch_bounds__(1024, 1)
     /* every CTA has passed the last barrier: zero the last targets so the
      * next launch starts from clean target lattices */
     if (alive && k1 > k0) clear_targets(prevBuf, (k1 - 1u) & 1u, warp);
-    /* positions (and the shared rows of the bond codes) back to global memory */
+    /* positions back to global memory */
     __syncthreads();
     for (uint32_t c = 0; c < nspec; ++c)
-        for (uint32_t w = threadIdx.x; w < s_n[c]; w += T) {
-            s.pos[s_off[c] + w] = spos[s_base[c] + w];
-            if (SBC) {
-                const uint32_t li = s_base[c] + w, slot = s_off[c] + w;
-                const uint32_t sd = sdeg[li], dg = sd & 15u, v = sbc[li];
-                if (dg > 0 && !(sd & 16u)) s.bcode[2 * (size_t)slot] = (uint16_t)(v & 0xFFFFu);
-                if (dg > 1 && !(sd & 32u)) s.bcode[2 * (size_t)slot + 1] = (uint16_t)(v >> 16);
-            }
-        }
+        for (uint32_t w = threadIdx.x; w < s_n[c]; w += T) s.pos[s_off[c] + w] = spos[s_base[c] + w];
     for (int o = 16; o > 0; o >>= 1) nAcc += __shfl_down_sync(0xFFFFFFFFu, nAcc, o);
     if (lane == 0 && s.counters) {
         if (nCand) atomicAdd(s.counters + 0, (unsigned long long)nCand);
@@ -1161,19 +1053,13 @@ constexpr int kWinU[5] = {1, 2, 4, 2, 2};
  * 8 or 16 CTAs, for systems small enough that each CTA holds few monomers */
 constexpr int kWinCluster[5] = {0, 0, 0, 8, 16};
 
-/* sbc: bond-code rows 0, 1 of bonds inside the CTA in shared memory */
-template <int RNG, bool SBC>
-const void *win_kernel_s(int i)
-{
-    return i == 0   ? (const void *)k_sweep_w<RNG, 1, false, SBC>
-           : i == 1 ? (const void *)k_sweep_w<RNG, 2, false, SBC>
-           : i == 2 ? (const void *)k_sweep_w<RNG, 4, false, SBC>
-                    : (const void *)k_sweep_w<RNG, 2, true, SBC>;
-}
 template <int RNG>
-const void *win_kernel(int i, bool sbc)
+const void *win_kernel(int i)
 {
-    return sbc ? win_kernel_s<RNG, true>(i) : win_kernel_s<RNG, false>(i);
+    return i == 0   ? (const void *)k_sweep_w<RNG, 1>
+           : i == 1 ? (const void *)k_sweep_w<RNG, 2>
+           : i == 2 ? (const void *)k_sweep_w<RNG, 4>
+                    : (const void *)k_sweep_w<RNG, 2, true>;
 }
 
 /* rounds grid barriers expecting `expected` CTAs; with expected > gridDim.x
@@ -1665,8 +1551,6 @@ struct Engine {
      * in shared memory when that fits. */
     int sweepMode = 0;
     uint32_t sweepWindow = 0;
-    bool sweepSharedCodes = false; /* windowed kernel keeps inner bond codes in shared memory */
-    bool noSharedCodes = false;    /* keep every bond code in global memory (comparisons) */
     int forcedShape = -1; /* -1 automatic; 0..2 bond mode; +3: candidate lists in global memory; 6 windowed */
     int extraRounds = 0;  /* windowed shapes: rounds of items per thread beyond the fewest (smaller CTAs) */
 
@@ -1744,12 +1628,9 @@ struct Engine {
         uint32_t P = 0; /* most items of all colours one CTA owns */
         for (uint32_t c = 0; c < nSpecies; ++c) P += (spec[c].n + grid - 1) / grid;
         P = (P + 15u) & ~15u;
-        size_t smem = WinLayout{W, threads, P}.bytes();
-        /* bond codes of bonds inside the CTA in shared memory when they fit */
-        const bool sbc = maxdeg > 0 && !noSharedCodes && smem + (size_t)P * 4 <= smemLimit;
-        if (sbc) smem += (size_t)P * 4;
+        const size_t smem = WinLayout{W, threads, P}.bytes();
         if (smem > smemLimit) return false;
-        const void *fn = win_kernel<RNG>(variant, sbc);
+        const void *fn = win_kernel<RNG>(variant);
         CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int fit = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, fn, (int)threads, smem));
@@ -1779,7 +1660,6 @@ struct Engine {
         sweepSmem = smem;
         sweepWindow = W;
         sweepMode = SWEEP_WINDOWED + variant;
-        sweepSharedCodes = sbc;
         sweepGlobalList = false;
         sweepThreads = (int)threads;
         sweepTotal = P;
@@ -1845,9 +1725,9 @@ struct Engine {
             uint32_t ns = nSpecies, pt = sweepTotal;
             void *wargs[] = {&s, (void *)&sched, &k0, &k1, &bar, &to, &md, &win, &ns, &pt};
             const int v = sweepMode - SWEEP_WINDOWED;
-            const void *wf = rng == BFM_RNG_SARU     ? win_kernel<RNG_SARU>(v, sweepSharedCodes)
-                             : rng == BFM_RNG_PHILOX ? win_kernel<RNG_PHILOX>(v, sweepSharedCodes)
-                                                     : win_kernel<RNG_INTHASH>(v, sweepSharedCodes);
+            const void *wf = rng == BFM_RNG_SARU     ? win_kernel<RNG_SARU>(v)
+                             : rng == BFM_RNG_PHILOX ? win_kernel<RNG_PHILOX>(v)
+                                                     : win_kernel<RNG_INTHASH>(v);
             if (kWinCluster[v]) { /* one cluster: hardware cluster barriers */
                 cudaLaunchConfig_t cfg = {};
                 cfg.gridDim = dim3((unsigned)sweepGrid);
@@ -2812,21 +2692,6 @@ int bfm_set_sweep_shape(bfm_handle *h, int shape)
         h->e.forcedShape = shape;
         if (h->e.initialized) h->e.configureSweep();
     });
-}
-
-int bfm_set_sweep_shared_codes(bfm_handle *h, int on)
-{
-    GUARD(h, {
-        h->e.noSharedCodes = on == 0;
-        if (h->e.initialized) h->e.configureSweep();
-    });
-}
-
-int bfm_get_sweep_shared_codes(const bfm_handle *h, int *on)
-{
-    if (!h || !on) return BFM_EINVAL;
-    *on = (h->e.sweepMode >= SWEEP_WINDOWED && h->e.sweepSharedCodes) ? 1 : 0;
-    return BFM_OK;
 }
 
 int bfm_set_sweep_autotune(bfm_handle *h, int on)

@@ -307,15 +307,7 @@ class UpdaterGPUScBFM_AB_Type:
         CTAs, threads per CTA, dynamic shared memory per CTA."""
         m, g, t, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_size_t()
         self._check(self._lib.bfm_get_launch_info(self._h, ctypes.byref(m), ctypes.byref(g), ctypes.byref(t), ctypes.byref(b)))
-        sc = ctypes.c_int()
-        self._check(self._lib.bfm_get_sweep_shared_codes(self._h, ctypes.byref(sc)))
-        return {"mode": m.value, "ctas": g.value, "threads": t.value, "smem_bytes": b.value,
-                "shared_codes": bool(sc.value)}
-
-    def setSweepSharedCodes(self, on: bool = True):
-        """windowed shapes: bond codes of bonds inside a CTA in its shared
-        memory (default, when they fit) or all in global memory"""
-        self._check(self._lib.bfm_set_sweep_shared_codes(self._h, int(bool(on))))
+        return {"mode": m.value, "ctas": g.value, "threads": t.value, "smem_bytes": b.value}
 
     def setSweepShape(self, shape: int):
         """-1 automatic; 0 gather, 1 stored bond codes, 2 staged; +3 global candidate lists;

@@ -281,27 +281,3 @@ def test_positions_into_page_locked_buffer():
         assert [u.getMonomerPositionInX(7), u.getMonomerPositionInY(7), u.getMonomerPositionInZ(7)] == list(want[7])
     with pytest.raises(ValueError):
         u.getAllMonomerPositions(out=np.empty((s.n, 2), np.int32))
-
-
-@pytest.mark.parametrize("shared", [True, False])
-@pytest.mark.parametrize("shape", [6, 7, 8, 10])
-@pytest.mark.parametrize("name", ["dense_chains", "crosslinked", "star_comb", "melt_L32"])
-def test_windowed_bond_codes_shared_or_global(name, shape, shared):
-    """the windowed kernel with the bond codes of bonds inside a CTA held in
-    its shared memory (rows of bonds that cross CTAs, and rows >= 2, in
-    global memory) or with every code in global memory: bit-exact against
-    the oracle, across re-sorts (which re-assign the rows' homes)"""
-    s = SYSTEMS[name]
-    pb.r250_seed(2468)
-    st = pb.r250_get_state()
-    u = pb.UpdaterGPUScBFM_AB_Type().setup(s, rng=pb.Rng.Saru, steps_between_sortings=23)
-    u.setSweepShape(shape)
-    u.setSweepSharedCodes(shared)
-    info = u.getLaunchInfo()
-    assert info["mode"] == shape and info["shared_codes"] == shared
-    o = oracle.Sweep(s, rng=2, sort_every=23, threads=4)
-    for nmcs in (9, 41):
-        u.runSimulationOnGPU(nmcs)
-        o.run(nmcs, st)
-        assert np.array_equal(u.getAllMonomerPositions(), o.positions())
-        assert np.array_equal(u.getLattice(), oracle.lattice_words(o.positions(), s.box))
