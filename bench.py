@@ -315,10 +315,13 @@ def run_b200(args, ranks):
     u = pb.UpdaterGPUScBFM_AB_Type().setup(system, gpu=gpu, rng=pb.Rng.Saru)
     if args.sweep_shape != -1:
         u.setSweepShape(args.sweep_shape)
+    else:
+        # the launch-shape autotuner times the candidate shapes on the first
+        # chunk of the untimed melt (or warm-up) and keeps the fastest
+        u.setSweepAutotune(True)
     S = args.mcs_per_step
     if args.melt_mcs:
         u.runSimulationOnGPU(args.melt_mcs)    # melt the ordered start (untimed)
-    launch_info = u.getLaunchInfo()
     flushbuf = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{gpu}")
     # the caller's page-locked position buffer, filled by one device-to-host copy per step
     pinned = torch.empty((system.n, 3), dtype=torch.int32, pin_memory=True)
@@ -327,6 +330,8 @@ def run_b200(args, ranks):
         flush_l2(flushbuf)
         u.runSimulationOnGPU(S)
         u.getAllMonomerPositions(out=hostpos)
+    launch_info = u.getLaunchInfo()
+    tuning = u.getSweepTuning()
 
     # live timing of every sweep-kernel launch for the roofline (same path)
     a0, c0, s0 = u.getCounters()
@@ -422,7 +427,7 @@ def run_b200(args, ranks):
                           if resident == "l2" else
                           "flushed before every step (256 MiB write); the state is larger than L2"),
                    "launch": "one persistent cooperative kernel per chunk of up to 4096 colour substeps",
-                   "kernel_shape": launch_info},
+                   "kernel_shape": launch_info, "shape_tuning": tuning},
         "e2e": {"value": e2e, "unit": UNIT,
                 "h2d_bytes_per_step": S * nspec * 16,
                 "d2h_bytes_per_step": system.n * 12,
