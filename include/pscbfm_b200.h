@@ -169,12 +169,6 @@ int bfm_batch_initialize(bfm_batch *b);
  * `size` CTAs: 2, 4 (default; 1 also selects it) or 8; 0 runs every system
  * on one CTA.  Every size gives the same trajectories. */
 int bfm_batch_set_clusters(bfm_batch *b, int size);
-/* words (32-bit) of each cluster CTA's lattice slice and target slice in
- * distributed shared memory: 8192 (default, 64 KB a CTA; 128^3 systems on
- * clusters of 8) or 16384 (128 KB a CTA; 128^3 systems on clusters of 4).
- * A system whose share does not fit keeps its lattices in global memory.
- * Same trajectories either way. */
-int bfm_batch_set_slice_words(bfm_batch *b, uint32_t words);
 /* autotuner: the next bfm_batch_run times, on trial launches (each an
  * eighth of the longest pending work, 2 .. 50 MCS; part of the run, same
  * trajectories), first the cluster sizes 4, 2, 8 and off, then 1 and 4

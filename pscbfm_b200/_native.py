@@ -112,7 +112,6 @@ _SIGS = {
     "bfm_batch_initialize": (_c.c_int, [_P]),
     "bfm_batch_set_clusters": (_c.c_int, [_P, _c.c_int]),
     "bfm_batch_set_autotune": (_c.c_int, [_P, _c.c_int]),
-    "bfm_batch_set_slice_words": (_c.c_int, [_P, _c.c_uint32]),
     "bfm_batch_get_clusters": (_c.c_int, [_P, _P, _P, _P]),
     "bfm_batch_run": (_c.c_int, [_P, _P, _c.c_size_t]),
     "bfm_batch_get_positions": (_c.c_int, [_P, _c.c_uint32, _P, _c.c_size_t]),

@@ -78,12 +78,6 @@ class Batch:
         self._check(self._lib.bfm_batch_get_clusters(self._h, ctypes.byref(size), ctypes.byref(tuned), ns.ctypes.data))
         return {"size": size.value, "tuned": bool(tuned.value), "trial_ns_per_move": dict(zip((4, 2, 8, 0), ns.tolist()))}
 
-    def set_slice_words(self, words: int):
-        """a cluster CTA's lattice slice in distributed shared memory: 8192
-        words (default) or 16384 (128^3 systems on clusters of 4)"""
-        self._check(self._lib.bfm_batch_set_slice_words(self._h, int(words)))
-        return self
-
     def set_shape(self, in_flight: int = 2, clusters_from_48: bool = False):
         """monomers per thread in flight (1, 2, 4); systems of 48^3..64^3 on clusters too"""
         self._check(self._lib.bfm_batch_set_shape(self._h, int(in_flight), int(bool(clusters_from_48))))

@@ -49,7 +49,6 @@ constexpr int kThreads = 512;
 constexpr uint32_t kMaxSpecies = 16;
 constexpr int kInFlight = 2; /* default monomers per thread in flight in the check phase (1 and 4: autotuner candidates) */
 constexpr uint32_t kSmemLatWords = 8192; /* 64^3 sites: lattice and targets of smaller systems in shared memory */
-constexpr uint32_t kWideSliceWords = 16384; /* the cluster kernel's wide slices: 128^3 sites on 4 CTAs */
 constexpr uint32_t kMaxCluster = 16;     /* CTAs of a cluster, at most */
 
 /* one system, read-only during a launch */
@@ -404,9 +403,9 @@ __device__ __forceinline__ uint32_t *cluster_map(uint32_t *p, uint32_t r)
 template <int IF>
 __global__ void __launch_bounds__(kThreads, 2)
     k_batch_cl(const SysDesc *__restrict__ desc, const Work *__restrict__ work, const uint32_t *__restrict__ order,
-               uint32_t nOrder, unsigned int *next, uint32_t *clusterItem, Arrays A, uint32_t sliceCap)
+               uint32_t nOrder, unsigned int *next, uint32_t *clusterItem, Arrays A)
 {
-    extern __shared__ uint32_t dyn[]; /* this CTA's slices: sliceCap occupation + sliceCap target words */
+    extern __shared__ uint32_t dyn[]; /* this CTA's slices: kSmemLatWords occupation + kSmemLatWords targets */
     __shared__ SysDesc s;
     __shared__ uint32_t st[251];
     __shared__ uint32_t s_sp, s_seed;
@@ -416,7 +415,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     const uint32_t first = rank * blockDim.x + tid, stride = cs * blockDim.x;
     if (tid < cs) {
         s_latRank[tid] = cluster_map(dyn, tid);
-        s_tmpRank[tid] = cluster_map(dyn + sliceCap, tid);
+        s_tmpRank[tid] = cluster_map(dyn + kSmemLatWords, tid);
     }
 
     for (;;) {
@@ -441,16 +440,16 @@ __global__ void __launch_bounds__(kThreads, 2)
         /* the lattices in the cluster's distributed shared memory when each
          * CTA's share fits its slices, else in global memory */
         const uint32_t slice = lw / cs;
-        if (slice * cs == lw && slice <= sliceCap && (slice & (slice - 1)) == 0 && slice >= 4) {
+        if (slice * cs == lw && slice <= kSmemLatWords && (slice & (slice - 1)) == 0 && slice >= 4) {
             const uint32_t *g = A.latPool + s.latOff + (size_t)rank * slice;
             for (uint32_t w = tid; w < slice; w += blockDim.x) {
                 dyn[w] = g[w];
-                dyn[sliceCap + w] = 0u;
+                dyn[kSmemLatWords + w] = 0u;
             }
             cluster_barrier();
             const uint32_t sh = 31u - __clz(slice);
             advance<true, IF>(s, st, wk, DistLat{s_latRank, sh, slice - 1u}, DistLat{s_tmpRank, sh, slice - 1u},
-                              dyn + sliceCap, slice, tid, blockDim.x, first, stride, A, s_sp, s_seed, s_att, tid == 0,
+                              dyn + kSmemLatWords, slice, tid, blockDim.x, first, stride, A, s_sp, s_seed, s_att, tid == 0,
                               myCand, myAcc, rank == 0);
             uint32_t *gw = A.latPool + s.latOff + (size_t)rank * slice;
             for (uint32_t w = tid; w < slice; w += blockDim.x) gw[w] = dyn[w];
@@ -667,7 +666,6 @@ struct Batch {
     int clusterSize = 4;     /* CTAs per system with a global-memory lattice; 0: one CTA */
     int inFlight = kInFlight; /* monomers per thread in flight in the check phase: 1, 2 or 4 */
     uint32_t clusterAbove = kSmemLatWords; /* systems with more lattice words go to the cluster kernel */
-    uint32_t sliceWords = kSmemLatWords;   /* a cluster CTA's lattice slice (and target slice), words */
     bool autotune = false;   /* time the launch shapes on the first launches of a run, keep the fastest */
     double tunedNs = 0;      /* ns per attempted move of the configuration chosen so far */
     bool tuned = false;
@@ -924,7 +922,7 @@ struct Batch {
         int perSm = 0;
         for (int f : {1, 2, 4}) {
             BCK(cudaFuncSetAttribute(batchKernel(f), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * kSmemLatWords * 4)));
-            BCK(cudaFuncSetAttribute(clusterKernel(f), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * kWideSliceWords * 4)));
+            BCK(cudaFuncSetAttribute(clusterKernel(f), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * kSmemLatWords * 4)));
         }
         BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_batch<kInFlight>, kThreads, 2 * kSmemLatWords * 4));
         int sms = 0;
@@ -996,7 +994,7 @@ struct Batch {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)cs);
         cfg.blockDim = dim3(kThreads);
-        cfg.dynamicSmemBytes = 2 * (size_t)sliceWords * 4;
+        cfg.dynamicSmemBytes = 2 * kSmemLatWords * 4;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
         attr[0].val.clusterDim.x = (unsigned)cs;
@@ -1143,7 +1141,7 @@ struct Batch {
                 cudaLaunchConfig_t cfg = {};
                 cfg.gridDim = dim3((unsigned)(clusters * (size_t)cs));
                 cfg.blockDim = dim3(kThreads);
-                cfg.dynamicSmemBytes = 2 * (size_t)sliceWords * 4; /* distributed lattice slices */
+                cfg.dynamicSmemBytes = 2 * kSmemLatWords * 4; /* distributed lattice slices */
                 cfg.stream = stream;
                 cudaLaunchAttribute attr[1];
                 attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1158,8 +1156,7 @@ struct Batch {
                 uint32_t a3 = (uint32_t)big.size();
                 unsigned int *a4 = d_next;
                 uint32_t *a5 = d_clItem;
-                uint32_t a6 = sliceWords;
-                void *args[] = {&a0, &a1, &a2, &a3, &a4, &a5, &A, &a6};
+                void *args[] = {&a0, &a1, &a2, &a3, &a4, &a5, &A};
                 BCK(cudaLaunchKernelExC(&cfg, clusterKernel(IF), args));
                 ++lastLaunches;
             }
@@ -1370,15 +1367,6 @@ int bfm_batch_set_clusters(bfm_batch *h, int size)
             throw bfm::ens::ArgErr("cluster size must be 0 (off), 1 (default, 4), 2, 4 or 8");
         h->b.clusterSize = size == 1 ? 4 : size;
         h->b.autotune = false;
-    });
-}
-
-int bfm_batch_set_slice_words(bfm_batch *h, uint32_t words)
-{
-    BGUARD(h, {
-        if (words != bfm::ens::kSmemLatWords && words != bfm::ens::kWideSliceWords)
-            throw bfm::ens::ArgErr("slice words must be 8192 or 16384");
-        h->b.sliceWords = words;
     });
 }
 

@@ -106,18 +106,15 @@ def _run_oracle(s, rng, age, sort_every, st, calls):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("clusters", [4, 0, 2, 8, "auto", "4 wide slices"])
+@pytest.mark.parametrize("clusters", [4, 0, 2, 8, "auto"])
 def test_batch_matches_oracle_and_single_runs(clusters):
-    """the 128^3 system shared by a cluster of 4, 2 or 8 CTAs (on 4 with its
-    lattices in 16384-word distributed shared-memory slices), run by one
-    CTA, or by the size the autotuner picks after timing all four on the
-    first launches of the run: the trajectories are the same"""
+    """the 128^3 system shared by a cluster of 4, 2 or 8 CTAs, run by one CTA,
+    or by the size the autotuner picks after timing all four on the first
+    launches of the run: the trajectories are the same"""
     made = [(make(), rng, age, se) for make, rng, age, se in CASES]
     b = pb.Batch()
     if clusters == "auto":
         b.set_autotune(True)
-    elif clusters == "4 wide slices":
-        b.set_clusters(4).set_slice_words(16384)
     else:
         b.set_clusters(clusters)
     states = [oracle.r250_state(100 + i) for i in range(len(made))]
@@ -152,8 +149,6 @@ def test_batch_matches_oracle_and_single_runs(clusters):
         assert t["tuned"] and t["in_flight"] in (1, 2, 4) and t["cluster_above_words"] in (1024, 8192)
         # every stage ran: the 64^3 system makes the threshold trial count too
         assert all(v > 0 for v in t["trial_ns_per_move"].values())
-    elif clusters == "4 wide slices":
-        assert info["size"] == 4
     else:
         assert info["size"] == clusters
 
