@@ -290,13 +290,15 @@ int bfm_get_launch_info(const bfm_handle *h, int *mode, int *grid, int *threads,
 int bfm_set_sweep_shape(bfm_handle *h, int shape);
 /* launch-shape autotuner (no counterpart in the reference, whose launch
  * configuration is fixed, UpdaterGPUScBFM_AB_Type.cu:2952-2981): with `on`,
- * the first schedule chunk of the next run is split into equal trial
- * launches of the automatic shape, the windowed shapes 6..10, the stored and
- * staged shapes 1, 2 and the windowed shape with one more round of items per
- * thread (smaller CTAs), each timed with events; the trials are part of the
- * run (every shape gives the same trajectory) and the fastest per attempted
- * move is kept unless the automatic shape is within 3% of it.  Shapes that
- * do not fit the system are skipped. */
+ * the first schedule chunk of the next run is split into equal pieces: one
+ * untimed piece of the automatic shape (warm caches), then two rounds of
+ * trial launches of the automatic shape, the windowed shapes 6..10, the
+ * stored and staged shapes 1, 2 and the windowed shape with one more round
+ * of items per thread (smaller CTAs), each timed with events, each shape
+ * keeping the faster of its two; the trials are part of the run (every
+ * shape gives the same trajectory) and the fastest per attempted move is
+ * kept unless the automatic shape is within 3% of it.  Shapes that do not
+ * fit the system are skipped. */
 int bfm_set_sweep_autotune(bfm_handle *h, int on);
 /* the autotuner's trials (up to cap): shape, extra rounds, threads per CTA
  * and ns per attempted move; *tuned = 1 once it has chosen */

@@ -1877,7 +1877,11 @@ struct Engine {
     }
 
     /* the autotuner's trials on substeps [0, m) of the uploaded chunk, then
-     * the rest of the chunk with the chosen shape; returns the launches */
+     * the rest of the chunk with the chosen shape; returns the launches.  A
+     * first piece with the automatic shape warms the caches (untimed); then
+     * every candidate runs two timed pieces, in two rounds, and keeps the
+     * faster -- so neither the cold start nor a drift of the acceptance
+     * rate along the chunk favours one shape. */
     uint64_t tuneShapes(const Substep *sched, const Substep *hs, uint32_t m)
     {
         const int savedShape = forcedShape, savedExtra = extraRounds;
@@ -1887,13 +1891,8 @@ struct Engine {
         for (int sh : {6, 7, 8, 9, 10, 1, 2})
             if (sh != autoMode) cand.push_back({sh, 0});
         cand.push_back({autoMode >= SWEEP_WINDOWED ? autoMode : 7, 1});
-        const uint32_t piece = std::max<uint32_t>(1, m / (uint32_t)(cand.size() + 1) / nSpecies) * nSpecies;
-        uint32_t k = 0;
-        uint64_t launches = 0;
-        trials.clear();
-        std::vector<cudaEvent_t> ev;
+        std::vector<std::pair<int, int>> ok;
         for (auto &c : cand) {
-            if (k + piece > m) break;
             forcedShape = c.first;
             extraRounds = c.second;
             try {
@@ -1901,29 +1900,59 @@ struct Engine {
             } catch (std::runtime_error const &) {
                 continue; /* this shape does not fit the system */
             }
-            cudaEvent_t e0, e1;
-            CK(cudaEventCreate(&e0));
-            CK(cudaEventCreate(&e1));
-            ev.push_back(e0);
-            ev.push_back(e1);
-            CK(cudaEventRecord(e0, stream));
+            ok.push_back(c);
+        }
+        const uint32_t pieces = 2u * (uint32_t)ok.size() + 1u;
+        const uint32_t piece = std::max<uint32_t>(1, m / pieces / nSpecies) * nSpecies;
+        uint32_t k = 0;
+        uint64_t launches = 0;
+        trials.clear();
+        std::vector<cudaEvent_t> ev;
+        std::vector<uint64_t> att;
+        std::vector<size_t> who;
+        auto use = [&](const std::pair<int, int> &c) {
+            forcedShape = c.first;
+            extraRounds = c.second;
+            configureSweep();
+        };
+        if (!ok.empty() && k + piece <= m) { /* warm-up piece, untimed */
+            use(ok[0]);
             launchSweep(sched, k, k + piece);
-            CK(cudaEventRecord(e1, stream));
             ++launches;
-            uint64_t att = 0;
-            for (uint32_t j = k; j < k + piece; ++j) att += spec[hs[j].species].n;
-            trials.push_back({c.first < 0 ? sweepMode : c.first, c.second, sweepThreads, (double)att});
             k += piece;
         }
+        for (int round = 0; round < 2; ++round)
+            for (size_t ci = 0; ci < ok.size(); ++ci) {
+                if (k + piece > m) break;
+                use(ok[ci]);
+                if (round == 0) trials.push_back({ok[ci].first < 0 ? sweepMode : ok[ci].first, ok[ci].second, sweepThreads, 0.0});
+                cudaEvent_t e0, e1;
+                CK(cudaEventCreate(&e0));
+                CK(cudaEventCreate(&e1));
+                ev.push_back(e0);
+                ev.push_back(e1);
+                CK(cudaEventRecord(e0, stream));
+                launchSweep(sched, k, k + piece);
+                CK(cudaEventRecord(e1, stream));
+                ++launches;
+                uint64_t a = 0;
+                for (uint32_t j = k; j < k + piece; ++j) a += spec[hs[j].species].n;
+                att.push_back(a);
+                who.push_back(ci);
+                k += piece;
+            }
         CK(cudaStreamSynchronize(stream));
-        size_t best = 0;
-        for (size_t i = 0; i < trials.size(); ++i) {
+        for (size_t t = 0; t < who.size(); ++t) {
             float ms = 0;
-            CK(cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]));
-            trials[i].nsPerMove = ms * 1e6 / std::max(trials[i].nsPerMove, 1.0);
-            if (trials[i].nsPerMove < trials[best].nsPerMove) best = i;
+            CK(cudaEventElapsedTime(&ms, ev[2 * t], ev[2 * t + 1]));
+            const double ns = ms * 1e6 / std::max<double>((double)att[t], 1.0);
+            double &best = trials[who[t]].nsPerMove;
+            if (best == 0.0 || ns < best) best = ns;
         }
         for (auto e : ev) cudaEventDestroy(e);
+        size_t best = 0;
+        for (size_t i = 0; i < trials.size(); ++i)
+            if (trials[i].nsPerMove > 0.0 && trials[i].nsPerMove < trials[best].nsPerMove) best = i;
         /* keep the automatic shape unless another is more than 3% faster */
         if (!trials.empty() && trials[best].nsPerMove < 0.97 * trials[0].nsPerMove) {
             forcedShape = trials[best].shape;
