@@ -363,6 +363,17 @@ class EndRecorder:
         self.nsys = len(mols)
         self.count = np.bincount(self.vsys, minlength=self.nsys).astype(np.float64)
 
+    def re2_of(self, i, pos):
+        """R_e^2 of system i from its whole position array (original ids)"""
+        sel = np.flatnonzero(self.sel_s == i)
+        p = np.asarray(pos, np.float64)[self.sel_i[sel]]
+        vm = self.vsys == i
+        a, b = self.a[vm] - sel[0], self.b[vm] - sel[0]
+        v = p[b] - p[a]
+        # summed in the same order as `snapshot`, so the values are identical
+        w = np.bincount(np.zeros(len(v), np.int64), weights=(v * v).sum(1), minlength=1)[0]
+        return float(w / max(self.count[i], 1))
+
     def snapshot(self, batch, batch_index=None):
         """(R_e^2 per system, end vectors of the first max_vectors molecules
         of each system); batch_index[i]: the batch's index of system i when
@@ -379,18 +390,29 @@ def round_up(x, every):
 
 
 def live_run(systems_, r250_seeds, budgets, every: int, recorder, max_mcs: int | None = None, grow: float = 1.5,
-             judge: bool = True, order=None, gpu: int = 0):
+             judge: bool = True, order=None, gpu: int = 0, solo_tail: int = 0, sort_every: int = 5000, report=None):
     """Run an ensemble live on the GPU under per-system budgets: system i
     advances `every` MCS per batched launch until its budget is spent; its
     R_e^2 is recorded after every launch; when the budget is spent and the
     drift check (`drifting`, on the second half of its own series) sees the
     run still relaxing, the budget grows by `grow` (up to max_mcs) and the
     system goes on.  Systems are added to the batch in `order` (admission:
-    longest predicted work first).  Returns (wall seconds, per-system MCS
-    run, per-system series {t, re2}, attempted moves, device ms)."""
+    longest predicted work first).
+
+    Tail: once at most `solo_tail` systems are left in the batch, the ones
+    whose box edges are powers of two leave it at their next sorting point
+    (age a multiple of `sort_every`, where the batch and the single-system
+    updater both re-sort by the same keys) and go on, one after another, on
+    the single-system updater -- the whole GPU per system -- from the
+    batch's positions, age and R250 state, on the same trajectory.  Returns
+    (wall seconds, per-system MCS run, per-system series {t, re2},
+    attempted moves, device ms); `report` (a dict) receives the systems
+    moved to the single-system updater."""
     import time
 
+    from . import updater as upd
     from .batch import Batch
+    from .systems import System
     from .updater import Rng
     nsys = len(systems_)
     order = np.arange(nsys) if order is None else np.asarray(order)
@@ -410,24 +432,64 @@ def live_run(systems_, r250_seeds, budgets, every: int, recorder, max_mcs: int |
     for i in range(nsys):
         series[i]["re2"].append(float(re2[i]))
     moves, dev_ms = 0, 0.0
+    solo = {}  # system -> [single-system updater, its R250 state]
+    pow2 = np.array([all(v > 0 and (v & (v - 1)) == 0 for v in s.box) for s in systems_])
     t0 = time.perf_counter()
+
+    def judged(i):
+        if remaining[i] == 0 and judge and ran[i] < cap[i]:
+            s_ = {"t": np.asarray(series[i]["t"]), "re2": np.asarray(series[i]["re2"])}
+            if drifting(s_, float(ran[i])):
+                remaining[i] = min(round_up(ran[i] * grow, every), cap[i]) - ran[i]
+
     while (remaining > 0).any():
-        step = np.where(remaining > 0, every, 0).astype(np.uint32)
-        b.run(step[order])
-        info = b.info()
-        moves += info["last_attempts"]
-        dev_ms += info["last_ms"]
-        ran += step
-        remaining -= step
-        re2, _ = rec.snapshot(b, pos_in_batch)
-        for i in np.flatnonzero(step):
+        in_batch = (remaining > 0) & np.array([i not in solo for i in range(nsys)])
+        if solo_tail and 0 < in_batch.sum() <= solo_tail:
+            for i in np.flatnonzero(in_batch & pow2):
+                if ran[i] % sort_every:
+                    continue
+                j = int(pos_in_batch[i])
+                pos = b.positions(j)
+                age, st, _ = b.state(j)
+                s0 = systems_[i]
+                si = System(s0.box, np.ascontiguousarray(pos, dtype=np.int32), s0.deg, s0.nbr, s0.allowed, s0.chains,
+                            s0.attributes, s0.name)
+                upd.r250_set_state(st)
+                u = upd.UpdaterGPUScBFM_AB_Type().setup(si, gpu=gpu, rng=Rng.Saru, age=int(age),
+                                                       steps_between_sortings=sort_every)
+                solo[i] = [u, upd.r250_get_state()]
+                in_batch[i] = False
+        step = np.where(in_batch, every, 0).astype(np.uint32)
+        if step.any():
+            b.run(step[order])
+            info = b.info()
+            moves += info["last_attempts"]
+            dev_ms += info["last_ms"]
+            ran += step
+            remaining -= step
+            re2, _ = rec.snapshot(b, pos_in_batch)
+            for i in np.flatnonzero(step):
+                series[i]["t"].append(float(ran[i]))
+                series[i]["re2"].append(float(re2[i]))
+                judged(i)
+        for i, (u, st) in solo.items():
+            if remaining[i] <= 0:
+                continue
+            upd.r250_set_state(st)
+            u.runSimulationOnGPU(every)
+            solo[i][1] = upd.r250_get_state()
+            moves += systems_[i].n * every
+            dev_ms += u.getLastRunMs()
+            ran[i] += every
+            remaining[i] -= every
             series[i]["t"].append(float(ran[i]))
-            series[i]["re2"].append(float(re2[i]))
-            if remaining[i] == 0 and judge and ran[i] < cap[i]:
-                s = {"t": np.asarray(series[i]["t"]), "re2": np.asarray(series[i]["re2"])}
-                if drifting(s, float(ran[i])):
-                    remaining[i] = min(round_up(ran[i] * grow, every), cap[i]) - ran[i]
+            series[i]["re2"].append(rec.re2_of(i, u.getAllMonomerPositions()))
+            judged(i)
     wall = time.perf_counter() - t0
+    for u, _ in solo.values():
+        u.cleanup()
+    if report is not None:
+        report["moved_to_single_system"] = len(solo)
     b.close()
     for s in series:
         s["t"] = np.asarray(s["t"])
@@ -489,7 +551,8 @@ def record_live(params, total_mcs: int, every: int, seed: int = 0, gpu: int = 0,
 
 
 def live_compare(n_systems: int = 2048, mcs: int = 200000, every: int = 1000, test_fraction: float = 0.25, epochs: int = 300,
-                 seed: int = 3, gpu: int = 0, boxes=(32, 48, 64, 96, 128), n_range=(16, 512), phi_range=(0.1, 0.5)):
+                 seed: int = 3, gpu: int = 0, boxes=(32, 48, 64, 96, 128), n_range=(16, 512), phi_range=(0.1, 0.5),
+                 solo_tail: int = 16):
     """The learned schedule run live against plain fixed budgets.
 
     An ensemble of the batched configuration's ranges is recorded for `mcs`
@@ -552,7 +615,9 @@ def live_compare(n_systems: int = 2048, mcs: int = 200000, every: int = 1000, te
     budgets = np.maximum(200.0, factor * 10.0 ** pred[:, 3])
     order = admission_order(pred[:, 3], [s.n for s in test_sys])
     rec = EndRecorder(mols)
-    wall_l, ran_l, ser_l, moves_l, dev_l = live_run(test_sys, seeds, budgets, every, rec, max_mcs=mcs, order=order, gpu=gpu)
+    rep_l, rep_p = {}, {}
+    wall_l, ran_l, ser_l, moves_l, dev_l = live_run(test_sys, seeds, budgets, every, rec, max_mcs=mcs, order=order, gpu=gpu,
+                                                    solo_tail=solo_tail, report=rep_l)
     est_l = np.array([window_estimate(s, float(r)) for s, r in zip(ser_l, ran_l)])
     rel_l = (est_l - truth) / truth
     # the live runs start from the recorded systems' initial states with the
@@ -569,7 +634,8 @@ def live_compare(n_systems: int = 2048, mcs: int = 200000, every: int = 1000, te
         if abs(rel.mean()) <= target:
             B = float(b_)
             break
-    wall_p, ran_p, ser_p, moves_p, dev_p = live_run(test_sys, seeds, np.full(len(te_a), B), every, rec, judge=False, gpu=gpu)
+    wall_p, ran_p, ser_p, moves_p, dev_p = live_run(test_sys, seeds, np.full(len(te_a), B), every, rec, judge=False, gpu=gpu,
+                                                    solo_tail=solo_tail, report=rep_p)
     est_p = np.array([window_estimate(s, float(r)) for s, r in zip(ser_p, ran_p)])
     rel_p = (est_p - truth) / truth
     # ensemble R_e^2 / N over molecules against the full-length runs
@@ -593,10 +659,12 @@ def live_compare(n_systems: int = 2048, mcs: int = 200000, every: int = 1000, te
         "learned": {"wall_s": wall_l, "device_s": dev_l / 1e3, "moves": int(moves_l), "mean_mcs": float(ran_l.mean()),
                     "extended": int(np.sum(ran_l > np.array([round_up(v, every) for v in np.minimum(budgets, mcs)]))),
                     "bias_re2": float(rel_l.mean()), "mean_abs_rel_err_re2": float(np.abs(rel_l).mean()),
-                    "ensemble_re2_per_n_vs_full": ens(est_l) / ens(est_full) - 1.0},
+                    "ensemble_re2_per_n_vs_full": ens(est_l) / ens(est_full) - 1.0,
+                    "moved_to_single_system": rep_l.get("moved_to_single_system", 0)},
         "plain": {"budget_mcs": B, "wall_s": wall_p, "device_s": dev_p / 1e3, "moves": int(moves_p),
                   "bias_re2": float(rel_p.mean()), "mean_abs_rel_err_re2": float(np.abs(rel_p).mean()),
-                  "ensemble_re2_per_n_vs_full": ens(est_p) / ens(est_full) - 1.0},
+                  "ensemble_re2_per_n_vs_full": ens(est_p) / ens(est_full) - 1.0,
+                  "moved_to_single_system": rep_p.get("moved_to_single_system", 0)},
         "solo": {"moves_per_s": solo, "wall_s_estimate": solo_wall},
         "systems_per_hour": {"learned": len(te_a) / wall_l * 3600.0, "plain": len(te_a) / wall_p * 3600.0,
                              "solo": (len(te_a) / solo_wall * 3600.0) if solo_wall else None},

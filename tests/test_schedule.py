@@ -298,9 +298,83 @@ def test_live_compare_plumbing_on_the_cpu(monkeypatch):
     monkeypatch.setattr(batch_mod, "Batch", _DetBatch)
     monkeypatch.setattr(sch, "Surrogate", Stand)
     monkeypatch.setattr(sch, "solo_rate", lambda *a, **k: 1e9)
-    rep = sch.live_compare(n_systems=40, mcs=6000, every=200, epochs=1, seed=5, boxes=(16, 24, 32), n_range=(8, 32))
+    rep = sch.live_compare(n_systems=40, mcs=6000, every=200, epochs=1, seed=5, boxes=(16, 24, 32), n_range=(8, 32),
+                           solo_tail=0)
     assert rep["test_systems"] == 10 and rep["test_systems_assessed"] >= 1
     assert rep["learned"]["wall_s"] > 0 and rep["plain"]["wall_s"] > 0
     assert rep["plain"]["budget_mcs"] > 0 and rep["ratio_learned_vs_plain"] > 0
     assert rep["budget_factor"] in (2.0, 3.0, 4.0, 6.0, 8.0, 12.0, 16.0)
     assert rep["systems_per_hour"]["learned"] > 0
+
+
+def test_live_run_moves_the_tail_to_the_single_system_updater(monkeypatch):
+    """with few systems left in the batch, the power-of-two ones continue on
+    the single-system updater from the batch's positions, age and R250
+    state at a sorting point; stand-ins with a trajectory fixed by (seed,
+    MCS) show that every series and budget is the same as without the move,
+    and that R_e^2 from whole positions equals the batch's gathered value"""
+    import pscbfm_b200.batch as batch_mod
+    import pscbfm_b200.updater as upd
+
+    class Batch(_DetBatch):
+        def add(self, system, rng=None, r250_seed=0):
+            glob["orig"][int(r250_seed)] = system      # the stand-in's trajectory is relative to the start
+            return super().add(system, rng=rng, r250_seed=r250_seed)
+
+        current = {}
+
+        def positions(self, j):
+            p = self._pos(j)
+            Batch.current[self.seed[j]] = p
+            return p
+
+        def state(self, j):
+            st = np.zeros(251, np.uint32)
+            st[0] = self.seed[j]
+            return self.t[j], st, (0, 0, 0)
+
+    glob = {"st": np.zeros(251, np.uint32), "orig": {}}
+    created = []
+
+    class Updater:
+        def setup(self, system, gpu=0, rng=None, age=0, steps_between_sortings=5000):
+            self.b = _DetBatch()
+            seed = int(glob["st"][0])
+            assert np.array_equal(system.pos, Batch.current[seed])   # handed the batch's positions
+            self.b.add(glob["orig"][seed], r250_seed=seed)
+            self.b.t[0] = int(age)
+            created.append(self)
+            return self
+
+        def runSimulationOnGPU(self, m):
+            self.b.run(m)
+
+        def getLastRunMs(self):
+            return 0.1
+
+        def getAllMonomerPositions(self):
+            return self.b._pos(0)
+
+        def cleanup(self):
+            pass
+
+    monkeypatch.setattr(batch_mod, "Batch", Batch)
+    monkeypatch.setattr(upd, "UpdaterGPUScBFM_AB_Type", Updater)
+    monkeypatch.setattr(upd, "r250_set_state", lambda st: glob.__setitem__("st", np.array(st, np.uint32)))
+    monkeypatch.setattr(upd, "r250_get_state", lambda: glob["st"].copy())
+    sys_ = [systems.ensemble_system(L, n, 0.3, False, seed=10 + k) for k, (L, n) in enumerate([(16, 12), (24, 16), (16, 20), (32, 16)])]
+    mols = [sch.molecules(s, n, False) for s, n in zip(sys_, (12, 16, 20, 16))]
+    budgets = [1000, 3000, 6000, 6000]
+    runs = []
+    for tail in (0, 2):
+        rec = sch.EndRecorder(mols)
+        rep = {}
+        runs.append(sch.live_run(sys_, [1, 2, 3, 4], budgets, 200, rec, max_mcs=20000, solo_tail=tail, sort_every=1000,
+                                 report=rep) + (rep,))
+    (w0, ran0, ser0, mv0, _, _), (w1, ran1, ser1, mv1, _, rep1) = runs
+    assert rep1["moved_to_single_system"] >= 1 and len(created) == rep1["moved_to_single_system"]
+    assert np.array_equal(ran0, ran1) and mv0 == mv1
+    for a, b in zip(ser0, ser1):
+        assert np.array_equal(a["t"], b["t"]) and np.array_equal(a["re2"], b["re2"])
+    # only power-of-two boxes move (the 24^3 system stays in the batch)
+    assert all(all((v & (v - 1)) == 0 for v in u.b.sys[0].box) for u in created)
