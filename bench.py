@@ -94,6 +94,10 @@ def parse():
                         "systems (batched-ensemble ranges), recorded for --schedule-mcs MCS")
     p.add_argument("--schedule-mcs", type=int, default=100000)
     p.add_argument("--schedule-every", type=int, default=500)
+    p.add_argument("--schedule-solo-tail", type=int, default=16,
+                   help="systems left in the batch at which power-of-two ones move to the single-system updater")
+    p.add_argument("--schedule-solo-tail-alt", default="",
+                   help="comma-separated other thresholds to time the learned schedule with as well")
     a = p.parse_args()
     cfg = CONFIGS[a.config]
     if a.mcs_per_step is None:
@@ -560,7 +564,9 @@ def run_schedule(args, ranks):
     torch.cuda.set_device(ranks.local)
     clocks = Clocks(ranks.local)
     clocks.start()
-    rep = sch.live_compare(args.schedule, args.schedule_mcs, args.schedule_every, gpu=ranks.local)
+    rep = sch.live_compare(args.schedule, args.schedule_mcs, args.schedule_every, gpu=ranks.local,
+                           solo_tail=args.schedule_solo_tail,
+                           solo_tail_alternatives=[int(v) for v in args.schedule_solo_tail_alt.split(",") if v])
     clk = clocks.stop()
     line = {"metric": "systems equilibrated per hour on 1 B200, learned schedule vs plain fixed budget at equal R_e^2 bias",
             "value": rep["systems_per_hour"]["learned"], "unit": "systems/hour", "n_gpus": 1, "higher_is_better": True,

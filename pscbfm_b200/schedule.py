@@ -433,6 +433,7 @@ def live_run(systems_, r250_seeds, budgets, every: int, recorder, max_mcs: int |
         series[i]["re2"].append(float(re2[i]))
     moves, dev_ms = 0, 0.0
     solo = {}  # system -> [single-system updater, its R250 state]
+    launches = []  # (systems in the launch, device ms) per batched launch
     pow2 = np.array([all(v > 0 and (v & (v - 1)) == 0 for v in s.box) for s in systems_])
     t0 = time.perf_counter()
 
@@ -465,6 +466,7 @@ def live_run(systems_, r250_seeds, budgets, every: int, recorder, max_mcs: int |
             info = b.info()
             moves += info["last_attempts"]
             dev_ms += info["last_ms"]
+            launches.append((int(in_batch.sum()), float(info["last_ms"])))
             ran += step
             remaining -= step
             re2, _ = rec.snapshot(b, pos_in_batch)
@@ -490,6 +492,11 @@ def live_run(systems_, r250_seeds, budgets, every: int, recorder, max_mcs: int |
         u.cleanup()
     if report is not None:
         report["moved_to_single_system"] = len(solo)
+        act = np.array([a for a, _ in launches], np.int64)
+        ms = np.array([m for _, m in launches], np.float64)
+        report["batched_launches"] = len(launches)
+        report["device_ms_by_systems_in_launch"] = {f"<={k}": float(ms[act <= k].sum()) for k in (8, 16, 32, 64, 128)}
+        report["device_ms_by_systems_in_launch"]["all"] = float(ms.sum())
     b.close()
     for s in series:
         s["t"] = np.asarray(s["t"])
@@ -552,7 +559,7 @@ def record_live(params, total_mcs: int, every: int, seed: int = 0, gpu: int = 0,
 
 def live_compare(n_systems: int = 2048, mcs: int = 200000, every: int = 1000, test_fraction: float = 0.25, epochs: int = 300,
                  seed: int = 3, gpu: int = 0, boxes=(32, 48, 64, 96, 128), n_range=(16, 512), phi_range=(0.1, 0.5),
-                 solo_tail: int = 16):
+                 solo_tail: int = 16, solo_tail_alternatives=()):
     """The learned schedule run live against plain fixed budgets.
 
     An ensemble of the batched configuration's ranges is recorded for `mcs`
@@ -619,6 +626,14 @@ def live_compare(n_systems: int = 2048, mcs: int = 200000, every: int = 1000, te
     wall_l, ran_l, ser_l, moves_l, dev_l = live_run(test_sys, seeds, budgets, every, rec, max_mcs=mcs, order=order, gpu=gpu,
                                                     solo_tail=solo_tail, report=rep_l)
     est_l = np.array([window_estimate(s, float(r)) for s, r in zip(ser_l, ran_l)])
+    # the same learned schedule with other tail thresholds (same trajectories, other executors)
+    alternatives = {}
+    for k in solo_tail_alternatives:
+        rep_k = {}
+        w_k, ran_k, _, mv_k, dev_k = live_run(test_sys, seeds, budgets, every, rec, max_mcs=mcs, order=order, gpu=gpu,
+                                              solo_tail=int(k), report=rep_k)
+        alternatives[str(int(k))] = {"wall_s": w_k, "device_s": dev_k / 1e3, "moves": int(mv_k),
+                                     "same_mcs": bool(np.array_equal(ran_k, ran_l)), **rep_k}
     rel_l = (est_l - truth) / truth
     # the live runs start from the recorded systems' initial states with the
     # same seeds, so (bit-exact simulation) their R_e^2 series are prefixes of
@@ -660,15 +675,20 @@ def live_compare(n_systems: int = 2048, mcs: int = 200000, every: int = 1000, te
                     "extended": int(np.sum(ran_l > np.array([round_up(v, every) for v in np.minimum(budgets, mcs)]))),
                     "bias_re2": float(rel_l.mean()), "mean_abs_rel_err_re2": float(np.abs(rel_l).mean()),
                     "ensemble_re2_per_n_vs_full": ens(est_l) / ens(est_full) - 1.0,
-                    "moved_to_single_system": rep_l.get("moved_to_single_system", 0)},
+                    "moved_to_single_system": rep_l.get("moved_to_single_system", 0),
+                    "batched_launches": rep_l.get("batched_launches"),
+                    "device_ms_by_systems_in_launch": rep_l.get("device_ms_by_systems_in_launch")},
         "plain": {"budget_mcs": B, "wall_s": wall_p, "device_s": dev_p / 1e3, "moves": int(moves_p),
                   "bias_re2": float(rel_p.mean()), "mean_abs_rel_err_re2": float(np.abs(rel_p).mean()),
                   "ensemble_re2_per_n_vs_full": ens(est_p) / ens(est_full) - 1.0,
-                  "moved_to_single_system": rep_p.get("moved_to_single_system", 0)},
+                  "moved_to_single_system": rep_p.get("moved_to_single_system", 0),
+                  "batched_launches": rep_p.get("batched_launches"),
+                  "device_ms_by_systems_in_launch": rep_p.get("device_ms_by_systems_in_launch")},
         "solo": {"moves_per_s": solo, "wall_s_estimate": solo_wall},
         "systems_per_hour": {"learned": len(te_a) / wall_l * 3600.0, "plain": len(te_a) / wall_p * 3600.0,
                              "solo": (len(te_a) / solo_wall * 3600.0) if solo_wall else None},
         "live_runs_reproduce_the_record": bool(prefix),
+        "learned_with_other_tail_thresholds": alternatives,
         "ratio_learned_vs_plain": wall_p / wall_l,
         "ratio_learned_vs_solo": (solo_wall / wall_l) if solo_wall else None,
     }
