@@ -30,6 +30,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -1142,6 +1143,25 @@ struct DeviceTimeout : std::runtime_error {
             throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_));                          \
     } while (0)
 
+/* The dynamic shared-memory limit of a kernel is an attribute of the
+ * function on a device, shared by every handle of the process; handles
+ * configured for different system sizes would otherwise lower each
+ * other's limit below what their own launches request.  It is only ever
+ * raised. */
+void raise_smem_limit(const void *fn, size_t bytes)
+{
+    static std::mutex mu;
+    static std::map<std::pair<int, const void *>, size_t> limit;
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    size_t &cur = limit[{dev, fn}];
+    if (bytes > cur) {
+        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        cur = bytes;
+    }
+}
+
 template <typename T>
 void dalloc(T *&p, size_t n)
 {
@@ -1593,7 +1613,7 @@ struct Engine {
             if ((size_t)cap * sizeof(uint2) > kSweepSmemListMax) globalList = true;
             if (!globalList) smem += (size_t)cap * sizeof(uint2);
         }
-        CK(cudaFuncSetAttribute(k_sweep<RNG, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        raise_smem_limit((const void *)k_sweep<RNG, MODE>, smem);
         int fit = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k_sweep<RNG, MODE>, kSweepThreads, smem));
         if (fit < 1) return false;
@@ -1631,7 +1651,7 @@ struct Engine {
         const size_t smem = WinLayout{W, threads, P}.bytes();
         if (smem > smemLimit) return false;
         const void *fn = win_kernel<RNG>(variant);
-        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        raise_smem_limit(fn, smem);
         int fit = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, fn, (int)threads, smem));
         if (fit < 1) return false;

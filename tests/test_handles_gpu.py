@@ -60,3 +60,26 @@ def test_two_handles_stepped_alternately():
         ob.run(nmcs, st)
         assert np.array_equal(ua.getAllMonomerPositions(), oa.positions())
         assert np.array_equal(ub.getAllMonomerPositions(), ob.positions())
+
+
+def test_handles_of_different_sizes_share_the_kernels():
+    """Two handles with the same generator use the same kernel functions,
+    whose dynamic shared-memory limit is per function: a handle configured
+    for a small system after one for a large system must not lower the
+    limit below the large one's launches (it is only ever raised)."""
+    big = systems.ordered_melt(64)
+    small = systems.saw_chains(12, 8, box=(16, 16, 16), seed=105)
+    pb.r250_seed(8)
+    st = pb.r250_get_state()
+    ub = pb.UpdaterGPUScBFM_AB_Type().setup(big, rng=pb.Rng.Saru)
+    us = pb.UpdaterGPUScBFM_AB_Type().setup(small, rng=pb.Rng.Saru)
+    assert ub.getLaunchInfo()["smem_bytes"] > us.getLaunchInfo()["smem_bytes"]
+    ob = oracle.Sweep(big, rng=2, threads=4)
+    osm = oracle.Sweep(small, rng=2, threads=4)
+    for nmcs in (15, 30):
+        ub.runSimulationOnGPU(nmcs)
+        ob.run(nmcs, st)
+        us.runSimulationOnGPU(nmcs)
+        osm.run(nmcs, st)
+        assert np.array_equal(ub.getAllMonomerPositions(), ob.positions())
+        assert np.array_equal(us.getAllMonomerPositions(), osm.positions())
