@@ -390,7 +390,8 @@ def round_up(x, every):
 
 
 def live_run(systems_, r250_seeds, budgets, every: int, recorder, max_mcs: int | None = None, grow: float = 1.5,
-             judge: bool = True, order=None, gpu: int = 0, solo_tail: int = 0, sort_every: int = 5000, report=None):
+             judge: bool = True, order=None, gpu: int = 0, solo_tail: int = 0, sort_every: int = 5000, report=None,
+             solo_min_monomers: int = 16384):
     """Run an ensemble live on the GPU under per-system budgets: system i
     advances `every` MCS per batched launch until its budget is spent; its
     R_e^2 is recorded after every launch; when the budget is spent and the
@@ -400,7 +401,10 @@ def live_run(systems_, r250_seeds, budgets, every: int, recorder, max_mcs: int |
     longest predicted work first).
 
     Tail: once at most `solo_tail` systems are left in the batch, the ones
-    whose box edges are powers of two leave it at their next sorting point
+    of at least `solo_min_monomers` monomers (where one system on the whole
+    GPU runs many times faster than on its share of the batch; smaller ones
+    run as fast in parallel in the batch) whose box edges are powers of two
+    leave it at their next sorting point
     (age a multiple of `sort_every`, where the batch and the single-system
     updater both re-sort by the same keys) and go on, one after another, on
     the single-system updater -- the whole GPU per system -- from the
@@ -434,7 +438,7 @@ def live_run(systems_, r250_seeds, budgets, every: int, recorder, max_mcs: int |
     moves, dev_ms = 0, 0.0
     solo = {}  # system -> [single-system updater, its R250 state]
     launches = []  # (systems in the launch, device ms) per batched launch
-    pow2 = np.array([all(v > 0 and (v & (v - 1)) == 0 for v in s.box) for s in systems_])
+    pow2 = np.array([all(v > 0 and (v & (v - 1)) == 0 for v in s.box) and s.n >= solo_min_monomers for s in systems_])
     t0 = time.perf_counter()
 
     def judged(i):

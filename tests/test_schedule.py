@@ -370,7 +370,7 @@ def test_live_run_moves_the_tail_to_the_single_system_updater(monkeypatch):
         rec = sch.EndRecorder(mols)
         rep = {}
         runs.append(sch.live_run(sys_, [1, 2, 3, 4], budgets, 200, rec, max_mcs=20000, solo_tail=tail, sort_every=1000,
-                                 report=rep) + (rep,))
+                                 report=rep, solo_min_monomers=0) + (rep,))
     (w0, ran0, ser0, mv0, _, _), (w1, ran1, ser1, mv1, _, rep1) = runs
     assert rep1["moved_to_single_system"] >= 1 and len(created) == rep1["moved_to_single_system"]
     assert np.array_equal(ran0, ran1) and mv0 == mv1
