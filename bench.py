@@ -94,7 +94,7 @@ def parse():
                         "systems (batched-ensemble ranges), recorded for --schedule-mcs MCS")
     p.add_argument("--schedule-mcs", type=int, default=100000)
     p.add_argument("--schedule-every", type=int, default=500)
-    p.add_argument("--schedule-solo-tail", type=int, default=16,
+    p.add_argument("--schedule-solo-tail", type=int, default=0,
                    help="systems left in the batch at which power-of-two ones move to the single-system updater")
     p.add_argument("--schedule-solo-tail-alt", default="",
                    help="comma-separated other thresholds to time the learned schedule with as well")

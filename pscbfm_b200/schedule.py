@@ -563,7 +563,7 @@ def record_live(params, total_mcs: int, every: int, seed: int = 0, gpu: int = 0,
 
 def live_compare(n_systems: int = 2048, mcs: int = 200000, every: int = 1000, test_fraction: float = 0.25, epochs: int = 300,
                  seed: int = 3, gpu: int = 0, boxes=(32, 48, 64, 96, 128), n_range=(16, 512), phi_range=(0.1, 0.5),
-                 solo_tail: int = 16, solo_tail_alternatives=()):
+                 solo_tail: int = 0, solo_tail_alternatives=()):
     """The learned schedule run live against plain fixed budgets.
 
     An ensemble of the batched configuration's ranges is recorded for `mcs`
