@@ -96,6 +96,8 @@ def parse():
     p.add_argument("--schedule-every", type=int, default=500)
     p.add_argument("--schedule-solo-tail", type=int, default=0,
                    help="systems left in the batch at which power-of-two ones move to the single-system updater")
+    p.add_argument("--schedule-clusters", type=int, default=4,
+                   help="CTAs per cluster for the large systems in the schedule's batched runs")
     p.add_argument("--schedule-solo-tail-alt", default="",
                    help="comma-separated other thresholds to time the learned schedule with as well")
     a = p.parse_args()
@@ -565,7 +567,7 @@ def run_schedule(args, ranks):
     clocks = Clocks(ranks.local)
     clocks.start()
     rep = sch.live_compare(args.schedule, args.schedule_mcs, args.schedule_every, gpu=ranks.local,
-                           solo_tail=args.schedule_solo_tail,
+                           solo_tail=args.schedule_solo_tail, clusters=args.schedule_clusters,
                            solo_tail_alternatives=[int(v) for v in args.schedule_solo_tail_alt.split(",") if v])
     clk = clocks.stop()
     line = {"metric": "systems equilibrated per hour on 1 B200, learned schedule vs plain fixed budget at equal R_e^2 bias",

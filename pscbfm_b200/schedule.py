@@ -391,7 +391,7 @@ def round_up(x, every):
 
 def live_run(systems_, r250_seeds, budgets, every: int, recorder, max_mcs: int | None = None, grow: float = 1.5,
              judge: bool = True, order=None, gpu: int = 0, solo_tail: int = 0, sort_every: int = 5000, report=None,
-             solo_min_monomers: int = 16384):
+             solo_min_monomers: int = 16384, clusters: int = 4):
     """Run an ensemble live on the GPU under per-system budgets: system i
     advances `every` MCS per batched launch until its budget is spent; its
     R_e^2 is recorded after every launch; when the budget is spent and the
@@ -426,6 +426,8 @@ def live_run(systems_, r250_seeds, budgets, every: int, recorder, max_mcs: int |
     for i in order:
         b.add(systems_[i], rng=Rng.Saru, r250_seed=int(r250_seeds[i]))
     b.initialize()
+    if clusters != 4:
+        b.set_clusters(clusters)
     rec = recorder
     remaining = np.array([round_up(x, every) for x in budgets], np.int64)
     ran = np.zeros(nsys, np.int64)
@@ -563,7 +565,7 @@ def record_live(params, total_mcs: int, every: int, seed: int = 0, gpu: int = 0,
 
 def live_compare(n_systems: int = 2048, mcs: int = 200000, every: int = 1000, test_fraction: float = 0.25, epochs: int = 300,
                  seed: int = 3, gpu: int = 0, boxes=(32, 48, 64, 96, 128), n_range=(16, 512), phi_range=(0.1, 0.5),
-                 solo_tail: int = 0, solo_tail_alternatives=()):
+                 solo_tail: int = 0, solo_tail_alternatives=(), clusters: int = 4):
     """The learned schedule run live against plain fixed budgets.
 
     An ensemble of the batched configuration's ranges is recorded for `mcs`
@@ -628,14 +630,14 @@ def live_compare(n_systems: int = 2048, mcs: int = 200000, every: int = 1000, te
     rec = EndRecorder(mols)
     rep_l, rep_p = {}, {}
     wall_l, ran_l, ser_l, moves_l, dev_l = live_run(test_sys, seeds, budgets, every, rec, max_mcs=mcs, order=order, gpu=gpu,
-                                                    solo_tail=solo_tail, report=rep_l)
+                                                    solo_tail=solo_tail, report=rep_l, clusters=clusters)
     est_l = np.array([window_estimate(s, float(r)) for s, r in zip(ser_l, ran_l)])
     # the same learned schedule with other tail thresholds (same trajectories, other executors)
     alternatives = {}
     for k in solo_tail_alternatives:
         rep_k = {}
         w_k, ran_k, _, mv_k, dev_k = live_run(test_sys, seeds, budgets, every, rec, max_mcs=mcs, order=order, gpu=gpu,
-                                              solo_tail=int(k), report=rep_k)
+                                              solo_tail=int(k), report=rep_k, clusters=clusters)
         alternatives[str(int(k))] = {"wall_s": w_k, "device_s": dev_k / 1e3, "moves": int(mv_k),
                                      "same_mcs": bool(np.array_equal(ran_k, ran_l)), **rep_k}
     rel_l = (est_l - truth) / truth
@@ -654,7 +656,7 @@ def live_compare(n_systems: int = 2048, mcs: int = 200000, every: int = 1000, te
             B = float(b_)
             break
     wall_p, ran_p, ser_p, moves_p, dev_p = live_run(test_sys, seeds, np.full(len(te_a), B), every, rec, judge=False, gpu=gpu,
-                                                    solo_tail=solo_tail, report=rep_p)
+                                                    solo_tail=solo_tail, report=rep_p, clusters=clusters)
     est_p = np.array([window_estimate(s, float(r)) for s, r in zip(ser_p, ran_p)])
     rel_p = (est_p - truth) / truth
     # ensemble R_e^2 / N over molecules against the full-length runs
@@ -693,6 +695,7 @@ def live_compare(n_systems: int = 2048, mcs: int = 200000, every: int = 1000, te
                              "solo": (len(te_a) / solo_wall * 3600.0) if solo_wall else None},
         "live_runs_reproduce_the_record": bool(prefix),
         "learned_with_other_tail_thresholds": alternatives,
+        "clusters": clusters,
         "ratio_learned_vs_plain": wall_p / wall_l,
         "ratio_learned_vs_solo": (solo_wall / wall_l) if solo_wall else None,
     }
