@@ -283,7 +283,10 @@ int bfm_get_launch_info(const bfm_handle *h, int *mode, int *grid, int *threads,
 /* force a shape of the persistent kernel (tests, tuning): -1 automatic
  * (default), 0 gather, 1 stored codes, 2 staged; 3..5 the same with the
  * candidate lists in global instead of shared memory; 6..8 windowed with
- * 1, 2, 4 items per thread in flight (one CTA per SM, grid barriers);
+ * 1, 2, 4 items per thread in flight (one CTA per SM, grid barriers; 8
+ * tests the bonds of every item first and the leading face only of the
+ * items that pass, the automatic shape from 2048 items of a colour per SM
+ * on, 7 below);
  * 9, 10 windowed with 2 in flight on one thread-block cluster of 8 or 16
  * CTAs (hardware cluster barriers; small systems).
  * BFM_ERUNTIME when the shape does not fit this system. */

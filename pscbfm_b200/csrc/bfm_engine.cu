@@ -694,16 +694,19 @@ constexpr uint32_t kWinMaxSpecies = 32;
  * CTA's monomers (4 B), direction | bonds << 3 of this substep's items
  * (1 B), bond counts of all the CTA's monomers (1 B), then two sets (this
  * substep's and the previous one's) of per-warp candidate lists of
- * seg = 32 * ceil(W / T) entries. */
+ * seg = 32 * ceil(W / T) entries, then the items of this substep whose
+ * bonds allow the move (4 B each, W). */
 struct WinLayout {
     uint32_t W, T, P;
+    bool bf; /* bonds-first check: the list of items whose bonds allow the move */
     __host__ __device__ uint32_t seg() const { return 32u * ((W + T - 1u) / T); }
     __host__ __device__ size_t table() const { return 0; }
     __host__ __device__ size_t pos() const { return kWinTableBytes; }
     __host__ __device__ size_t x() const { return pos() + (size_t)P * 4; }
     __host__ __device__ size_t deg() const { return x() + W; }
     __host__ __device__ size_t lists() const { return (deg() + P + 15) & ~(size_t)15; }
-    __host__ __device__ size_t bytes() const { return lists() + (size_t)2 * (T / 32u) * seg() * 8u; }
+    __host__ __device__ size_t bondok() const { return lists() + (size_t)2 * (T / 32u) * seg() * 8u; }
+    __host__ __device__ size_t bytes() const { return bondok() + (bf ? (size_t)W * 4u : 0u); }
 };
 
 /* apply an accepted move: lattice bits, position (shared memory), image
@@ -770,8 +773,10 @@ __device__ __forceinline__ bool win_wait(GridBarrier *bar, unsigned int target, 
 
 /* one shape of the windowed kernel: U items per thread in flight in the
  * check phase; blockDim.x threads (a multiple of 32, 64 to 1024); CL: the
- * grid is one cluster (cluster barriers instead of grid barriers) */
-template <int RNG, int U, bool CL = false>
+ * grid is one cluster (cluster barriers instead of grid barriers); BF: the
+ * check tests the bonds of every item first and the leading face only of
+ * the items that pass (otherwise face and bonds together, item by item) */
+template <int RNG, int U, bool CL = false, bool BF = false>
 __global__ void __launch_bounds__(1024, 1)
     k_sweep_w(Sys s, const Substep *__restrict__ sched, uint32_t k0, uint32_t k1, GridBarrier *bar,
               unsigned long long timeoutNs, uint32_t maxdeg, uint32_t window, uint32_t nspec, uint32_t ptotal)
@@ -782,13 +787,15 @@ __global__ void __launch_bounds__(1024, 1)
     __shared__ uint32_t s_lo[kWinMaxSpecies], s_n[kWinMaxSpecies], s_off[kWinMaxSpecies], s_base[kWinMaxSpecies];
     __shared__ unsigned int s_wcnt[2][32];
 
-    const WinLayout lay{window, T, ptotal};
+    const WinLayout lay{window, T, ptotal, BF};
     const uint32_t seg = lay.seg();
     unsigned long long *s_tab = reinterpret_cast<unsigned long long *>(s_dyn + lay.table());
     uint32_t *spos = reinterpret_cast<uint32_t *>(s_dyn + lay.pos());
     uint8_t *px = s_dyn + lay.x();
     uint8_t *sdeg = s_dyn + lay.deg();
     uint2 *lists = reinterpret_cast<uint2 *>(s_dyn + lay.lists());
+    uint32_t *bondok = reinterpret_cast<uint32_t *>(s_dyn + lay.bondok());
+    __shared__ unsigned int s_nok[2];
 
     build_split_table(s_tab);
     for (uint32_t e = threadIdx.x; e < 96; e += T) { /* the CTA may have fewer than 96 threads */
@@ -811,6 +818,7 @@ __global__ void __launch_bounds__(1024, 1)
         s_off[threadIdx.x] = sp.off + lo;
     }
     if (threadIdx.x < 64) s_wcnt[threadIdx.x >> 5][threadIdx.x & 31u] = 0;
+    if (threadIdx.x < 2) s_nok[threadIdx.x] = 0;
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t b = 0;
@@ -874,8 +882,71 @@ __global__ void __launch_bounds__(1024, 1)
         uint2 *wlist = lists + ((size_t)p * NW + warp) * seg;
         unsigned long long *tb = tmp + (size_t)d.buf * words;
         unsigned int wc = 0; /* this warp's candidates (warp-uniform) */
+        if constexpr (BF) {
+        if (threadIdx.x == 0) s_nok[p ^ 1u] = 0; /* the next substep's count (last read a substep ago) */
 
-        /* phase A: U items per thread at a time */
+        /* phase A, pass 1: the bonds (and walls) of every item, U items per
+         * thread at a time.  In a dense melt most moves already fail here
+         * (about 70 % at volume fraction 0.5), so the items that pass are
+         * gathered into one CTA-wide list (a shared-memory atomic per warp
+         * and round) and only they take the leading-face test of pass 2,
+         * in full warps.  The candidates are the same items as with the
+         * face tested first; only their order in the lists differs, which
+         * no result depends on. */
+        for (uint32_t b0 = 0; b0 < n; b0 += (uint32_t)U * T) {
+            uint32_t x[U], ca[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint32_t w = b0 + (uint32_t)u * T + threadIdx.x;
+                x[u] = px[w < n ? w : 0u];
+                ca[u] = (maxdeg > 0 && w < n) ? bc_pair(bcode)[off + w] : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint32_t w = b0 + (uint32_t)u * T + threadIdx.x;
+                const int dir = (int)(x[u] & 7u);
+                const uint32_t dg = x[u] >> 3;
+                bool ok = w < n;
+                if (ok && geo.open) ok = !leaves_box(spos[base + w], dir, geo);
+                if (ok) {
+                    const uint32_t *after = s_after + dir * 16;
+                    const uint32_t a0 = ca[u] & 0x1FFu, a1 = (ca[u] >> 16) & 0x1FFu;
+                    if (dg > 0) ok = !((after[a0 >> 5] >> (a0 & 31u)) & 1u);
+                    if (dg > 1) ok = ok && !((after[a1 >> 5] >> (a1 & 31u)) & 1u);
+                    for (uint32_t j = 2; ok && j < dg; ++j) {
+                        const uint32_t c = bcode[(size_t)j * npad + off + w];
+                        if ((after[c >> 5] >> (c & 31u)) & 1u) ok = false;
+                    }
+                }
+                const unsigned int m = __ballot_sync(0xFFFFFFFFu, ok);
+                unsigned int at = 0;
+                if (lane == 0 && m) at = atomicAdd(&s_nok[p], (unsigned int)__popc(m));
+                at = __shfl_sync(0xFFFFFFFFu, at, 0);
+                if (ok) bondok[at + __popc(m & lanemask)] = w | ((uint32_t)dir << 28);
+            }
+        }
+        __syncthreads();
+        /* pass 2: the leading face of the items that passed, one per thread */
+        const uint32_t nok = s_nok[p];
+        for (uint32_t jw = warp * 32u; jw < nok; jw += T) { /* warp-uniform */
+            const uint32_t j = jw + lane;
+            const bool valid = j < nok;
+            const uint32_t e = bondok[valid ? j : jw];
+            const uint32_t w = e & 0x0FFFFFFFu;
+            const int dir = (int)(e >> 28);
+            const uint32_t r0 = spos[base + w];
+            const FaceW f = face_words(r0, dir, geo);
+            const bool ok = valid && occupied(lat, f) == 0ull;
+            if (ok) {
+                const uint32_t r1 = (dir & 1) ? zinc(r0, f.ma, f.ua) : zdec(r0, f.ma, f.ua);
+                atomicOr(tb + (r1 >> 6), 1ull << (r1 & 63u));
+            }
+            const unsigned int m = __ballot_sync(0xFFFFFFFFu, ok);
+            if (ok) wlist[wc + __popc(m & lanemask)] = make_uint2(e, r0);
+            wc += __popc(m);
+        }
+        } else {
+        /* phase A: U items per thread at a time, face and bonds together */
         for (uint32_t b0 = 0; b0 < n; b0 += (uint32_t)U * T) {
             FaceW f[U];
             uint32_t r0[U], x[U], ca[U];
@@ -922,6 +993,7 @@ __global__ void __launch_bounds__(1024, 1)
                 if (ok) wlist[wc + __popc(m & lanemask)] = make_uint2(w | ((uint32_t)dir << 28), r0[u]);
                 wc += __popc(m);
             }
+        }
         }
         if (lane == 0) s_wcnt[p][warp] = wc;
         nCand += lane == 0 ? wc : 0u;
@@ -1053,13 +1125,19 @@ constexpr int kWinU[5] = {1, 2, 4, 2, 2};
 /* windowed variants 3 and 4 (shapes 9, 10): the launch is one cluster of
  * 8 or 16 CTAs, for systems small enough that each CTA holds few monomers */
 constexpr int kWinCluster[5] = {0, 0, 0, 8, 16};
+/* variant 2 (shape 8) tests bonds first and the face of the items that pass */
+constexpr bool kWinBondFirst[5] = {false, false, true, false, false};
+/* the automatic shape: variant 2 once a CTA holds this many items of a
+ * colour (dense large systems, where most moves fail on their bonds and the
+ * face tests saved outweigh the extra pass), variant 1 below */
+constexpr uint32_t kWinBondFirstItems = 2048;
 
 template <int RNG>
 const void *win_kernel(int i)
 {
     return i == 0   ? (const void *)k_sweep_w<RNG, 1>
            : i == 1 ? (const void *)k_sweep_w<RNG, 2>
-           : i == 2 ? (const void *)k_sweep_w<RNG, 4>
+           : i == 2 ? (const void *)k_sweep_w<RNG, 4, false, true>
                     : (const void *)k_sweep_w<RNG, 2, true>;
 }
 
@@ -1648,7 +1726,7 @@ struct Engine {
         uint32_t P = 0; /* most items of all colours one CTA owns */
         for (uint32_t c = 0; c < nSpecies; ++c) P += (spec[c].n + grid - 1) / grid;
         P = (P + 15u) & ~15u;
-        const size_t smem = WinLayout{W, threads, P}.bytes();
+        const size_t smem = WinLayout{W, threads, P, kWinBondFirst[variant]}.bytes();
         if (smem > smemLimit) return false;
         const void *fn = win_kernel<RNG>(variant);
         raise_smem_limit(fn, smem);
@@ -1704,6 +1782,7 @@ struct Engine {
             return;
         }
         if (storedBonds) {
+            if (nmax / (uint32_t)smCount >= kWinBondFirstItems && configureWindowed<RNG>(smCount, smemLimit, 2)) return;
             if (configureWindowed<RNG>(smCount, smemLimit, 1)) return; /* 2 items in flight per thread */
             if (configureFor<RNG, SWEEP_STAGED>(smCount, smemLimit)) return;
             if (configureFor<RNG, SWEEP_STORED>(smCount, smemLimit)) return;
