@@ -699,7 +699,13 @@ constexpr uint32_t kWinMaxSpecies = 32;
 struct WinLayout {
     uint32_t W, T, P;
     bool bf; /* bonds-first check: the list of items whose bonds allow the move */
-    __host__ __device__ uint32_t seg() const { return 32u * ((W + T - 1u) / T); }
+    __host__ __device__ uint32_t seg() const
+    {
+        /* a warp's candidates: 32 per round of items (one-pass check), or
+         * 64 per block of the bonds-first list (W / 64 blocks over T / 32 warps) */
+        const uint32_t rounds = 32u * ((W + T - 1u) / T), blocks = 64u * ((W + 2u * T - 1u) / (2u * T));
+        return bf && blocks > rounds ? blocks : rounds;
+    }
     __host__ __device__ size_t table() const { return 0; }
     __host__ __device__ size_t pos() const { return kWinTableBytes; }
     __host__ __device__ size_t x() const { return pos() + (size_t)P * 4; }
@@ -926,24 +932,37 @@ __global__ void __launch_bounds__(1024, 1)
             }
         }
         __syncthreads();
-        /* pass 2: the leading face of the items that passed, one per thread */
+        /* pass 2: the leading face of the items that passed, in blocks of
+         * 64 per warp, a lane's two items with their lattice loads in
+         * flight together (one L2 round trip per block) */
         const uint32_t nok = s_nok[p];
-        for (uint32_t jw = warp * 32u; jw < nok; jw += T) { /* warp-uniform */
-            const uint32_t j = jw + lane;
-            const bool valid = j < nok;
-            const uint32_t e = bondok[valid ? j : jw];
-            const uint32_t w = e & 0x0FFFFFFFu;
-            const int dir = (int)(e >> 28);
-            const uint32_t r0 = spos[base + w];
-            const FaceW f = face_words(r0, dir, geo);
-            const bool ok = valid && occupied(lat, f) == 0ull;
-            if (ok) {
-                const uint32_t r1 = (dir & 1) ? zinc(r0, f.ma, f.ua) : zdec(r0, f.ma, f.ua);
-                atomicOr(tb + (r1 >> 6), 1ull << (r1 & 63u));
+        for (uint32_t cb = warp * 64u; cb < nok; cb += 64u * NW) { /* warp-uniform */
+            uint32_t e[2], r0[2];
+            FaceW f[2];
+            bool v[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const uint32_t j = cb + (uint32_t)u * 32u + lane;
+                v[u] = j < nok;
+                e[u] = bondok[v[u] ? j : cb];
+                r0[u] = spos[base + (e[u] & 0x0FFFFFFFu)];
+                f[u] = face_words(r0[u], (int)(e[u] >> 28), geo);
             }
-            const unsigned int m = __ballot_sync(0xFFFFFFFFu, ok);
-            if (ok) wlist[wc + __popc(m & lanemask)] = make_uint2(e, r0);
-            wc += __popc(m);
+            unsigned long long occ[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) occ[u] = v[u] ? occupied(lat, f[u]) : 1ull;
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const bool ok = occ[u] == 0ull;
+                if (ok) {
+                    const int dir = (int)(e[u] >> 28);
+                    const uint32_t r1 = (dir & 1) ? zinc(r0[u], f[u].ma, f[u].ua) : zdec(r0[u], f[u].ma, f[u].ua);
+                    atomicOr(tb + (r1 >> 6), 1ull << (r1 & 63u));
+                }
+                const unsigned int m = __ballot_sync(0xFFFFFFFFu, ok);
+                if (ok) wlist[wc + __popc(m & lanemask)] = make_uint2(e[u], r0[u]);
+                wc += __popc(m);
+            }
         }
         } else {
         /* phase A: U items per thread at a time, face and bonds together */
