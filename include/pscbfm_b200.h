@@ -282,7 +282,9 @@ int bfm_set_launch_mode(bfm_handle *h, int mode);
 int bfm_get_launch_info(const bfm_handle *h, int *mode, int *grid, int *threads, size_t *smem_bytes);
 /* force a shape of the persistent kernel (tests, tuning): -1 automatic
  * (default), 0 gather, 1 stored codes, 2 staged; 3..5 the same with the
- * candidate lists in global instead of shared memory; 6..8 windowed with
+ * candidate lists in global instead of shared memory (1 and 4 test the
+ * bonds of every item first and the leading face only of the items that
+ * pass); 6..8 windowed with
  * 1, 2, 4 items per thread in flight (one CTA per SM, grid barriers; 8
  * tests the bonds of every item first and the leading face only of the
  * items that pass, the automatic shape from 2048 items of a colour per SM

@@ -323,6 +323,13 @@ enum SweepMode {
     SWEEP_WINDOWED = 6 /* stored codes; independent work done inside the barrier waits (k_sweep_w), 6..8 */
 };
 
+/* k_sweep in the stored-code mode tests bonds first, on chunks of
+ * kBondFirstRounds items per thread, and keeps the items that pass (index
+ * and direction, position) in shared memory after the face table and the
+ * candidate list: 8 B for each item of a chunk */
+constexpr uint32_t kBondFirstRounds = 4;
+constexpr size_t kBondFirstBytes = (size_t)kBondFirstRounds * kSweepThreads * sizeof(uint2);
+
 /* The face-mask table in shared memory, split by word g of the face and
  * replicated kTabReplicas times (entry e, word g, copy r at
  * (g * 192 + e) * kTabReplicas + r), read by lane % kTabReplicas: lanes
@@ -396,6 +403,10 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
     uint8_t *st_dir = s_dyn + lay.dirs();
     uint2 *list = glist ? glist + (size_t)blockIdx.x * cap : reinterpret_cast<uint2 *>(s_dyn + (STAGE ? lay.list() : kWinTableBytes));
     unsigned long long *s_tab = reinterpret_cast<unsigned long long *>(s_dyn);
+    /* stored-code mode: the items of a chunk whose bonds allow the move */
+    uint2 *bondok = reinterpret_cast<uint2 *>(s_dyn + kWinTableBytes + (glist ? 0 : (size_t)cap * sizeof(uint2)));
+    __shared__ unsigned int s_nok[2];
+    uint32_t chunk = 0;
 
     build_split_table(s_tab);
     build_dir_table(s_dir, s.g);
@@ -412,6 +423,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
     }
     if (threadIdx.x == 0) {
         s_cnt[0] = s_cnt[1] = 0;
+        s_nok[0] = s_nok[1] = 0;
         if (STAGE) {
             mbar_init(&s_mbar, 1);
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -477,6 +489,90 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
 
         /* phase A: check this CTA's contiguous range [lo, hi) of the slab */
         unsigned long long *tb = tmp + (size_t)d.buf * words;
+        if constexpr (MODE == SWEEP_STORED) {
+            /* bonds first, on chunks of kBondFirstRounds items per thread
+             * (bond counts, bond codes and positions of a chunk loaded
+             * together); the items that pass -- most moves of a dense melt
+             * fail on their bonds -- take the leading-face test in blocks of
+             * 64 per warp, a lane's two lattice probes in flight together.
+             * Same candidates as the one-pass loop below, in another list
+             * order, on which no result depends.  Two counters alternate
+             * between chunks, so one CTA barrier per pass suffices. */
+            const uint32_t T = blockDim.x, NW = T >> 5, warp = threadIdx.x >> 5, lanemask = (1u << lane) - 1u;
+            for (uint32_t cb = lo; cb < hi; cb += kBondFirstRounds * T, ++chunk) {
+                unsigned int &nokc = s_nok[chunk & 1u];
+                if (threadIdx.x == 0) s_nok[(chunk + 1u) & 1u] = 0; /* last read before the previous chunk's end */
+                uint32_t dg[kBondFirstRounds], pr[kBondFirstRounds], r0[kBondFirstRounds];
+#pragma unroll
+                for (uint32_t u = 0; u < kBondFirstRounds; ++u) {
+                    const uint32_t ii = cb + u * T + threadIdx.x;
+                    const bool live = ii < hi;
+                    const uint32_t slot = sp.off + (live ? ii : lo);
+                    dg[u] = live ? deg[slot] : 0u;
+                    pr[u] = (live && maxdeg > 0) ? bc_pair(bcode)[slot] : 0u;
+                    r0[u] = live ? pos[slot] : 0u;
+                }
+#pragma unroll
+                for (uint32_t u = 0; u < kBondFirstRounds; ++u) {
+                    const uint32_t ii = cb + u * T + threadIdx.x;
+                    bool ok = ii < hi;
+                    int dir = 0;
+                    if (ok) {
+                        dir = direction(draw<RNG>(d.seed, d.iter, ii, d.iterHi));
+                        if (s.g.open) ok = !leaves_box(r0[u], dir, s.g);
+                        const uint32_t *after = s_after + dir * 16;
+                        const uint32_t ea = pr[u] & 0xFFFFu, eb = pr[u] >> 16;
+                        if (dg[u] > 0) ok = ok && !((after[ea >> 5] >> (ea & 31u)) & 1u);
+                        if (dg[u] > 1) ok = ok && !((after[eb >> 5] >> (eb & 31u)) & 1u);
+                        for (uint32_t j = 2; ok && j < dg[u]; ++j) {
+                            const uint32_t c = bcode[(size_t)j * npad + sp.off + ii];
+                            if ((after[c >> 5] >> (c & 31u)) & 1u) ok = false;
+                        }
+                    }
+                    const unsigned int m = __ballot_sync(0xFFFFFFFFu, ok);
+                    unsigned int at = 0;
+                    if (lane == 0 && m) at = atomicAdd(&nokc, (unsigned int)__popc(m));
+                    at = __shfl_sync(0xFFFFFFFFu, at, 0);
+                    if (ok) bondok[at + __popc(m & lanemask)] = make_uint2((ii - cb) | ((uint32_t)dir << 28), r0[u]);
+                }
+                __syncthreads();
+                const uint32_t nok = nokc;
+                for (uint32_t kb = warp * 64u; kb < nok; kb += 64u * NW) { /* warp-uniform */
+                    uint2 e[2];
+                    FaceW fw[2];
+                    bool v[2];
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        const uint32_t j = kb + (uint32_t)u * 32u + lane;
+                        v[u] = j < nok;
+                        e[u] = bondok[v[u] ? j : kb];
+                        fw[u] = face_words(e[u].y, (int)(e[u].x >> 28), s.g);
+                    }
+                    unsigned long long occ[2];
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) occ[u] = v[u] ? split_occupied(lat, fw[u], s_tab, lane) : 1ull;
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        const bool ok = occ[u] == 0ull;
+                        const int dir = (int)(e[u].x >> 28);
+                        if (ok) {
+                            const uint32_t r1 = dstep(e[u].y, dir, s_dir[dir]);
+                            atomicOr(tb + (r1 >> 6), 1ull << (r1 & 63u));
+                        }
+                        const unsigned int m = __ballot_sync(0xFFFFFFFFu, ok);
+                        if (m) {
+                            const int leader = __ffs(m) - 1;
+                            unsigned int at = 0;
+                            if ((int)lane == leader) at = atomicAdd(&cnt, (unsigned int)__popc(m));
+                            at = __shfl_sync(0xFFFFFFFFu, at, leader);
+                            if (ok) list[at + __popc(m & lanemask)] = make_uint2((sp.off + cb + (e[u].x & 0x0FFFFFFFu)) | ((uint32_t)dir << 28), e[u].y);
+                        }
+                        nCand += ok ? 1u : 0u;
+                    }
+                }
+                __syncthreads();
+            }
+        } else {
         uint32_t i = lo + threadIdx.x;
         uint32_t nr0 = 0, ndg = 0, na = 0, nb = 0;
         if (!STAGE && i < hi) {
@@ -567,6 +663,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
                 if (ok) list[at + __popc(m & ((1u << lane) - 1u))] = make_uint2((sp.off + i) | ((uint32_t)dir << 28), r0);
             }
             nCand += ok ? 1u : 0u;
+        }
         }
         if (!grid_barrier_count(bar, target, gridDim.x, timeoutNs)) {
             alive = false;
@@ -1709,6 +1806,10 @@ struct Engine {
         } else {
             if ((size_t)cap * sizeof(uint2) > kSweepSmemListMax) globalList = true;
             if (!globalList) smem += (size_t)cap * sizeof(uint2);
+            if (MODE == SWEEP_STORED) {
+                smem += kBondFirstBytes;
+                if (smem > smemLimit) return false;
+            }
         }
         raise_smem_limit((const void *)k_sweep<RNG, MODE>, smem);
         int fit = 0;

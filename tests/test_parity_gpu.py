@@ -111,7 +111,8 @@ def test_large_box_global_list_path():
     pb.r250_seed(12)
     u = pb.UpdaterGPUScBFM_AB_Type().setup(s, rng=pb.Rng.Saru)
     info = u.getLaunchInfo()
-    assert info["mode"] == 1 and info["smem_bytes"] == 4 * 192 * 8 * 8   # the face-mask table only
+    # the face-mask table and the bonds-first chunk (4 items x 1024 threads, 8 B each)
+    assert info["mode"] == 1 and info["smem_bytes"] == 4 * 192 * 8 * 8 + 4 * 1024 * 8
     u.runSimulationOnGPU(20)
     pos = u.getAllMonomerPositions().astype(np.int64)
     assert np.array_equal(u.getLattice(), oracle.lattice_words(pos, s.box))
