@@ -310,7 +310,7 @@ class UpdaterGPUScBFM_AB_Type:
         return {"mode": m.value, "ctas": g.value, "threads": t.value, "smem_bytes": b.value}
 
     def setSweepShape(self, shape: int):
-        """-1 automatic; 0 gather, 1 stored bond codes, 2 staged; +3 global
+        """-1 automatic; 0 gather, 1 stored bond codes (bonds tested first), 2 staged; +3 global
         candidate lists; 6..8 windowed with 1, 2, 4 items per thread in flight (8: bonds tested
         first, the leading face only of the items that pass); 9, 10 windowed on one cluster."""
         self._check(self._lib.bfm_set_sweep_shape(self._h, int(shape)))
