@@ -565,7 +565,8 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
                             unsigned int at = 0;
                             if ((int)lane == leader) at = atomicAdd(&cnt, (unsigned int)__popc(m));
                             at = __shfl_sync(0xFFFFFFFFu, at, leader);
-                            if (ok) list[at + __popc(m & lanemask)] = make_uint2((sp.off + cb + (e[u].x & 0x0FFFFFFFu)) | ((uint32_t)dir << 28), e[u].y);
+                            const uint32_t slot = sp.off + cb + (e[u].x & 0x0FFFFFFFu);
+                            if (ok) list[at + __popc(m & lanemask)] = make_uint2(slot | ((uint32_t)dir << 28), e[u].y);
                         }
                         nCand += ok ? 1u : 0u;
                     }
@@ -573,97 +574,97 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
                 __syncthreads();
             }
         } else {
-        uint32_t i = lo + threadIdx.x;
-        uint32_t nr0 = 0, ndg = 0, na = 0, nb = 0;
-        if (!STAGE && i < hi) {
-            const uint32_t slot = sp.off + i;
-            nr0 = pos[slot];
-            ndg = deg[slot];
-            if (STORED) {
-                const uint32_t pr = maxdeg > 0 ? bc_pair(bcode)[slot] : 0u;
-                na = pr & 0xFFFFu;
-                nb = pr >> 16;
-            } else {
-                na = maxdeg > 0 ? nbr[slot] : 0u;
-                nb = maxdeg > 1 ? nbr[(size_t)npad + slot] : 0u;
-            }
-        }
-        for (uint32_t base = lo; base < hi; base += blockDim.x, i += blockDim.x) {
-            const bool valid = i < hi;
-            uint32_t r0, dg, ea, eb;
-            int dir = 0;
-            if (STAGE) {
-                const uint32_t w = valid ? i - wlo : 0u;
-                r0 = st_pos[w];
-                dg = st_dg[w];
-                const uint32_t pr = maxdeg > 0 ? st_bc[w] : 0u;
-                ea = pr & 0xFFFFu;
-                eb = pr >> 16;
-                dir = st_dir[w];
-            } else {
-                r0 = nr0;
-                dg = ndg;
-                ea = na;
-                eb = nb;
-                const uint32_t inext = i + blockDim.x;
-                if (inext < hi) {
-                    const uint32_t slot = sp.off + inext;
-                    nr0 = pos[slot];
-                    ndg = deg[slot];
-                    if (STORED) {
-                        const uint32_t pr = maxdeg > 0 ? bc_pair(bcode)[slot] : 0u;
-                        na = pr & 0xFFFFu;
-                        nb = pr >> 16;
-                    } else {
-                        na = maxdeg > 0 ? nbr[slot] : 0u;
-                        nb = maxdeg > 1 ? nbr[(size_t)npad + slot] : 0u;
-                    }
-                }
-            }
-            bool ok = false;
-            if (valid) {
-                if (!STAGE) dir = direction(draw<RNG>(d.seed, d.iter, i, d.iterHi));
-                const DirConst dc = s_dir[dir];
-                const FaceW fw = face_words(r0, dir, s.g);
-                const uint32_t r1 = dstep(r0, dir, dc);
+            uint32_t i = lo + threadIdx.x;
+            uint32_t nr0 = 0, ndg = 0, na = 0, nb = 0;
+            if (!STAGE && i < hi) {
+                const uint32_t slot = sp.off + i;
+                nr0 = pos[slot];
+                ndg = deg[slot];
                 if (STORED) {
-                    const uint32_t *after = s_after + dir * 16;
-                    ok = !split_occupied(lat, fw, s_tab, lane) && !leaves_box(r0, dir, s.g);
-                    if (dg > 0) ok = ok && !((after[ea >> 5] >> (ea & 31u)) & 1u);
-                    if (dg > 1) ok = ok && !((after[eb >> 5] >> (eb & 31u)) & 1u);
-                    for (uint32_t j = 2; j < dg; ++j) {
-                        const uint32_t c = bcode[(size_t)j * npad + sp.off + i];
-                        if ((after[c >> 5] >> (c & 31u)) & 1u) ok = false;
-                    }
+                    const uint32_t pr = maxdeg > 0 ? bc_pair(bcode)[slot] : 0u;
+                    na = pr & 0xFFFFu;
+                    nb = pr >> 16;
                 } else {
-                    const uint32_t p0 = pos[ea];
-                    const uint32_t p1 = pos[eb];
-                    ok = !split_occupied(lat, fw, s_tab, lane) && !leaves_box(r0, dir, s.g);
-                    if (dg > 0) {
-                        const uint32_t c = zbond(p0, r1);
-                        ok = ok && !((s_forbid[c >> 5] >> (c & 31u)) & 1u);
-                    }
-                    if (dg > 1) {
-                        const uint32_t c = zbond(p1, r1);
-                        ok = ok && !((s_forbid[c >> 5] >> (c & 31u)) & 1u);
-                    }
-                    for (uint32_t j = 2; j < dg; ++j) {
-                        const uint32_t c = zbond(pos[nbr[(size_t)j * npad + sp.off + i]], r1);
-                        if ((s_forbid[c >> 5] >> (c & 31u)) & 1u) ok = false;
+                    na = maxdeg > 0 ? nbr[slot] : 0u;
+                    nb = maxdeg > 1 ? nbr[(size_t)npad + slot] : 0u;
+                }
+            }
+            for (uint32_t base = lo; base < hi; base += blockDim.x, i += blockDim.x) {
+                const bool valid = i < hi;
+                uint32_t r0, dg, ea, eb;
+                int dir = 0;
+                if (STAGE) {
+                    const uint32_t w = valid ? i - wlo : 0u;
+                    r0 = st_pos[w];
+                    dg = st_dg[w];
+                    const uint32_t pr = maxdeg > 0 ? st_bc[w] : 0u;
+                    ea = pr & 0xFFFFu;
+                    eb = pr >> 16;
+                    dir = st_dir[w];
+                } else {
+                    r0 = nr0;
+                    dg = ndg;
+                    ea = na;
+                    eb = nb;
+                    const uint32_t inext = i + blockDim.x;
+                    if (inext < hi) {
+                        const uint32_t slot = sp.off + inext;
+                        nr0 = pos[slot];
+                        ndg = deg[slot];
+                        if (STORED) {
+                            const uint32_t pr = maxdeg > 0 ? bc_pair(bcode)[slot] : 0u;
+                            na = pr & 0xFFFFu;
+                            nb = pr >> 16;
+                        } else {
+                            na = maxdeg > 0 ? nbr[slot] : 0u;
+                            nb = maxdeg > 1 ? nbr[(size_t)npad + slot] : 0u;
+                        }
                     }
                 }
-                if (ok) atomicOr(tb + (r1 >> 6), 1ull << (r1 & 63u));
+                bool ok = false;
+                if (valid) {
+                    if (!STAGE) dir = direction(draw<RNG>(d.seed, d.iter, i, d.iterHi));
+                    const DirConst dc = s_dir[dir];
+                    const FaceW fw = face_words(r0, dir, s.g);
+                    const uint32_t r1 = dstep(r0, dir, dc);
+                    if (STORED) {
+                        const uint32_t *after = s_after + dir * 16;
+                        ok = !split_occupied(lat, fw, s_tab, lane) && !leaves_box(r0, dir, s.g);
+                        if (dg > 0) ok = ok && !((after[ea >> 5] >> (ea & 31u)) & 1u);
+                        if (dg > 1) ok = ok && !((after[eb >> 5] >> (eb & 31u)) & 1u);
+                        for (uint32_t j = 2; j < dg; ++j) {
+                            const uint32_t c = bcode[(size_t)j * npad + sp.off + i];
+                            if ((after[c >> 5] >> (c & 31u)) & 1u) ok = false;
+                        }
+                    } else {
+                        const uint32_t p0 = pos[ea];
+                        const uint32_t p1 = pos[eb];
+                        ok = !split_occupied(lat, fw, s_tab, lane) && !leaves_box(r0, dir, s.g);
+                        if (dg > 0) {
+                            const uint32_t c = zbond(p0, r1);
+                            ok = ok && !((s_forbid[c >> 5] >> (c & 31u)) & 1u);
+                        }
+                        if (dg > 1) {
+                            const uint32_t c = zbond(p1, r1);
+                            ok = ok && !((s_forbid[c >> 5] >> (c & 31u)) & 1u);
+                        }
+                        for (uint32_t j = 2; j < dg; ++j) {
+                            const uint32_t c = zbond(pos[nbr[(size_t)j * npad + sp.off + i]], r1);
+                            if ((s_forbid[c >> 5] >> (c & 31u)) & 1u) ok = false;
+                        }
+                    }
+                    if (ok) atomicOr(tb + (r1 >> 6), 1ull << (r1 & 63u));
+                }
+                const unsigned int m = __ballot_sync(0xFFFFFFFFu, ok);
+                if (m) {
+                    const int leader = __ffs(m) - 1;
+                    unsigned int at = 0;
+                    if ((int)lane == leader) at = atomicAdd(&cnt, (unsigned int)__popc(m));
+                    at = __shfl_sync(0xFFFFFFFFu, at, leader);
+                    if (ok) list[at + __popc(m & ((1u << lane) - 1u))] = make_uint2((sp.off + i) | ((uint32_t)dir << 28), r0);
+                }
+                nCand += ok ? 1u : 0u;
             }
-            const unsigned int m = __ballot_sync(0xFFFFFFFFu, ok);
-            if (m) {
-                const int leader = __ffs(m) - 1;
-                unsigned int at = 0;
-                if ((int)lane == leader) at = atomicAdd(&cnt, (unsigned int)__popc(m));
-                at = __shfl_sync(0xFFFFFFFFu, at, leader);
-                if (ok) list[at + __popc(m & ((1u << lane) - 1u))] = make_uint2((sp.off + i) | ((uint32_t)dir << 28), r0);
-            }
-            nCand += ok ? 1u : 0u;
-        }
         }
         if (!grid_barrier_count(bar, target, gridDim.x, timeoutNs)) {
             alive = false;
@@ -986,130 +987,130 @@ __global__ void __launch_bounds__(1024, 1)
         unsigned long long *tb = tmp + (size_t)d.buf * words;
         unsigned int wc = 0; /* this warp's candidates (warp-uniform) */
         if constexpr (BF) {
-        if (threadIdx.x == 0) s_nok[p ^ 1u] = 0; /* the next substep's count (last read a substep ago) */
+            if (threadIdx.x == 0) s_nok[p ^ 1u] = 0; /* the next substep's count (last read a substep ago) */
 
-        /* phase A, pass 1: the bonds (and walls) of every item, U items per
-         * thread at a time.  In a dense melt most moves already fail here
-         * (about 70 % at volume fraction 0.5), so the items that pass are
-         * gathered into one CTA-wide list (a shared-memory atomic per warp
-         * and round) and only they take the leading-face test of pass 2,
-         * in full warps.  The candidates are the same items as with the
-         * face tested first; only their order in the lists differs, which
-         * no result depends on. */
-        for (uint32_t b0 = 0; b0 < n; b0 += (uint32_t)U * T) {
-            uint32_t x[U], ca[U];
+            /* phase A, pass 1: the bonds (and walls) of every item, U items per
+             * thread at a time.  In a dense melt most moves already fail here
+             * (about 70 % at volume fraction 0.5), so the items that pass are
+             * gathered into one CTA-wide list (a shared-memory atomic per warp
+             * and round) and only they take the leading-face test of pass 2,
+             * in full warps.  The candidates are the same items as with the
+             * face tested first; only their order in the lists differs, which
+             * no result depends on. */
+            for (uint32_t b0 = 0; b0 < n; b0 += (uint32_t)U * T) {
+                uint32_t x[U], ca[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const uint32_t w = b0 + (uint32_t)u * T + threadIdx.x;
-                x[u] = px[w < n ? w : 0u];
-                ca[u] = (maxdeg > 0 && w < n) ? bc_pair(bcode)[off + w] : 0u;
-            }
+                for (int u = 0; u < U; ++u) {
+                    const uint32_t w = b0 + (uint32_t)u * T + threadIdx.x;
+                    x[u] = px[w < n ? w : 0u];
+                    ca[u] = (maxdeg > 0 && w < n) ? bc_pair(bcode)[off + w] : 0u;
+                }
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const uint32_t w = b0 + (uint32_t)u * T + threadIdx.x;
-                const int dir = (int)(x[u] & 7u);
-                const uint32_t dg = x[u] >> 3;
-                bool ok = w < n;
-                if (ok && geo.open) ok = !leaves_box(spos[base + w], dir, geo);
-                if (ok) {
-                    const uint32_t *after = s_after + dir * 16;
-                    const uint32_t a0 = ca[u] & 0x1FFu, a1 = (ca[u] >> 16) & 0x1FFu;
-                    if (dg > 0) ok = !((after[a0 >> 5] >> (a0 & 31u)) & 1u);
-                    if (dg > 1) ok = ok && !((after[a1 >> 5] >> (a1 & 31u)) & 1u);
-                    for (uint32_t j = 2; ok && j < dg; ++j) {
-                        const uint32_t c = bcode[(size_t)j * npad + off + w];
-                        if ((after[c >> 5] >> (c & 31u)) & 1u) ok = false;
+                for (int u = 0; u < U; ++u) {
+                    const uint32_t w = b0 + (uint32_t)u * T + threadIdx.x;
+                    const int dir = (int)(x[u] & 7u);
+                    const uint32_t dg = x[u] >> 3;
+                    bool ok = w < n;
+                    if (ok && geo.open) ok = !leaves_box(spos[base + w], dir, geo);
+                    if (ok) {
+                        const uint32_t *after = s_after + dir * 16;
+                        const uint32_t a0 = ca[u] & 0x1FFu, a1 = (ca[u] >> 16) & 0x1FFu;
+                        if (dg > 0) ok = !((after[a0 >> 5] >> (a0 & 31u)) & 1u);
+                        if (dg > 1) ok = ok && !((after[a1 >> 5] >> (a1 & 31u)) & 1u);
+                        for (uint32_t j = 2; ok && j < dg; ++j) {
+                            const uint32_t c = bcode[(size_t)j * npad + off + w];
+                            if ((after[c >> 5] >> (c & 31u)) & 1u) ok = false;
+                        }
                     }
+                    const unsigned int m = __ballot_sync(0xFFFFFFFFu, ok);
+                    unsigned int at = 0;
+                    if (lane == 0 && m) at = atomicAdd(&s_nok[p], (unsigned int)__popc(m));
+                    at = __shfl_sync(0xFFFFFFFFu, at, 0);
+                    if (ok) bondok[at + __popc(m & lanemask)] = w | ((uint32_t)dir << 28);
                 }
-                const unsigned int m = __ballot_sync(0xFFFFFFFFu, ok);
-                unsigned int at = 0;
-                if (lane == 0 && m) at = atomicAdd(&s_nok[p], (unsigned int)__popc(m));
-                at = __shfl_sync(0xFFFFFFFFu, at, 0);
-                if (ok) bondok[at + __popc(m & lanemask)] = w | ((uint32_t)dir << 28);
             }
-        }
-        __syncthreads();
-        /* pass 2: the leading face of the items that passed, in blocks of
-         * 64 per warp, a lane's two items with their lattice loads in
-         * flight together (one L2 round trip per block) */
-        const uint32_t nok = s_nok[p];
-        for (uint32_t cb = warp * 64u; cb < nok; cb += 64u * NW) { /* warp-uniform */
-            uint32_t e[2], r0[2];
-            FaceW f[2];
-            bool v[2];
+            __syncthreads();
+            /* pass 2: the leading face of the items that passed, in blocks of
+             * 64 per warp, a lane's two items with their lattice loads in
+             * flight together (one L2 round trip per block) */
+            const uint32_t nok = s_nok[p];
+            for (uint32_t cb = warp * 64u; cb < nok; cb += 64u * NW) { /* warp-uniform */
+                uint32_t e[2], r0[2];
+                FaceW f[2];
+                bool v[2];
 #pragma unroll
-            for (int u = 0; u < 2; ++u) {
-                const uint32_t j = cb + (uint32_t)u * 32u + lane;
-                v[u] = j < nok;
-                e[u] = bondok[v[u] ? j : cb];
-                r0[u] = spos[base + (e[u] & 0x0FFFFFFFu)];
-                f[u] = face_words(r0[u], (int)(e[u] >> 28), geo);
-            }
-            unsigned long long occ[2];
-#pragma unroll
-            for (int u = 0; u < 2; ++u) occ[u] = v[u] ? occupied(lat, f[u]) : 1ull;
-#pragma unroll
-            for (int u = 0; u < 2; ++u) {
-                const bool ok = occ[u] == 0ull;
-                if (ok) {
-                    const int dir = (int)(e[u] >> 28);
-                    const uint32_t r1 = (dir & 1) ? zinc(r0[u], f[u].ma, f[u].ua) : zdec(r0[u], f[u].ma, f[u].ua);
-                    atomicOr(tb + (r1 >> 6), 1ull << (r1 & 63u));
+                for (int u = 0; u < 2; ++u) {
+                    const uint32_t j = cb + (uint32_t)u * 32u + lane;
+                    v[u] = j < nok;
+                    e[u] = bondok[v[u] ? j : cb];
+                    r0[u] = spos[base + (e[u] & 0x0FFFFFFFu)];
+                    f[u] = face_words(r0[u], (int)(e[u] >> 28), geo);
                 }
-                const unsigned int m = __ballot_sync(0xFFFFFFFFu, ok);
-                if (ok) wlist[wc + __popc(m & lanemask)] = make_uint2(e[u], r0[u]);
-                wc += __popc(m);
+                unsigned long long occ[2];
+#pragma unroll
+                for (int u = 0; u < 2; ++u) occ[u] = v[u] ? occupied(lat, f[u]) : 1ull;
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const bool ok = occ[u] == 0ull;
+                    if (ok) {
+                        const int dir = (int)(e[u] >> 28);
+                        const uint32_t r1 = (dir & 1) ? zinc(r0[u], f[u].ma, f[u].ua) : zdec(r0[u], f[u].ma, f[u].ua);
+                        atomicOr(tb + (r1 >> 6), 1ull << (r1 & 63u));
+                    }
+                    const unsigned int m = __ballot_sync(0xFFFFFFFFu, ok);
+                    if (ok) wlist[wc + __popc(m & lanemask)] = make_uint2(e[u], r0[u]);
+                    wc += __popc(m);
+                }
             }
-        }
         } else {
-        /* phase A: U items per thread at a time, face and bonds together */
-        for (uint32_t b0 = 0; b0 < n; b0 += (uint32_t)U * T) {
-            FaceW f[U];
-            uint32_t r0[U], x[U], ca[U];
-            unsigned long long occ[U];
+            /* phase A: U items per thread at a time, face and bonds together */
+            for (uint32_t b0 = 0; b0 < n; b0 += (uint32_t)U * T) {
+                FaceW f[U];
+                uint32_t r0[U], x[U], ca[U];
+                unsigned long long occ[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const uint32_t w = b0 + (uint32_t)u * T + threadIdx.x;
-                const uint32_t ws = w < n ? w : 0u;
-                r0[u] = spos[base + ws];
-                x[u] = px[ws];
-            }
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const uint32_t w = b0 + (uint32_t)u * T + threadIdx.x;
-                f[u] = face_words(r0[u], (int)(x[u] & 7u), geo);
-                occ[u] = 1ull;
-                ca[u] = 0u;
-                if (w < n) {
-                    occ[u] = occupied(lat, f[u]);
-                    if (maxdeg > 0) ca[u] = bc_pair(bcode)[off + w];
+                for (int u = 0; u < U; ++u) {
+                    const uint32_t w = b0 + (uint32_t)u * T + threadIdx.x;
+                    const uint32_t ws = w < n ? w : 0u;
+                    r0[u] = spos[base + ws];
+                    x[u] = px[ws];
                 }
-            }
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const uint32_t w = b0 + (uint32_t)u * T + threadIdx.x;
-                const int dir = (int)(x[u] & 7u);
-                const uint32_t dg = x[u] >> 3;
-                bool ok = occ[u] == 0ull && !leaves_box(r0[u], dir, geo);
-                if (ok) {
-                    const uint32_t *after = s_after + dir * 16;
-                    const uint32_t a0 = ca[u] & 0x1FFu, a1 = (ca[u] >> 16) & 0x1FFu;
-                    if (dg > 0) ok = !((after[a0 >> 5] >> (a0 & 31u)) & 1u);
-                    if (dg > 1) ok = ok && !((after[a1 >> 5] >> (a1 & 31u)) & 1u);
-                    for (uint32_t j = 2; ok && j < dg; ++j) {
-                        const uint32_t c = bcode[(size_t)j * npad + off + w];
-                        if ((after[c >> 5] >> (c & 31u)) & 1u) ok = false;
+                for (int u = 0; u < U; ++u) {
+                    const uint32_t w = b0 + (uint32_t)u * T + threadIdx.x;
+                    f[u] = face_words(r0[u], (int)(x[u] & 7u), geo);
+                    occ[u] = 1ull;
+                    ca[u] = 0u;
+                    if (w < n) {
+                        occ[u] = occupied(lat, f[u]);
+                        if (maxdeg > 0) ca[u] = bc_pair(bcode)[off + w];
                     }
                 }
-                if (ok) {
-                    const uint32_t r1 = (dir & 1) ? zinc(r0[u], f[u].ma, f[u].ua) : zdec(r0[u], f[u].ma, f[u].ua);
-                    atomicOr(tb + (r1 >> 6), 1ull << (r1 & 63u));
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const uint32_t w = b0 + (uint32_t)u * T + threadIdx.x;
+                    const int dir = (int)(x[u] & 7u);
+                    const uint32_t dg = x[u] >> 3;
+                    bool ok = occ[u] == 0ull && !leaves_box(r0[u], dir, geo);
+                    if (ok) {
+                        const uint32_t *after = s_after + dir * 16;
+                        const uint32_t a0 = ca[u] & 0x1FFu, a1 = (ca[u] >> 16) & 0x1FFu;
+                        if (dg > 0) ok = !((after[a0 >> 5] >> (a0 & 31u)) & 1u);
+                        if (dg > 1) ok = ok && !((after[a1 >> 5] >> (a1 & 31u)) & 1u);
+                        for (uint32_t j = 2; ok && j < dg; ++j) {
+                            const uint32_t c = bcode[(size_t)j * npad + off + w];
+                            if ((after[c >> 5] >> (c & 31u)) & 1u) ok = false;
+                        }
+                    }
+                    if (ok) {
+                        const uint32_t r1 = (dir & 1) ? zinc(r0[u], f[u].ma, f[u].ua) : zdec(r0[u], f[u].ma, f[u].ua);
+                        atomicOr(tb + (r1 >> 6), 1ull << (r1 & 63u));
+                    }
+                    const unsigned int m = __ballot_sync(0xFFFFFFFFu, ok);
+                    if (ok) wlist[wc + __popc(m & lanemask)] = make_uint2(w | ((uint32_t)dir << 28), r0[u]);
+                    wc += __popc(m);
                 }
-                const unsigned int m = __ballot_sync(0xFFFFFFFFu, ok);
-                if (ok) wlist[wc + __popc(m & lanemask)] = make_uint2(w | ((uint32_t)dir << 28), r0[u]);
-                wc += __popc(m);
             }
-        }
         }
         if (lane == 0) s_wcnt[p][warp] = wc;
         nCand += lane == 0 ? wc : 0u;
