@@ -126,6 +126,44 @@ def test_large_box_global_list_path():
         assert s.allowed[(d[:, 0] & 7) | ((d[:, 1] & 7) << 3) | ((d[:, 2] & 7) << 6)].all()
 
 
+def test_large_box_bonds_first_chunks_bit_exact():
+    """The 512^3 melt on the stored-code kernel: 28,000 items per CTA and
+    colour, so its bonds-first check runs seven chunks per substep with the
+    two alternating counters; bit-exact against the oracle."""
+    s = systems.ordered_melt(512)
+    pb.r250_seed(77)
+    st = pb.r250_get_state()
+    u = pb.UpdaterGPUScBFM_AB_Type().setup(s, rng=pb.Rng.Saru)
+    assert u.getLaunchInfo()["mode"] == 1
+    o = oracle.Sweep(s, rng=2, threads=8)
+    for nmcs in (2, 1):
+        u.runSimulationOnGPU(nmcs)
+        o.run(nmcs, st)
+        got = u.getAllMonomerPositions()
+        assert np.array_equal(got, o.positions())
+        assert np.array_equal(u.getLattice(), oracle.lattice_words(got, s.box))
+
+
+def test_windowed_bonds_first_several_blocks_per_warp():
+    """Shape 8 on 30,000 lone monomers (no bonds: every item passes the bond
+    test): about 200 list entries per CTA of 64 threads, so each warp takes
+    several blocks of 64 in the face pass; bit-exact against the oracle."""
+    s = systems.saw_chains(30000, 1, box=(128, 128, 128), seed=31)
+    pb.r250_seed(78)
+    st = pb.r250_get_state()
+    u = pb.UpdaterGPUScBFM_AB_Type().setup(s, rng=pb.Rng.Saru, steps_between_sortings=11)
+    u.setSweepShape(8)
+    info = u.getLaunchInfo()
+    assert info["mode"] == 8 and info["threads"] == 64
+    o = oracle.Sweep(s, rng=2, sort_every=11, threads=4)
+    for nmcs in (7, 20):
+        u.runSimulationOnGPU(nmcs)
+        o.run(nmcs, st)
+        got = u.getAllMonomerPositions()
+        assert np.array_equal(got, o.positions())
+        assert np.array_equal(u.getLattice(), oracle.lattice_words(got, s.box))
+
+
 def test_launch_paths_agree_and_can_be_switched():
     s = SYSTEMS["crosslinked"]
     out = []
